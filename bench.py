@@ -1,0 +1,576 @@
+#!/usr/bin/env python
+"""Benchmark: pseudo-spectral NS steps/s at 256^3 (FP32 bulk, FP64
+reductions) on B200, with the 3D-FFT GB/s and the FP64 step as secondary
+figures.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload ns256_fp32|ns256_fp64|fft256_c64|fft256_c128|...]
+
+A step is one fused NS step (exec/ns.cpp:167-217) of the stepper state that
+stays in HBM; `value` counts steps of all ranks per second (independent
+replicas, one per GPU, no collectives).  The 12 resident fields
+(1.6 GB at 256^3 complex64) exceed the 126 MB L2, so every step streams from
+HBM without a flush.  `e2e` runs the same job through the C-ABI from pinned
+host buffers: upload of the initial fields, bootstrap, K steps each followed
+by the divergence-monitor read (ns.cpp:210), download of the final velocity.
+
+`--impl reference` times the reference's own CPU code (src/*.cpp built in
+place against the project's FFTW/UPC++ shims, oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "NS steps/s @256^3 FP32 (3D FFT GB/s secondary)"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+# Algorithmic bytes of each pass of the fused step, in units of one field
+# (N^3 elements): the bytes it must read and write once.
+PASS_NAMES = ["K1 z-inverse+curl", "K2 y-inverse x6", "K3 x-inv+cross+x-fwd", "K4 y-forward x3",
+              "K5 z-forward+update"]
+PASS_FIELDS = [3 + 6, 6 + 6, 6 + 3, 3 + 3, 9 + 6]
+STEP_FIELDS = 30  # 9 FFTs x 2 + 12 for the spectral update
+
+WORKLOADS = {
+    "ns256_fp32": dict(kind="ns", n=256, prec="c64"),
+    "ns256_fp64": dict(kind="ns", n=256, prec="c128"),
+    "ns128_fp32": dict(kind="ns", n=128, prec="c64"),
+    "ns64_fp64": dict(kind="ns", n=64, prec="c128"),
+    "fft128_c64": dict(kind="fft", n=128, prec="c64"),
+    "fft256_c64": dict(kind="fft", n=256, prec="c64"),
+    "fft512_c64": dict(kind="fft", n=512, prec="c64"),
+    "fft128_c128": dict(kind="fft", n=128, prec="c128"),
+    "fft256_c128": dict(kind="fft", n=256, prec="c128"),
+    "fft512_c128": dict(kind="fft", n=512, prec="c128"),
+}
+NU, DT = 1.0 / 400, 2e-3  # config: nu = 1/400, dt = 2e-3
+
+
+def peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a window."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples = []
+        self.proc = None
+        self.t0 = self.t1 = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append((time.time(), line.strip()))
+
+    def window(self, t0, t1):
+        self.t0, self.t1 = t0, t1
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None:
+            return None
+        rows = []
+        for t, line in self.samples:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            rows.append((t, parts))
+        inwin = [p for t, p in rows if self.t0 is not None and self.t0 <= t <= self.t1]
+        used = inwin if inwin else [p for _, p in rows]
+        if not used:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(p[1]) for p in used if num(p[1]) is not None]
+        mx = [num(p[2]) for p in used if num(p[2]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for p in used:
+            for name, v in zip(names, p[5:9]):
+                if v.strip().lower() in ("active", "1", "yes"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(used), "in_timed_window": bool(inwin)}
+
+
+# ---------------------------------------------------------------- helpers
+def dist_setup(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def initial_velocity_hat(n, seed):
+    """Config-3 input: spectrum-seeded solenoidal field, Fourier, Nyquist zeroed."""
+    from spectral_upcxx_b200 import ic
+    u = ic.solenoidal_spectrum(n, seed=seed)
+    h = n // 2
+    out = []
+    for c in u:
+        f = np.fft.fftn(c)
+        f[h, :, :] = 0
+        f[:, h, :] = 0
+        f[:, :, h] = 0
+        out.append(f)
+    return out
+
+
+# ---------------------------------------------------------------- CPU side
+def cpu_ns_sample(n, V1, w1, c0, budget_s=25.0, max_steps=1):
+    """Time the reference's own ns.cpp loop body on the host cores."""
+    from oracle import pyoracle as O
+    cores = os.cpu_count() or 1
+    V = [np.ascontiguousarray(x, dtype=np.complex128) for x in V1]
+    W = [np.ascontiguousarray(x, dtype=np.complex128) for x in w1]
+    Cc = [np.ascontiguousarray(x, dtype=np.complex128) for x in c0]
+    if O.have_ref():
+        kind = "reference"
+        O.ref(True).ref_set_threads(cores)
+        secs, steps = 0.0, 0
+        while steps < max_steps and secs < budget_s:
+            secs += O.ref_ns_steps(V, W, Cc, NU, DT, 1)
+            steps += 1
+    else:
+        kind = "port"
+        os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+        steps = 1
+        secs = O.port_ns_seconds(V, W, Cc, NU, DT, 1)
+    return {"value": steps / secs, "unit": "steps/s", "cores": cores, "kind": kind,
+            "sample": f"{steps} NS step(s) of the {n}^3 complex128 exec/ns.cpp loop body "
+                      f"({secs:.2f} s), OpenMP over {cores} host threads"}
+
+
+def cpu_fft_sample(n, budget_s=20.0):
+    from oracle import pyoracle as O
+    from spectral_upcxx_b200 import ic
+    cores = os.cpu_count() or 1
+    f = ic.uniform_complex((n, n, n), 0)
+    if O.have_ref():
+        kind = "reference"
+        L = O.ref(False)
+        L.ref_set_threads(cores)
+        secs = L.ref_fft_roundtrip(O._ptr(f), n, n, n, 1)
+    else:
+        kind = "port"
+        t0 = time.perf_counter()
+        O.inverse(O.forward(f, zero=False))
+        secs = time.perf_counter() - t0
+    gbs = 4 * n ** 3 * 16 / secs / 1e9
+    return {"value": gbs, "unit": "GB/s", "cores": cores, "kind": kind,
+            "sample": f"1 forward+inverse 3D FFT of {n}^3 complex128 (exec/fft.cpp), "
+                      f"{secs:.2f} s"}
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    from oracle import pyoracle as O
+    wl = WORKLOADS[args.workload]
+    n = wl["n"]
+    cores = os.cpu_count() or 1
+    if wl["kind"] == "ns":
+        Vh = initial_velocity_hat(n, 1)
+        k = _k1d(n)
+        KZ, KY, KX = np.meshgrid(k, k, k, indexing="ij")
+        w = [1j * (KY * Vh[2] - KZ * Vh[1]), 1j * (KZ * Vh[0] - KX * Vh[2]),
+             1j * (KX * Vh[1] - KY * Vh[0])]
+        c0 = [np.zeros_like(Vh[0]) for _ in range(3)]
+        have = O.have_ref()
+        if have:
+            O.ref(True).ref_set_threads(cores)
+        step = (lambda: O.ref_ns_steps(Vh, w, c0, NU, DT, 1)) if have else \
+            (lambda: O.port_ns_seconds(Vh, w, c0, NU, DT, 1))
+        first = step()  # warm-up (page-in, plan caches)
+        budget = 150.0
+        steps = max(1, min(args.steps, int(budget / max(first, 1e-9))))
+        secs = sum(step() for _ in range(steps))
+        value = steps / secs
+        unit = "steps/s"
+        sample = (f"{steps} timed NS step(s) of {n}^3 complex128 (exec/ns.cpp loop body) after "
+                  f"1 warm-up step, {cores} host threads")
+        dtype = "f64"
+    else:
+        f = __import__("spectral_upcxx_b200.ic", fromlist=["ic"]).uniform_complex((n, n, n), 0)
+        if O.have_ref():
+            L = O.ref(False)
+            L.ref_set_threads(cores)
+            L.ref_fft_roundtrip(O._ptr(f), n, n, n, 1)
+            steps = max(1, min(args.steps, 10))
+            secs = sum(L.ref_fft_roundtrip(O._ptr(f), n, n, n, 1) for _ in range(steps))
+        else:
+            steps = 1
+            t0 = time.perf_counter()
+            O.inverse(O.forward(f, zero=False))
+            secs = time.perf_counter() - t0
+        value = 4 * n ** 3 * 16 * steps / secs / 1e9
+        unit = "GB/s"
+        sample = f"{steps} forward+inverse 3D FFT(s) of {n}^3 complex128 (exec/fft.cpp)"
+        dtype = "f64"
+    kind = "reference" if O.have_ref() else "port"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": unit, "n_gpus": world,
+        "steps": steps, "warmup": 1, "ms_per_step": 1000.0 / value if unit == "steps/s" else None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+        "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "grid": f"{n}^3", "nu": NU, "dt": DT,
+                   "backend": "reference src/*.cpp + project FP64 FFT behind the FFTW API"
+                   if kind == "reference" else "CPU oracle port"},
+        "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def _k1d(n):
+    i = np.arange(n)
+    return np.where(i <= n // 2, i, i - n).astype(np.float64)
+
+
+# ---------------------------------------------------------------- B200 arm
+def run_b200(args, rank, world, local):
+    import torch
+    import spectral_upcxx_b200 as S
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+    S.lib()
+    wl = WORKLOADS[args.workload]
+    n = wl["n"]
+    dtype = torch.complex64 if wl["prec"] == "c64" else torch.complex128
+    esz = 8 if wl["prec"] == "c64" else 16
+    field_bytes = n ** 3 * esz
+    hbm, peak_src = peaks()
+    stream = torch.cuda.Stream(dev)
+    clocks = ClockSampler(local)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return t.item()
+
+    result = {}
+    if wl["kind"] == "ns":
+        Vh = initial_velocity_hat(n, 1 + rank)
+        with torch.cuda.stream(stream):
+            Vd = [torch.from_numpy(x).to(dev, dtype) for x in Vh]
+            wd = S.curl(Vd)
+            st = S.NSStepper((n, n, n), NU, DT, dtype, device=dev)
+            st.bootstrap(Vd, wd)
+            st.step(args.warmup)
+        stream.synchronize()
+        clocks.start()
+        time.sleep(0.3)
+        barrier()
+        stream.synchronize()
+        st.profile(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t_wall0 = time.time()
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            st.step(args.steps)
+            e1.record(stream)
+        stream.synchronize()
+        t_wall1 = time.time()
+        barrier()
+        clocks.window(t_wall0, t_wall1)
+        ms = e0.elapsed_time(e1)
+        ms = max_over_ranks(ms)
+        passes = st.pass_times()
+        st.profile(False)
+        time.sleep(0.2)
+        clocks.stop()
+        stats = st.stats()
+        value = world * args.steps / (ms / 1e3)
+        # dominant kernel
+        avg = [tot / max(cnt, 1) for tot, cnt in passes]
+        top = int(np.argmax(avg))
+        alg = PASS_FIELDS[top] * field_bytes
+        achieved = alg / (avg[top] / 1e3) / 1e9
+        share = [a / sum(avg) for a in avg]
+        step_ms = ms / args.steps
+        result.update(
+            metric=METRIC, value=value, unit="steps/s", ms_per_step=step_ms,
+            dtype="fp32 bulk + fp64 reductions" if esz == 8 else "fp64",
+            roofline={"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                      "frac": achieved / hbm, "traffic": None,
+                      "kernel": PASS_NAMES[top],
+                      "algorithmic_bytes_per_launch": alg,
+                      "peak_source": f"{peak_src} hbm_gbs",
+                      "step": {"algorithmic_bytes": STEP_FIELDS * field_bytes,
+                               "achieved_gbs": STEP_FIELDS * field_bytes / (step_ms / 1e3) / 1e9,
+                               "frac": STEP_FIELDS * field_bytes / (step_ms / 1e3) / 1e9 / hbm},
+                      "passes": [{"name": nm, "ms": a, "share": sh,
+                                  "gbs": PASS_FIELDS[i] * field_bytes / (a / 1e3) / 1e9}
+                                 for i, (nm, a, sh) in enumerate(zip(PASS_NAMES, avg, share))]},
+            gpu_launches=args.steps * st.launches_per_step(),
+            diagnostics=stats)
+        # ---- e2e through the C-ABI from pinned host buffers
+        host_V = [torch.from_numpy(x).to(dtype).pin_memory() for x in Vh]
+        w_np = [w.cpu() for w in wd]
+        host_w = [w.pin_memory() for w in w_np]
+        out_V = [torch.empty((n, n, n), dtype=dtype).pin_memory() for _ in range(3)]
+        del Vd, wd
+        st.close()
+        torch.cuda.empty_cache()
+        e2e_steps = args.steps
+        barrier()
+        torch.cuda.synchronize()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            s0.record(stream)
+            Vd = [torch.empty((n, n, n), dtype=dtype, device=dev) for _ in range(3)]
+            wd = [torch.empty((n, n, n), dtype=dtype, device=dev) for _ in range(3)]
+            for a, b in zip(Vd + wd, host_V + host_w):
+                a.copy_(b, non_blocking=True)
+            st2 = S.NSStepper((n, n, n), NU, DT, dtype, device=dev)
+            st2.bootstrap(Vd, wd)
+            divs = []
+            for _ in range(e2e_steps):
+                st2.step(1)
+                divs.append(st2.stats()["div_avg"])  # ns.cpp:210 monitor, D2H + sync
+            fin = st2.state()["V1"]
+            for a, b in zip(out_V, fin):
+                a.copy_(b, non_blocking=True)
+            s1.record(stream)
+        stream.synchronize()
+        e2e_ms = max_over_ranks(s0.elapsed_time(s1))
+        st2.close()
+        result["e2e"] = {
+            "value": world * e2e_steps / (e2e_ms / 1e3), "unit": "steps/s",
+            "h2d_bytes_per_step": 6 * field_bytes / e2e_steps,
+            "d2h_bytes_per_step": (3 * field_bytes + 32 * e2e_steps) / e2e_steps,
+            "includes": "upload of V0/omega0 from pinned host, bootstrap (ns.cpp:132-153), "
+                        "K steps each with the div.average() read (ns.cpp:210), download of V1"}
+        del Vd, wd, fin
+        torch.cuda.empty_cache()
+        # ---- secondary figures (untimed for the headline)
+        if not args.no_secondary and rank == 0:
+            result["secondary"] = secondary(S, torch, dev, stream, n, hbm)
+        # ---- CPU baseline (rank 0, N = 1 only)
+        if rank == 0 and world == 1 and not args.no_cpu:
+            c0 = [np.zeros_like(Vh[0]) for _ in range(3)]
+            k = _k1d(n)
+            KZ, KY, KX = np.meshgrid(k, k, k, indexing="ij")
+            w = [1j * (KY * Vh[2] - KZ * Vh[1]), 1j * (KZ * Vh[0] - KX * Vh[2]),
+                 1j * (KX * Vh[1] - KY * Vh[0])]
+            result["cpu_baseline"] = cpu_ns_sample(n, Vh, w, c0)
+        cfg = {"workload": f"{args.workload}: plain NS step {n}^3, spectrum-seeded solenoidal "
+                           f"field (seed 1+rank), nu=1/400, dt=2e-3",
+               "grid": f"{n}^3", "precision": wl["prec"], "parallelism": f"replicas x{world}",
+               "l2": "no flush: 12 resident fields (%.2f GB) exceed the 126 MB L2" % (
+                   12 * field_bytes / 1e9)}
+    else:
+        result.update(fft_bench(S, torch, dev, stream, n, dtype, esz, args, world, hbm, peak_src,
+                                clocks, barrier, max_over_ranks))
+        if rank == 0 and world == 1 and not args.no_cpu:
+            result["cpu_baseline"] = cpu_fft_sample(n)
+        cfg = {"workload": f"{args.workload}: 3D C2C FFT forward+inverse {n}^3 {wl['prec']}, "
+                           f"uniform[-1,1) re/im (seeded)",
+               "grid": f"{n}^3", "precision": wl["prec"], "parallelism": f"replicas x{world}",
+               "l2": "inputs of %.2f GB per transform vs 126 MB L2" % (field_bytes / 1e9)}
+    clk = clocks.summary()
+    line = {"metric": result.pop("metric", METRIC), "value": result.pop("value"),
+            "unit": result.pop("unit"), "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": result.pop("ms_per_step"),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": result.pop("dtype"), "data": "synthetic (seeded)", "config": cfg}
+    if clk is not None:
+        line["clocks"] = clk
+    line.update(result)
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def fft_bench(S, torch, dev, stream, n, dtype, esz, args, world, hbm, peak_src, clocks, barrier,
+              max_over_ranks):
+    g = torch.Generator(device=dev).manual_seed(1)
+    with torch.cuda.stream(stream):
+        x = torch.complex(torch.rand((n, n, n), device=dev, generator=g) * 2 - 1,
+                          torch.rand((n, n, n), device=dev, generator=g) * 2 - 1).to(dtype)
+        for _ in range(args.warmup):
+            S.fft3d(x, -1)
+            S.fft3d(x, +1, normalise=True)
+    stream.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.time()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            S.fft3d(x, -1)
+            S.fft3d(x, +1, normalise=True)
+        e1.record(stream)
+    stream.synchronize()
+    t1 = time.time()
+    barrier()
+    clocks.window(t0, t1)
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    time.sleep(0.2)
+    clocks.stop()
+    alg = 4 * n ** 3 * esz
+    gbs = world * alg * args.steps / (ms / 1e3) / 1e9
+    per_pass = alg / 6
+    achieved = per_pass / (ms / args.steps / 6 / 1e3) / 1e9
+    # e2e: pinned host in, pinned host out
+    h = x.cpu().pin_memory()
+    out = torch.empty_like(h).pin_memory()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        s0.record(stream)
+        for _ in range(args.steps):
+            x.copy_(h, non_blocking=True)
+            S.fft3d(x, -1)
+            S.fft3d(x, +1, normalise=True)
+            out.copy_(x, non_blocking=True)
+        s1.record(stream)
+    stream.synchronize()
+    e2e_ms = max_over_ranks(s0.elapsed_time(s1))
+    return {"metric": "3D FFT forward+inverse GB/s", "value": gbs, "unit": "GB/s",
+            "ms_per_step": ms / args.steps, "dtype": "fp32" if esz == 8 else "fp64",
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None,
+                         "kernel": "line pass (avg of 6 per fwd+inv)",
+                         "peak_source": f"{peak_src} hbm_gbs"},
+            "gpu_launches": 6 * args.steps,
+            "e2e": {"value": world * alg * args.steps / (e2e_ms / 1e3) / 1e9, "unit": "GB/s",
+                    "h2d_bytes_per_step": n ** 3 * esz, "d2h_bytes_per_step": n ** 3 * esz}}
+
+
+def secondary(S, torch, dev, stream, n, hbm):
+    """FP64 NS step and 3D-FFT GB/s at n^3 (short runs, device events)."""
+    out = {}
+    Vh = initial_velocity_hat(n, 7)
+    for prec, dtype, esz in (("c128", torch.complex128, 16),):
+        with torch.cuda.stream(stream):
+            Vd = [torch.from_numpy(x).to(dev, dtype) for x in Vh]
+            wd = S.curl(Vd)
+            st = S.NSStepper((n, n, n), NU, DT, dtype, device=dev)
+            st.bootstrap(Vd, wd)
+            st.step(3)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st.step(20)
+            e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1) / 20
+        out[f"ns{n}_{prec}_steps_per_s"] = 1e3 / ms
+        out[f"ns{n}_{prec}_step_frac_of_hbm"] = 30 * n ** 3 * esz / (ms / 1e3) / 1e9 / hbm
+        st.close()
+        del Vd, wd
+    for prec, dtype, esz in (("c64", torch.complex64, 8), ("c128", torch.complex128, 16)):
+        g = torch.Generator(device=dev).manual_seed(2)
+        with torch.cuda.stream(stream):
+            x = torch.complex(torch.rand((n, n, n), device=dev, generator=g, dtype=torch.float64),
+                              torch.rand((n, n, n), device=dev, generator=g,
+                                         dtype=torch.float64)).to(dtype)
+            for _ in range(3):
+                S.fft3d(x, -1)
+                S.fft3d(x, +1, normalise=True)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(10):
+                S.fft3d(x, -1)
+                S.fft3d(x, +1, normalise=True)
+            e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1) / 10
+        out[f"fft{n}_{prec}_fwd_inv_gbs"] = 4 * n ** 3 * esz / (ms / 1e3) / 1e9
+        del x
+    torch.cuda.empty_cache()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="ns256_fp32")
+    ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, world, local = dist_setup(args)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_b200(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,170 @@
+/*
+ * spectral_b200 C-ABI -- the drop-in boundary of the B200 pseudo-spectral
+ * Navier-Stokes path.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status
+ * (0 = success, negative = error; sns_last_error() describes the last
+ * failure of the calling thread) and never throws or exits.  Field arrays are
+ * device pointers to interleaved complex numbers in the reference layout
+ * n = i + nx*j + nx*ny*k, x fastest (src/Scalar.cpp:683), either complex64
+ * (prec = SNS_C64) or complex128 (prec = SNS_C128).  `stream` is a
+ * cudaStream_t passed as void* (NULL = the legacy default stream); work is
+ * queued on it asynchronously unless a function says it synchronises.
+ * Dimensions must be powers of two up to 4096 per axis for the transforms.
+ *
+ * The reference (smsolivier/spectral_upcxx) is a C++ library; its callers use
+ * the Scalar / Vector / Operators / FFT1D classes.  Those classes are provided
+ * with unchanged signatures by spectral_upcxx_b200/api/*.H on top of this
+ * ABI, so the ABI is what an FFI (ctypes, cgo, JNI) binds.  Each declaration
+ * names the reference code it replaces.
+ */
+#ifndef SPECTRAL_B200_H
+#define SPECTRAL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SNS_C64 0  /* complex64: FP32 bulk arithmetic */
+#define SNS_C128 1 /* complex128: FP64, the reference's precision (src/FFT1D.H:13) */
+
+#define SNS_OK 0
+#define SNS_ERR_ARG (-1)
+#define SNS_ERR_UNSUPPORTED (-2)
+#define SNS_ERR_CUDA (-3)
+#define SNS_ERR_ALLOC (-4)
+#define SNS_ERR_TIMEOUT (-5)
+
+/* flags of sns_fft3d */
+#define SNS_FFT_NORMALISE 1   /* multiply by 1/(nx ny nz) (Scalar::inverse, src/Scalar.cpp:223-227) */
+#define SNS_FFT_ZERO_NYQUIST 2 /* zero the i=nx/2, j=ny/2, k=nz/2 planes (Scalar::zeroHighModes, src/Scalar.cpp:336-370) */
+
+/* ---- status ---------------------------------------------------------- */
+/* Text of the calling thread's last error ("" if none).  Replaces the
+ * print-and-exit ERROR macro (src/Scalar.cpp:9-13) below the C++ API. */
+const char* sns_last_error(void);
+int sns_version(void);
+
+/* ---- device memory (caching pool) ------------------------------------ */
+/* Stream-ordered caching allocator for field storage.  Replaces
+ * upcxx::new_array / delete_array in Scalar::init and ~Scalar
+ * (src/Scalar.cpp:38-40, 95, 117).  sns_free returns the block to the pool;
+ * a later sns_malloc may hand it out again for work on the same stream. */
+int sns_malloc(void** ptr, size_t bytes);
+int sns_free(void* ptr);
+int sns_pool_trim(void);
+int sns_memcpy_h2d(void* dst, const void* src, size_t bytes, void* stream);
+int sns_memcpy_d2h(void* dst, const void* src, size_t bytes, void* stream);
+/* deep copy (Scalar copy constructor / operator=, src/Scalar.cpp:52-66) */
+int sns_memcpy_d2d(void* dst, const void* src, size_t bytes, void* stream);
+int sns_memset(void* ptr, int value, size_t bytes, void* stream);
+int sns_stream_synchronize(void* stream);
+/* precision conversion of n complex values (either direction or a copy) */
+int sns_convert(void* dst, int dst_prec, const void* src, int src_prec, int64_t n,
+                void* stream);
+
+/* ---- transforms -------------------------------------------------------- */
+/* In-place unnormalised 3D DFT of one field.  dir = -1 forward
+ * (exp(-2 pi i jk/n)), +1 inverse -- the sign convention of
+ * Scalar::transform (src/Scalar.cpp:400-646; FFT1D::transform's DIR,
+ * src/FFT1D.cpp:95-101).  flags: SNS_FFT_NORMALISE | SNS_FFT_ZERO_NYQUIST. */
+int sns_fft3d(void* field, int64_t nx, int64_t ny, int64_t nz, int dir, int flags, int prec,
+              void* stream);
+/* The same transform over up to 6 fields of equal shape in one batch. */
+int sns_fft3d_many(void* const* fields, int nfields, int64_t nx, int64_t ny, int64_t nz,
+                   int dir, int flags, int prec, void* stream);
+/* Scalar::forward(): transform(-1) + zeroHighModes (src/Scalar.cpp:208-215). */
+int sns_forward(void* field, int64_t nx, int64_t ny, int64_t nz, int prec, void* stream);
+/* Scalar::inverse(): transform(+1) then divide by N (src/Scalar.cpp:217-229). */
+int sns_inverse(void* field, int64_t nx, int64_t ny, int64_t nz, int prec, void* stream);
+/* Batched in-place 1D DFTs: `howmany` lines of n elements `stride` apart,
+ * line b starting at element b*dist.  Backs FFT1D::transform(ptr, N, stride,
+ * DIR) and FFT1D::init/transform(ptr, DIR) (src/FFT1D.cpp:14-101), which
+ * run one strided line per FFTW call; unnormalised. */
+int sns_fft1d_many(void* data, int64_t n, int64_t stride, int64_t howmany, int64_t dist,
+                   int dir, int prec, void* stream);
+
+/* ---- spectral operators (Fourier-space fields) ------------------------ */
+/* Scalar::zeroHighModes (src/Scalar.cpp:336-370). */
+int sns_zero_high_modes(void* field, int64_t nx, int64_t ny, int64_t nz, int prec,
+                        void* stream);
+/* Scalar::gradient: g_d = i k_d f (src/Scalar.cpp:245-276). */
+int sns_gradient(const void* f, void* gx, void* gy, void* gz, int64_t nx, int64_t ny,
+                 int64_t nz, int prec, void* stream);
+/* Scalar::laplacian: -|k|^2 f (src/Scalar.cpp:278-306). */
+int sns_laplacian(const void* f, void* out, int64_t nx, int64_t ny, int64_t nz, int prec,
+                  void* stream);
+/* Scalar::laplacian_inverse(a, b): f /= (a - b|k|^2) where |k|^2 != 0
+ * (src/Scalar.cpp:308-334). */
+int sns_laplacian_inverse(void* f, double a, double b, int64_t nx, int64_t ny, int64_t nz,
+                          int prec, void* stream);
+/* Vector::curl: i k x v (src/Vector.cpp:92-122). */
+int sns_curl(const void* const v[3], void* const out[3], int64_t nx, int64_t ny, int64_t nz,
+             int prec, void* stream);
+/* Vector::divergence: sum_d i k_d v_d (src/Vector.cpp:124-153). */
+int sns_divergence(const void* const v[3], void* out, int64_t nx, int64_t ny, int64_t nz,
+                   int prec, void* stream);
+/* Vector::laplacian: -|k|^2 v_d (src/Vector.cpp:155-181). */
+int sns_vector_laplacian(const void* const v[3], void* const out[3], int64_t nx, int64_t ny,
+                         int64_t nz, int prec, void* stream);
+/* Vector::cross (src/Vector.cpp:66-90): inverse-transform copies of both
+ * Fourier operands, complex point-wise a x b, forward transform with Nyquist
+ * zeroing.  out may alias neither input.  Uses 6 fields of pooled scratch. */
+int sns_cross(const void* const a[3], const void* const b[3], void* const out[3], int64_t nx,
+              int64_t ny, int64_t nz, int prec, void* stream);
+/* Scalar::average: mean of |f_i| over n values, accumulated in FP64
+ * (src/Scalar.cpp:15-22).  Synchronises `stream`; the result is written to
+ * the host double *out. */
+int sns_average_abs(const void* f, int64_t n, int prec, double* out, void* stream);
+
+/* ---- element-wise Operators (src/Operators.cpp:9-99) ------------------ */
+/* out = alpha*x + beta*y; y may be NULL (out = alpha*x).  Covers Scalar and
+ * Vector +, -, and double*Scalar / double*Vector. */
+int sns_axpby(double alpha, const void* x, double beta, const void* y, void* out, int64_t n,
+              int prec, void* stream);
+/* out = a*b element-wise (Scalar operator*, src/Operators.cpp:9-19). */
+int sns_mul(const void* a, const void* b, void* out, int64_t n, int prec, void* stream);
+
+/* ---- fused Navier-Stokes stepper (exec/ns.cpp:132-217) ---------------- */
+typedef struct sns_ns sns_ns;
+/* Create a stepper for an nx*ny*nz box with viscosity nu and time step dt
+ * (ns.cpp:43-46).  Allocates its state and work fields (12 fields). */
+int sns_ns_create(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double nu, double dt,
+                  int prec, void* stream);
+int sns_ns_destroy(sns_ns* handle);
+/* Start from Fourier V0 and omega0 = curl V0: the Pi0 projection and the
+ * Forward-Euler first step (ns.cpp:132-153).  Device pointers in the
+ * stepper's precision. */
+int sns_ns_bootstrap(sns_ns* handle, const void* const V0[3], const void* const omega0[3]);
+/* Set the AB2 state directly: Fourier V1 and cross0 (= V0 x omega0). */
+int sns_ns_set_state(sns_ns* handle, const void* const V1[3], const void* const cross0[3]);
+/* Advance nsteps AB2 / projection / Crank-Nicolson steps (ns.cpp:167-217),
+ * queued on the stepper's stream without host synchronisation. */
+int sns_ns_step(sns_ns* handle, int nsteps);
+/* Copy out V1, omega1 = curl V1 and cross0 (any pointer may be NULL). */
+int sns_ns_get_state(sns_ns* handle, void* const V1[3], void* const omega1[3],
+                     void* const cross0[3]);
+/* Diagnostics of the velocity after the last step, accumulated in FP64:
+ * the divergence monitor div.average() (ns.cpp:209-210), kinetic energy
+ * 0.5<|u|^2>, enstrophy 0.5<|omega|^2> and max |div u_hat|.  Synchronises. */
+int sns_ns_stats(sns_ns* handle, double* div_avg, double* energy, double* enstrophy,
+                 double* max_div);
+/* Number of kernel launches one sns_ns_step(h, 1) issues. */
+int sns_ns_launches_per_step(sns_ns* handle);
+/* Per-pass timing (no reference counterpart; the reference times phases with
+ * CH_Timer, src/Scalar.cpp:421-617).  While enabled, every step records CUDA
+ * events between its passes on the stepper's stream; enabling clears the
+ * totals.  sns_ns_pass_times synchronises and returns, per pass, the summed
+ * milliseconds and the number of timed launches (arrays of `max` entries);
+ * the return value is the number of passes per step, or a negative error. */
+int sns_ns_profile(sns_ns* handle, int enable);
+int sns_ns_pass_times(sns_ns* handle, double* total_ms, int* launches, int max);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

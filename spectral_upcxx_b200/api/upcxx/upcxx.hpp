@@ -1,0 +1,105 @@
+// Single-GPU stand-in for the UPC++ calls the reference's drivers make
+// (exec/ns.cpp:28, 79, 162, 225, 229; test/operators.cpp:9, 200; exec/fft.cpp
+// and test/3d_fft.cpp use the pointer and future calls).  The B200 build runs
+// one process per box, so there is one rank; the field classes keep their
+// data in HBM and never use these pointers.  Copies are host memcpys and
+// futures are always ready.
+#ifndef SNS_UPCXX_SINGLE_RANK_HPP
+#define SNS_UPCXX_SINGLE_RANK_HPP
+
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <iostream>
+#include <utility>
+
+namespace upcxx {
+
+inline void init() {}
+inline void finalize() {}
+inline int rank_me() { return 0; }
+inline int rank_n() { return 1; }
+inline void barrier() {}
+
+template <typename T>
+class global_ptr {
+ public:
+  global_ptr() = default;
+  global_ptr(std::nullptr_t) {}
+  explicit global_ptr(T* p) : p_(p) {}
+  T* local() const { return p_; }
+  template <typename I>
+  global_ptr operator+(I d) const {
+    return global_ptr(p_ + d);
+  }
+  bool operator==(std::nullptr_t) const { return p_ == nullptr; }
+  bool operator!=(std::nullptr_t) const { return p_ != nullptr; }
+  bool operator==(const global_ptr& o) const { return p_ == o.p_; }
+  bool operator!=(const global_ptr& o) const { return p_ != o.p_; }
+  bool is_null() const { return p_ == nullptr; }
+  int where() const { return 0; }
+
+ private:
+  T* p_ = nullptr;
+};
+
+template <typename... T>
+class future;
+template <>
+class future<> {
+ public:
+  void wait() const {}
+  bool ready() const { return true; }
+};
+template <typename T>
+class future<T> {
+ public:
+  explicit future(T v) : v_(std::move(v)) {}
+  T wait() const { return v_; }
+  bool ready() const { return true; }
+
+ private:
+  T v_;
+};
+
+inline future<> make_future() { return {}; }
+inline future<> when_all(const future<>&, const future<>&) { return {}; }
+
+template <typename T>
+global_ptr<T> new_array(std::size_t n) {
+  return global_ptr<T>(new T[n]());
+}
+template <typename T>
+void delete_array(global_ptr<T> p) {
+  delete[] p.local();
+}
+template <typename T>
+future<T> broadcast(T v, int) {
+  return future<T>(std::move(v));
+}
+template <typename T>
+future<> rput(T v, global_ptr<T> dst) {
+  *dst.local() = v;
+  return {};
+}
+template <typename T>
+future<> rput(const T* src, global_ptr<T> dst, std::size_t n) {
+  std::memcpy((void*)dst.local(), (const void*)src, n * sizeof(T));
+  return {};
+}
+template <typename T>
+future<T> rget(global_ptr<T> src) {
+  return future<T>(*src.local());
+}
+template <typename T, typename Op>
+future<T> allreduce(T v, Op) {
+  return future<T>(v);
+}
+struct persona_scope {};
+inline persona_scope default_persona_scope() { return {}; }
+
+}  // namespace upcxx
+
+#endif

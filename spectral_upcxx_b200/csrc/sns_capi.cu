@@ -1,0 +1,638 @@
+// extern "C" entry points of include/spectral_b200.h: argument checking,
+// the caching device pool, and the fused NS stepper object.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/spectral_b200.h"
+#include "sns_common.cuh"
+#include "sns_fft.cuh"
+#include "sns_ns.cuh"
+#include "sns_ops.cuh"
+
+namespace sns {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string& msg) { g_err = msg; }
+const char* last_error() { return g_err.c_str(); }
+
+int cuda_status(cudaError_t e, const char* where) {
+  if (e == cudaSuccess) return OK;
+  set_error(std::string(where) + ": " + cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? ERR_ALLOC : ERR_CUDA;
+}
+
+int sm_count() {
+  static int cached[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int& c = cached[dev & 63];
+  if (c == 0) {
+    if (cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || c <= 0)
+      c = 148;
+  }
+  return c;
+}
+
+// ---- caching pool ----------------------------------------------------------
+namespace {
+struct Pool {
+  std::mutex mu;
+  std::map<void*, std::pair<int, size_t>> live;          // ptr -> (device, bytes)
+  std::map<std::pair<int, size_t>, std::vector<void*>> free_;  // (device, bytes) -> blocks
+};
+Pool& pool() {
+  static Pool* p = new Pool();  // never destroyed: blocks outlive static teardown
+  return *p;
+}
+size_t round_bytes(size_t b) { return (b + 255) & ~(size_t)255; }
+
+int trim_locked(Pool& p) {
+  for (auto& kv : p.free_)
+    for (void* q : kv.second) cudaFree(q);
+  p.free_.clear();
+  return OK;
+}
+}  // namespace
+
+int pool_malloc(void** ptr, size_t bytes) {
+  if (!ptr) {
+    set_error("sns_malloc: null output pointer");
+    return ERR_ARG;
+  }
+  *ptr = nullptr;
+  if (bytes == 0) return OK;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const size_t b = round_bytes(bytes);
+  Pool& p = pool();
+  std::lock_guard<std::mutex> lock(p.mu);
+  auto key = std::make_pair(dev, b);
+  auto it = p.free_.find(key);
+  if (it != p.free_.end() && !it->second.empty()) {
+    *ptr = it->second.back();
+    it->second.pop_back();
+    p.live[*ptr] = key;
+    return OK;
+  }
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, b);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    trim_locked(p);
+    e = cudaMalloc(&q, b);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      set_error("sns_malloc(" + std::to_string(bytes) + " bytes): " + cudaGetErrorString(e));
+      return ERR_ALLOC;
+    }
+  }
+  p.live[q] = key;
+  *ptr = q;
+  return OK;
+}
+
+int pool_free(void* ptr) {
+  if (!ptr) return OK;
+  Pool& p = pool();
+  std::lock_guard<std::mutex> lock(p.mu);
+  auto it = p.live.find(ptr);
+  if (it == p.live.end()) {
+    set_error("sns_free: pointer not from sns_malloc");
+    return ERR_ARG;
+  }
+  p.free_[it->second].push_back(ptr);
+  p.live.erase(it);
+  return OK;
+}
+
+static inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+static inline size_t esize(int prec) { return prec == PREC_C128 ? 16 : 8; }
+
+static bool check_prec(int prec) {
+  if (prec != PREC_C64 && prec != PREC_C128) {
+    set_error("precision must be SNS_C64 (0) or SNS_C128 (1)");
+    return false;
+  }
+  return true;
+}
+static bool check_dims(int64_t nx, int64_t ny, int64_t nz) {
+  if (nx < 1 || ny < 1 || nz < 1 || nx > (1 << 20) || ny > (1 << 20) || nz > (1 << 20) ||
+      nx * ny * nz >= ((int64_t)1 << 32)) {
+    set_error("dimensions out of range");
+    return false;
+  }
+  return true;
+}
+static bool nonnull(const void* p, const char* what) {
+  if (!p) {
+    set_error(std::string(what) + ": null pointer");
+    return false;
+  }
+  return true;
+}
+
+// Vector::cross on device fields (src/Vector.cpp:66-90), scratch = 6 fields.
+int vector_cross(const void* const a[3], const void* const b[3], void* const out[3], Dims d,
+                 int prec, void* const scratch[6], cudaStream_t s) {
+  const size_t bytes = esize(prec) * d.n();
+  int rc;
+  for (int i = 0; i < 3; i++) {
+    if ((rc = cuda_status(cudaMemcpyAsync(scratch[i], a[i], bytes, cudaMemcpyDeviceToDevice, s),
+                          "cross copy")))
+      return rc;
+    if ((rc = cuda_status(
+             cudaMemcpyAsync(scratch[3 + i], b[i], bytes, cudaMemcpyDeviceToDevice, s),
+             "cross copy")))
+      return rc;
+  }
+  if ((rc = fft3d(scratch, 6, d.nx, d.ny, d.nz, +1, PASS_SCALE, prec, s))) return rc;
+  const void* u[3] = {scratch[0], scratch[1], scratch[2]};
+  const void* w[3] = {scratch[3], scratch[4], scratch[5]};
+  if ((rc = op_cross_pointwise(u, w, out, d.n(), prec, s))) return rc;
+  return fft3d(out, 3, d.nx, d.ny, d.nz, -1, PASS_ZERO_NYQUIST, prec, s);
+}
+
+}  // namespace sns
+
+using namespace sns;
+
+// ---- stepper object ----------------------------------------------------------
+struct sns_ns {
+  NSPlan pl;
+  double nu, dt;
+  cudaStream_t s;
+  void* V[3];
+  void* C0[3];
+  void* U[6];
+  double* stats_part;
+  double* stats_out;
+  bool stepped;
+  // per-pass profiling
+  bool profiling = false;
+  int recorded = 0;
+  std::vector<cudaEvent_t> events;  // (kNSPasses + 1) per recorded step
+};
+
+extern "C" {
+
+const char* sns_last_error(void) { return sns::last_error(); }
+int sns_version(void) { return 1; }
+
+int sns_malloc(void** ptr, size_t bytes) { return pool_malloc(ptr, bytes); }
+int sns_free(void* ptr) { return pool_free(ptr); }
+int sns_pool_trim(void) {
+  Pool& p = pool();
+  std::lock_guard<std::mutex> lock(p.mu);
+  return trim_locked(p);
+}
+
+int sns_memcpy_h2d(void* dst, const void* src, size_t bytes, void* stream) {
+  if (bytes == 0) return OK;
+  if (!nonnull(dst, "sns_memcpy_h2d") || !nonnull(src, "sns_memcpy_h2d")) return ERR_ARG;
+  return cuda_status(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, S(stream)),
+                     "sns_memcpy_h2d");
+}
+int sns_memcpy_d2h(void* dst, const void* src, size_t bytes, void* stream) {
+  if (bytes == 0) return OK;
+  if (!nonnull(dst, "sns_memcpy_d2h") || !nonnull(src, "sns_memcpy_d2h")) return ERR_ARG;
+  return cuda_status(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, S(stream)),
+                     "sns_memcpy_d2h");
+}
+int sns_memcpy_d2d(void* dst, const void* src, size_t bytes, void* stream) {
+  if (bytes == 0) return OK;
+  if (!nonnull(dst, "sns_memcpy_d2d") || !nonnull(src, "sns_memcpy_d2d")) return ERR_ARG;
+  return cuda_status(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, S(stream)),
+                     "sns_memcpy_d2d");
+}
+int sns_memset(void* ptr, int value, size_t bytes, void* stream) {
+  if (bytes == 0) return OK;
+  if (!nonnull(ptr, "sns_memset")) return ERR_ARG;
+  return cuda_status(cudaMemsetAsync(ptr, value, bytes, S(stream)), "sns_memset");
+}
+int sns_stream_synchronize(void* stream) {
+  return cuda_status(cudaStreamSynchronize(S(stream)), "sns_stream_synchronize");
+}
+int sns_convert(void* dst, int dst_prec, const void* src, int src_prec, int64_t n,
+                void* stream) {
+  if (!check_prec(dst_prec) || !check_prec(src_prec)) return ERR_ARG;
+  if (n < 0) {
+    set_error("sns_convert: negative count");
+    return ERR_ARG;
+  }
+  if (n == 0) return OK;
+  if (!nonnull(dst, "sns_convert") || !nonnull(src, "sns_convert")) return ERR_ARG;
+  return op_convert(dst, dst_prec, src, src_prec, n, S(stream));
+}
+
+int sns_fft3d_many(void* const* fields, int nfields, int64_t nx, int64_t ny, int64_t nz,
+                   int dir, int flags, int prec, void* stream) {
+  if (!check_prec(prec) || !check_dims(nx, ny, nz)) return ERR_ARG;
+  if (dir != 1 && dir != -1) {
+    set_error("sns_fft3d: dir must be -1 (forward) or +1 (inverse)");
+    return ERR_ARG;
+  }
+  if (flags & ~(SNS_FFT_NORMALISE | SNS_FFT_ZERO_NYQUIST)) {
+    set_error("sns_fft3d: unknown flags");
+    return ERR_ARG;
+  }
+  if (!fields || nfields < 1 || nfields > kMaxFields) {
+    set_error("sns_fft3d_many: 1..6 fields");
+    return ERR_ARG;
+  }
+  for (int i = 0; i < nfields; i++)
+    if (!nonnull(fields[i], "sns_fft3d")) return ERR_ARG;
+  int fl = 0;
+  if (flags & SNS_FFT_NORMALISE) fl |= PASS_SCALE;
+  if (flags & SNS_FFT_ZERO_NYQUIST) fl |= PASS_ZERO_NYQUIST;
+  return fft3d(fields, nfields, (int)nx, (int)ny, (int)nz, dir, fl, prec, S(stream));
+}
+
+int sns_fft3d(void* field, int64_t nx, int64_t ny, int64_t nz, int dir, int flags, int prec,
+              void* stream) {
+  void* f[1] = {field};
+  return sns_fft3d_many(f, 1, nx, ny, nz, dir, flags, prec, stream);
+}
+
+int sns_forward(void* field, int64_t nx, int64_t ny, int64_t nz, int prec, void* stream) {
+  return sns_fft3d(field, nx, ny, nz, -1, SNS_FFT_ZERO_NYQUIST, prec, stream);
+}
+int sns_inverse(void* field, int64_t nx, int64_t ny, int64_t nz, int prec, void* stream) {
+  return sns_fft3d(field, nx, ny, nz, +1, SNS_FFT_NORMALISE, prec, stream);
+}
+
+int sns_fft1d_many(void* data, int64_t n, int64_t stride, int64_t howmany, int64_t dist,
+                   int dir, int prec, void* stream) {
+  if (!check_prec(prec)) return ERR_ARG;
+  if (!nonnull(data, "sns_fft1d_many")) return ERR_ARG;
+  if (n < 1 || stride < 1 || howmany < 0 || dist < 0 || (dir != 1 && dir != -1)) {
+    set_error("sns_fft1d_many: bad arguments");
+    return ERR_ARG;
+  }
+  if (howmany == 0 || n == 1) return OK;
+  if (!line_supported(n)) {
+    set_error("sns_fft1d_many: n must be a power of two up to 4096");
+    return ERR_UNSUPPORTED;
+  }
+  LineGeo g{};
+  g.L = (int)n;
+  g.ps = stride;
+  g.nx = g.ny = g.nz = 1;
+  const int TPL = (int)(n >= 16 ? n / 16 : 1);
+  auto pow2_divisor = [](int64_t v, int cap) {
+    int d = 1;
+    while (d * 2 <= cap && v % (d * 2) == 0) d *= 2;
+    return d;
+  };
+  if (dist == 1 && stride > 1) {
+    g.W = pow2_divisor(howmany, std::min(prec == PREC_C128 ? 8 : 16, std::max(1, max_threads(prec) / TPL)));
+    g.G = 1;
+    g.gs = 0;
+    g.TA = howmany / g.W;
+    g.sa = g.W;
+  } else {
+    g.W = 1;
+    g.G = pow2_divisor(howmany, std::max(1, 256 / TPL));
+    g.gs = dist;
+    g.TA = howmany / g.G;
+    g.sa = dist * g.G;
+  }
+  g.TB = 1;
+  g.sb = 0;
+  FieldPtrs f{};
+  f.n = 1;
+  f.in[0] = f.out[0] = data;
+  return run_line_pass(g, f, dir, 0, 1.0, prec, S(stream));
+}
+
+#define SNS_DIMS_ARGS(nx, ny, nz) Dims{(int)(nx), (int)(ny), (int)(nz)}
+
+int sns_zero_high_modes(void* field, int64_t nx, int64_t ny, int64_t nz, int prec, void* stream) {
+  if (!check_prec(prec) || !check_dims(nx, ny, nz) || !nonnull(field, "sns_zero_high_modes"))
+    return ERR_ARG;
+  return op_zero_high_modes(field, SNS_DIMS_ARGS(nx, ny, nz), prec, S(stream));
+}
+
+int sns_gradient(const void* f, void* gx, void* gy, void* gz, int64_t nx, int64_t ny, int64_t nz,
+                 int prec, void* stream) {
+  if (!check_prec(prec) || !check_dims(nx, ny, nz)) return ERR_ARG;
+  if (!nonnull(f, "sns_gradient") || !nonnull(gx, "sns_gradient") ||
+      !nonnull(gy, "sns_gradient") || !nonnull(gz, "sns_gradient"))
+    return ERR_ARG;
+  return op_gradient(f, gx, gy, gz, SNS_DIMS_ARGS(nx, ny, nz), prec, S(stream));
+}
+
+int sns_laplacian(const void* f, void* out, int64_t nx, int64_t ny, int64_t nz, int prec,
+                  void* stream) {
+  if (!check_prec(prec) || !check_dims(nx, ny, nz)) return ERR_ARG;
+  if (!nonnull(f, "sns_laplacian") || !nonnull(out, "sns_laplacian")) return ERR_ARG;
+  return op_laplacian(f, out, SNS_DIMS_ARGS(nx, ny, nz), prec, S(stream));
+}
+
+int sns_laplacian_inverse(void* f, double a, double b, int64_t nx, int64_t ny, int64_t nz,
+                          int prec, void* stream) {
+  if (!check_prec(prec) || !check_dims(nx, ny, nz) || !nonnull(f, "sns_laplacian_inverse"))
+    return ERR_ARG;
+  return op_laplacian_inverse(f, a, b, SNS_DIMS_ARGS(nx, ny, nz), prec, S(stream));
+}
+
+static bool vec_ok(const void* const v[3], const char* what) {
+  if (!v) {
+    set_error(std::string(what) + ": null vector");
+    return false;
+  }
+  for (int d = 0; d < 3; d++)
+    if (!nonnull(v[d], what)) return false;
+  return true;
+}
+
+int sns_curl(const void* const v[3], void* const out[3], int64_t nx, int64_t ny, int64_t nz,
+             int prec, void* stream) {
+  if (!check_prec(prec) || !check_dims(nx, ny, nz) || !vec_ok(v, "sns_curl") ||
+      !vec_ok((const void* const*)out, "sns_curl"))
+    return ERR_ARG;
+  return op_curl(v, out, SNS_DIMS_ARGS(nx, ny, nz), prec, S(stream));
+}
+
+int sns_divergence(const void* const v[3], void* out, int64_t nx, int64_t ny, int64_t nz,
+                   int prec, void* stream) {
+  if (!check_prec(prec) || !check_dims(nx, ny, nz) || !vec_ok(v, "sns_divergence") ||
+      !nonnull(out, "sns_divergence"))
+    return ERR_ARG;
+  return op_divergence(v, out, SNS_DIMS_ARGS(nx, ny, nz), prec, S(stream));
+}
+
+int sns_vector_laplacian(const void* const v[3], void* const out[3], int64_t nx, int64_t ny,
+                         int64_t nz, int prec, void* stream) {
+  if (!check_prec(prec) || !check_dims(nx, ny, nz) || !vec_ok(v, "sns_vector_laplacian") ||
+      !vec_ok((const void* const*)out, "sns_vector_laplacian"))
+    return ERR_ARG;
+  return op_vlaplacian(v, out, SNS_DIMS_ARGS(nx, ny, nz), prec, S(stream));
+}
+
+int sns_cross(const void* const a[3], const void* const b[3], void* const out[3], int64_t nx,
+              int64_t ny, int64_t nz, int prec, void* stream) {
+  if (!check_prec(prec) || !check_dims(nx, ny, nz) || !vec_ok(a, "sns_cross") ||
+      !vec_ok(b, "sns_cross") || !vec_ok((const void* const*)out, "sns_cross"))
+    return ERR_ARG;
+  if (!line_supported(nx) || !line_supported(ny) || !line_supported(nz)) {
+    set_error("sns_cross: dimensions must be powers of two up to 4096");
+    return ERR_UNSUPPORTED;
+  }
+  const Dims d = SNS_DIMS_ARGS(nx, ny, nz);
+  void* scratch[6] = {nullptr};
+  int rc = OK;
+  for (int i = 0; i < 6 && rc == OK; i++) rc = pool_malloc(&scratch[i], esize(prec) * d.n());
+  if (rc == OK) rc = vector_cross(a, b, out, d, prec, scratch, S(stream));
+  for (int i = 0; i < 6; i++) pool_free(scratch[i]);
+  return rc;
+}
+
+int sns_average_abs(const void* f, int64_t n, int prec, double* out, void* stream) {
+  if (!check_prec(prec) || !nonnull(f, "sns_average_abs") || !nonnull(out, "sns_average_abs"))
+    return ERR_ARG;
+  void* part = nullptr;
+  int rc = pool_malloc(&part, sizeof(double) * reduce_partials_count());
+  if (rc) return rc;
+  rc = op_average_abs(f, n, prec, (double*)part, out, S(stream));
+  pool_free(part);
+  return rc;
+}
+
+int sns_axpby(double alpha, const void* x, double beta, const void* y, void* out, int64_t n,
+              int prec, void* stream) {
+  if (!check_prec(prec) || !nonnull(x, "sns_axpby") || !nonnull(out, "sns_axpby")) return ERR_ARG;
+  if (n < 0) {
+    set_error("sns_axpby: negative count");
+    return ERR_ARG;
+  }
+  if (n == 0) return OK;
+  return op_axpby(alpha, x, beta, y, out, n, prec, S(stream));
+}
+
+int sns_mul(const void* a, const void* b, void* out, int64_t n, int prec, void* stream) {
+  if (!check_prec(prec) || !nonnull(a, "sns_mul") || !nonnull(b, "sns_mul") ||
+      !nonnull(out, "sns_mul"))
+    return ERR_ARG;
+  if (n < 0) {
+    set_error("sns_mul: negative count");
+    return ERR_ARG;
+  }
+  if (n == 0) return OK;
+  return op_mul(a, b, out, n, prec, S(stream));
+}
+
+// ---- fused stepper -------------------------------------------------------------
+int sns_ns_create(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double nu, double dt,
+                  int prec, void* stream) {
+  if (!nonnull(handle, "sns_ns_create")) return ERR_ARG;
+  *handle = nullptr;
+  if (!check_prec(prec) || !check_dims(nx, ny, nz)) return ERR_ARG;
+  sns_ns* h = new sns_ns();
+  int rc = ns_plan(h->pl, (int)nx, (int)ny, (int)nz, prec);
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  h->nu = nu;
+  h->dt = dt;
+  h->s = S(stream);
+  const size_t bytes = esize(prec) * (size_t)nx * ny * nz;
+  void** all[12];
+  for (int d = 0; d < 3; d++) {
+    all[d] = &h->V[d];
+    all[3 + d] = &h->C0[d];
+  }
+  for (int i = 0; i < 6; i++) all[6 + i] = &h->U[i];
+  for (int i = 0; i < 12 && rc == OK; i++) rc = pool_malloc(all[i], bytes);
+  if (rc == OK) rc = pool_malloc((void**)&h->stats_part, sizeof(double) * 4 * h->pl.update_blocks);
+  if (rc == OK) rc = pool_malloc((void**)&h->stats_out, sizeof(double) * 4);
+  if (rc == OK) {
+    for (int i = 0; i < 6 && rc == OK; i++)
+      rc = cuda_status(cudaMemsetAsync(*all[i], 0, bytes, h->s), "sns_ns_create");
+  }
+  if (rc) {
+    sns_ns_destroy(h);
+    return rc;
+  }
+  h->stepped = false;
+  *handle = h;
+  return OK;
+}
+
+int sns_ns_destroy(sns_ns* h) {
+  if (!h) return OK;
+  cudaStreamSynchronize(h->s);
+  for (int d = 0; d < 3; d++) {
+    pool_free(h->V[d]);
+    pool_free(h->C0[d]);
+  }
+  for (int i = 0; i < 6; i++) pool_free(h->U[i]);
+  pool_free(h->stats_part);
+  pool_free(h->stats_out);
+  for (cudaEvent_t e : h->events) cudaEventDestroy(e);
+  delete h;
+  return OK;
+}
+
+int sns_ns_set_state(sns_ns* h, const void* const V1[3], const void* const cross0[3]) {
+  if (!nonnull(h, "sns_ns_set_state") || !vec_ok(V1, "sns_ns_set_state") ||
+      !vec_ok(cross0, "sns_ns_set_state"))
+    return ERR_ARG;
+  const size_t bytes = esize(h->pl.prec) * (size_t)h->pl.nx * h->pl.ny * h->pl.nz;
+  int rc;
+  for (int d = 0; d < 3; d++) {
+    if ((rc = cuda_status(cudaMemcpyAsync(h->V[d], V1[d], bytes, cudaMemcpyDeviceToDevice, h->s),
+                          "sns_ns_set_state")))
+      return rc;
+    if ((rc = cuda_status(
+             cudaMemcpyAsync(h->C0[d], cross0[d], bytes, cudaMemcpyDeviceToDevice, h->s),
+             "sns_ns_set_state")))
+      return rc;
+  }
+  h->stepped = false;
+  return OK;
+}
+
+int sns_ns_bootstrap(sns_ns* h, const void* const V0[3], const void* const omega0[3]) {
+  if (!nonnull(h, "sns_ns_bootstrap") || !vec_ok(V0, "sns_ns_bootstrap") ||
+      !vec_ok(omega0, "sns_ns_bootstrap"))
+    return ERR_ARG;
+  const Dims d{h->pl.nx, h->pl.ny, h->pl.nz};
+  const int prec = h->pl.prec;
+  const int64_t n = d.n();
+  int rc;
+  // cross0 = V0 x omega0 (ns.cpp:133, 137, 153)
+  if ((rc = vector_cross(V0, omega0, h->C0, d, prec, h->U, h->s))) return rc;
+  // t = cross0 + nu * laplacian(V0), held in V
+  if ((rc = op_vlaplacian(V0, h->V, d, prec, h->s))) return rc;
+  for (int i = 0; i < 3; i++) {
+    if ((rc = op_axpby(h->nu, h->V[i], 0.0, nullptr, h->V[i], n, prec, h->s))) return rc;
+    if ((rc = op_axpby(1.0, h->C0[i], 1.0, h->V[i], h->V[i], n, prec, h->s))) return rc;
+  }
+  // Pi0 = ilap(div t) (ns.cpp:133-134) in U[0]; grad Pi0 in U[1..3]
+  const void* t[3] = {h->V[0], h->V[1], h->V[2]};
+  if ((rc = op_divergence(t, h->U[0], d, prec, h->s))) return rc;
+  if ((rc = op_laplacian_inverse(h->U[0], 0.0, 1.0, d, prec, h->s))) return rc;
+  if ((rc = op_gradient(h->U[0], h->U[1], h->U[2], h->U[3], d, prec, h->s))) return rc;
+  // V1 = V0 + K (t - grad Pi0)  (ns.cpp:137)
+  for (int i = 0; i < 3; i++) {
+    if ((rc = op_axpby(1.0, h->V[i], -1.0, h->U[1 + i], h->V[i], n, prec, h->s))) return rc;
+    if ((rc = op_axpby(1.0, V0[i], h->dt, h->V[i], h->V[i], n, prec, h->s))) return rc;
+  }
+  h->stepped = false;
+  return OK;
+}
+
+int sns_ns_step(sns_ns* h, int nsteps) {
+  if (!nonnull(h, "sns_ns_step")) return ERR_ARG;
+  if (nsteps < 0) {
+    set_error("sns_ns_step: negative step count");
+    return ERR_ARG;
+  }
+  for (int t = 0; t < nsteps; t++) {
+    cudaEvent_t* ev = nullptr;
+    if (h->profiling) {
+      const size_t need = (size_t)(h->recorded + 1) * (kNSPasses + 1);
+      while (h->events.size() < need) {
+        cudaEvent_t e;
+        int rc = cuda_status(cudaEventCreate(&e), "sns_ns_step(profile)");
+        if (rc) return rc;
+        h->events.push_back(e);
+      }
+      ev = &h->events[(size_t)h->recorded * (kNSPasses + 1)];
+    }
+    int rc = ns_step_once(h->pl, h->V, h->C0, h->U, h->stats_part, h->nu, h->dt, h->s, ev);
+    if (rc) return rc;
+    if (ev) h->recorded++;
+    h->stepped = true;
+  }
+  return OK;
+}
+
+int sns_ns_profile(sns_ns* h, int enable) {
+  if (!nonnull(h, "sns_ns_profile")) return ERR_ARG;
+  h->profiling = enable != 0;
+  h->recorded = 0;
+  return OK;
+}
+
+int sns_ns_pass_times(sns_ns* h, double* total_ms, int* launches, int max) {
+  if (!nonnull(h, "sns_ns_pass_times") || !nonnull(total_ms, "sns_ns_pass_times") ||
+      !nonnull(launches, "sns_ns_pass_times") || max < 0)
+    return ERR_ARG;
+  int rc = cuda_status(cudaStreamSynchronize(h->s), "sns_ns_pass_times");
+  if (rc) return rc;
+  for (int p = 0; p < max; p++) {
+    total_ms[p] = 0;
+    launches[p] = 0;
+  }
+  for (int t = 0; t < h->recorded; t++) {
+    cudaEvent_t* ev = &h->events[(size_t)t * (kNSPasses + 1)];
+    for (int p = 0; p < kNSPasses && p < max; p++) {
+      float ms = 0;
+      if ((rc = cuda_status(cudaEventElapsedTime(&ms, ev[p], ev[p + 1]), "sns_ns_pass_times")))
+        return rc;
+      total_ms[p] += ms;
+      launches[p] += 1;
+    }
+  }
+  return kNSPasses;
+}
+
+int sns_ns_get_state(sns_ns* h, void* const V1[3], void* const omega1[3], void* const cross0[3]) {
+  if (!nonnull(h, "sns_ns_get_state")) return ERR_ARG;
+  const Dims d{h->pl.nx, h->pl.ny, h->pl.nz};
+  const size_t bytes = esize(h->pl.prec) * (size_t)d.n();
+  int rc;
+  for (int i = 0; i < 3; i++) {
+    if (V1 && V1[i] &&
+        (rc = cuda_status(cudaMemcpyAsync(V1[i], h->V[i], bytes, cudaMemcpyDeviceToDevice, h->s),
+                          "sns_ns_get_state")))
+      return rc;
+    if (cross0 && cross0[i] &&
+        (rc = cuda_status(
+             cudaMemcpyAsync(cross0[i], h->C0[i], bytes, cudaMemcpyDeviceToDevice, h->s),
+             "sns_ns_get_state")))
+      return rc;
+  }
+  if (omega1) {
+    if (!vec_ok((const void* const*)omega1, "sns_ns_get_state")) return ERR_ARG;
+    const void* v[3] = {h->V[0], h->V[1], h->V[2]};
+    if ((rc = op_curl(v, omega1, d, h->pl.prec, h->s))) return rc;
+  }
+  return OK;
+}
+
+int sns_ns_stats(sns_ns* h, double* div_avg, double* energy, double* enstrophy, double* max_div) {
+  if (!nonnull(h, "sns_ns_stats")) return ERR_ARG;
+  if (!h->stepped) {
+    set_error("sns_ns_stats: no step has run since the state was set");
+    return ERR_ARG;
+  }
+  int rc = ns_stats_final(h->pl, h->stats_part, h->stats_out, h->s);
+  if (rc) return rc;
+  double v[4];
+  if ((rc = cuda_status(cudaMemcpyAsync(v, h->stats_out, sizeof(v), cudaMemcpyDeviceToHost, h->s),
+                        "sns_ns_stats")))
+    return rc;
+  if ((rc = cuda_status(cudaStreamSynchronize(h->s), "sns_ns_stats"))) return rc;
+  const double N = (double)h->pl.nx * h->pl.ny * h->pl.nz;
+  if (div_avg) *div_avg = v[0] / N;
+  if (energy) *energy = 0.5 * v[1] / (N * N);
+  if (enstrophy) *enstrophy = 0.5 * v[2] / (N * N);
+  if (max_div) *max_div = v[3];
+  return OK;
+}
+
+int sns_ns_launches_per_step(sns_ns* h) {
+  (void)h;
+  return kNSPasses;
+}
+
+}  // extern "C"

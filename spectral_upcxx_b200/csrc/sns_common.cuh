@@ -1,0 +1,87 @@
+// Shared device helpers: complex types, error plumbing, grid sizing.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+namespace sns {
+
+// Precision codes of the C-ABI (spectral_b200.h): 0 = complex64, 1 = complex128.
+enum Prec : int { PREC_C64 = 0, PREC_C128 = 1 };
+
+template <typename T>
+struct cx;
+template <>
+struct cx<float> {
+  using type = float2;
+};
+template <>
+struct cx<double> {
+  using type = double2;
+};
+template <typename T>
+using cx_t = typename cx<T>::type;
+
+__device__ __forceinline__ float2 mk(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 mk(double a, double b) { return make_double2(a, b); }
+
+template <typename C>
+__device__ __forceinline__ C cadd(C a, C b) {
+  return mk(a.x + b.x, a.y + b.y);
+}
+template <typename C>
+__device__ __forceinline__ C csub(C a, C b) {
+  return mk(a.x - b.x, a.y - b.y);
+}
+template <typename C>
+__device__ __forceinline__ C cmul(C a, C b) {
+  return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// (0, k) * z, the product std::complex forms for i*k*z.
+template <typename C, typename T>
+__device__ __forceinline__ C ikmul(T k, C z) {
+  return mk(-k * z.y, k * z.x);
+}
+template <typename C, typename T>
+__device__ __forceinline__ C cscale(T s, C z) {
+  return mk(s * z.x, s * z.y);
+}
+
+// Largest CTA of the FFT kernels: FP64 lines need about twice the registers.
+template <typename T>
+struct MaxThreads {
+  static constexpr int value = sizeof(T) == 8 ? 512 : 768;
+};
+inline int max_threads(int prec) { return prec == PREC_C128 ? 512 : 768; }
+
+// Scalar::freq (src/Scalar.cpp:198-206): k = i for i <= n/2, else i - n.
+__device__ __forceinline__ int freq_i(int i, int n) { return (i <= (n >> 1)) ? i : i - n; }
+
+// Thread-local last-error string of the C-ABI.
+void set_error(const std::string& msg);
+const char* last_error();
+
+// Status codes of the C-ABI.
+enum Status : int {
+  OK = 0,
+  ERR_ARG = -1,
+  ERR_UNSUPPORTED = -2,
+  ERR_CUDA = -3,
+  ERR_ALLOC = -4,
+  ERR_TIMEOUT = -5,
+};
+
+int cuda_status(cudaError_t e, const char* where);
+
+// Number of SMs of the current device (cached).
+int sm_count();
+
+}  // namespace sns
+
+#define SNS_CHECK_LAUNCH(where)                                    \
+  do {                                                             \
+    cudaError_t _e = cudaGetLastError();                           \
+    if (_e != cudaSuccess) return ::sns::cuda_status(_e, where);   \
+  } while (0)

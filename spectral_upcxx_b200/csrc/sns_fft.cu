@@ -1,0 +1,364 @@
+// Batched line-FFT passes: the replacement for FFT1D's per-line FFTW calls
+// (src/FFT1D.cpp:95-101) and for the three 1D phases of Scalar::transform
+// (src/Scalar.cpp:419-566).  One kernel launch transforms every line along
+// one axis of up to six fields.  A CTA owns a tile of W adjacent lines x G
+// groups: it loads the tile with unit-stride (coalesced) global reads into
+// padded shared-memory rows, runs the register/shared Stockham line FFT, and
+// stores the tile back with the epilogue (1/N scaling, Nyquist zeroing)
+// applied.  Tiles are disjoint, so passes run in place; the reference's
+// transpose buffer (`tmp`, src/Scalar.cpp:113-122) is not needed.
+#include <math.h>
+
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "sns_fft.cuh"
+#include "sns_fft_core.cuh"
+
+namespace sns {
+
+bool is_pow2(int64_t n) { return n >= 1 && (n & (n - 1)) == 0; }
+bool line_supported(int64_t L) { return L == 1 || (is_pow2(L) && L <= kMaxLine); }
+
+// cos/sin(2 pi m / n) in FP64 with reduction of the angle to the first octant.
+static void cis_octant(int64_t m, int64_t n, double* c, double* s) {
+  m %= n;
+  if (m < 0) m += n;
+  const int64_t m8 = 8 * m;
+  const int64_t oct = m8 / n;
+  const int64_t rem = m8 - oct * n;
+  const double t = (oct & 1) ? (M_PI / 4) * ((double)(n - rem) / (double)n)
+                             : (M_PI / 4) * ((double)rem / (double)n);
+  const double ct = cos(t), st = sin(t);
+  double x, y;
+  switch (oct) {
+    case 0: x = ct; y = st; break;
+    case 1: x = st; y = ct; break;
+    case 2: x = -st; y = ct; break;
+    case 3: x = -ct; y = st; break;
+    case 4: x = -ct; y = -st; break;
+    case 5: x = -st; y = -ct; break;
+    case 6: x = st; y = -ct; break;
+    default: x = ct; y = -st; break;
+  }
+  *c = x;
+  *s = y;
+}
+
+const void* twiddles(int L, int prec) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int>, void*> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  auto key = std::make_tuple(dev, L, prec);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  std::vector<double> tab(2 * (size_t)L);
+  for (int m = 0; m < L; m++) {
+    double c, s;
+    cis_octant(m, L, &c, &s);
+    tab[2 * m] = c;
+    tab[2 * m + 1] = -s;  // exp(-i 2 pi m / L)
+  }
+  void* d = nullptr;
+  size_t bytes;
+  if (prec == PREC_C128) {
+    bytes = sizeof(double) * tab.size();
+    if (cudaMalloc(&d, bytes) != cudaSuccess) return nullptr;
+    cudaMemcpy(d, tab.data(), bytes, cudaMemcpyHostToDevice);
+  } else {
+    std::vector<float> f(tab.size());
+    for (size_t i = 0; i < tab.size(); i++) f[i] = (float)tab[i];
+    bytes = sizeof(float) * f.size();
+    if (cudaMalloc(&d, bytes) != cudaSuccess) return nullptr;
+    cudaMemcpy(d, f.data(), bytes, cudaMemcpyHostToDevice);
+  }
+  cache[key] = d;
+  return d;
+}
+
+// Element idx of field `field` as the prologue forms it.
+template <int PRO, typename C>
+__device__ __forceinline__ C pro_load(const FieldPtrs& f, int field, int64_t idx,
+                                      const LineGeo& geo) {
+  if constexpr (PRO == PRO_CURL6) {
+    if (field < 3) return reinterpret_cast<const C*>(f.in[field])[idx];
+    const int64_t nxy = (int64_t)geo.nx * geo.ny;
+    const int z = (int)(idx / nxy);
+    const int64_t r = idx - (int64_t)z * nxy;
+    const int y = (int)(r / geo.nx);
+    const int x = (int)(r - (int64_t)y * geo.nx);
+    using T = decltype(C().x);
+    const T kx = (T)freq_i(x, geo.nx), ky = (T)freq_i(y, geo.ny), kz = (T)freq_i(z, geo.nz);
+    const C* v0 = reinterpret_cast<const C*>(f.in[0]);
+    const C* v1 = reinterpret_cast<const C*>(f.in[1]);
+    const C* v2 = reinterpret_cast<const C*>(f.in[2]);
+    if (field == 3) return csub(ikmul(ky, v2[idx]), ikmul(kz, v1[idx]));
+    if (field == 4) return csub(ikmul(kz, v0[idx]), ikmul(kx, v2[idx]));
+    return csub(ikmul(kx, v1[idx]), ikmul(ky, v0[idx]));
+  } else {
+    return reinterpret_cast<const C*>(f.in[field])[idx];
+  }
+}
+
+template <typename T, int L, int PRO>
+__global__ void __launch_bounds__(MaxThreads<T>::value)
+    k_line_pass(const LineGeo geo, const FieldPtrs f, const cx_t<T>* __restrict__ tw, T sg,
+                T scale, int flags, int wshift) {
+  using C = cx_t<T>;
+  using P = LinePlan<L>;
+  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(L);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sm = reinterpret_cast<C*>(smem_raw);
+
+  const int nf = f.n;
+  const int field = blockIdx.x % nf;
+  const int64_t t = blockIdx.x / nf;
+  C* __restrict__ dst = reinterpret_cast<C*>(f.out[field]);
+  const int64_t base = (t % geo.TA) * geo.sa + (t / geo.TA) * geo.sb;
+  const int W = geo.W;
+  const int total = (W * geo.G) * L;
+
+  // coalesced tile load: consecutive threads walk the unit-stride index
+  for (int q = threadIdx.x; q < total; q += blockDim.x) {
+    const int w = q & (W - 1);
+    const int rest = q >> wshift;
+    const int p = rest & (L - 1);
+    const int g = rest / L;
+    const int64_t idx = base + w + g * geo.gs + (int64_t)p * geo.ps;
+    sm[(w + W * g) * RS + pad_pos(p)] = pro_load<PRO, C>(f, field, idx, geo);
+  }
+  __syncthreads();
+
+  const int j = threadIdx.x % TPL;
+  const int line = threadIdx.x / TPL;
+  C* row = sm + line * RS;
+  C v[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
+  line_sync<TPL>();
+  line_fft<L>(v, row, j, tw, sg);
+#pragma unroll
+  for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
+  __syncthreads();
+
+  const bool do_scale = flags & PASS_SCALE;
+  const bool do_zero = flags & PASS_ZERO_NYQUIST;
+  const int64_t nxy = (int64_t)geo.nx * geo.ny;
+  for (int q = threadIdx.x; q < total; q += blockDim.x) {
+    const int w = q & (W - 1);
+    const int rest = q >> wshift;
+    const int p = rest & (L - 1);
+    const int g = rest / L;
+    const int64_t idx = base + w + g * geo.gs + (int64_t)p * geo.ps;
+    C val = sm[(w + W * g) * RS + pad_pos(p)];
+    if (do_scale) val = cscale(scale, val);
+    if (do_zero) {
+      const int64_t z = idx / nxy;
+      const int64_t r = idx - z * nxy;
+      const int64_t y = r / geo.nx;
+      const int64_t x = r - y * geo.nx;
+      if (x == (geo.nx >> 1) || y == (geo.ny >> 1) || z == (geo.nz >> 1)) val = mk((T)0, (T)0);
+    }
+    dst[idx] = val;
+  }
+}
+
+// epilogue-only pass (used when every axis has length 1)
+template <typename T>
+__global__ void k_scale_zero(const FieldPtrs f, int64_t n, int nx, int ny, int nz, T scale,
+                             int flags) {
+  using C = cx_t<T>;
+  const int field = blockIdx.y;
+  C* d = reinterpret_cast<C*>(f.out[field]);
+  const C* s = reinterpret_cast<const C*>(f.in[field]);
+  const int64_t nxy = (int64_t)nx * ny;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    C v = s[i];
+    if (flags & PASS_SCALE) v = cscale(scale, v);
+    if (flags & PASS_ZERO_NYQUIST) {
+      int64_t z = i / nxy, r = i - z * nxy, y = r / nx, x = r - y * nx;
+      if (x == (nx >> 1) || y == (ny >> 1) || z == (nz >> 1)) v = mk((T)0, (T)0);
+    }
+    d[i] = v;
+  }
+}
+
+template <typename T, int L, int PRO>
+static int launch_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags,
+                       double scale, cudaStream_t stream) {
+  using C = cx_t<T>;
+  constexpr int TPL = LinePlan<L>::TPL;
+  const int lines = geo.W * geo.G;
+  const int threads = lines * TPL;
+  const size_t smem = (size_t)lines * row_stride(L) * sizeof(C);
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63]) {
+    cudaError_t e = cudaFuncSetAttribute(k_line_pass<T, L, PRO>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_line_pass)");
+    attr_set[dev & 63] = true;
+  }
+  const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
+  if (!tw) {
+    set_error("twiddle table allocation failed");
+    return ERR_ALLOC;
+  }
+  int wshift = 0;
+  while ((1 << wshift) < geo.W) wshift++;
+  const int64_t blocks = geo.TA * geo.TB * f.n;
+  if (blocks > 0x7fffffff) {
+    set_error("line pass: grid too large");
+    return ERR_UNSUPPORTED;
+  }
+  k_line_pass<T, L, PRO><<<(unsigned)blocks, threads, smem, stream>>>(geo, f, tw, (T)sign, (T)scale,
+                                                                 flags, wshift);
+  SNS_CHECK_LAUNCH("k_line_pass");
+  return OK;
+}
+
+template <typename T, int PRO>
+static int dispatch_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags,
+                         double scale, cudaStream_t stream) {
+  switch (geo.L) {
+    case 2: return launch_pass<T, 2, PRO>(geo, f, sign, flags, scale, stream);
+    case 4: return launch_pass<T, 4, PRO>(geo, f, sign, flags, scale, stream);
+    case 8: return launch_pass<T, 8, PRO>(geo, f, sign, flags, scale, stream);
+    case 16: return launch_pass<T, 16, PRO>(geo, f, sign, flags, scale, stream);
+    case 32: return launch_pass<T, 32, PRO>(geo, f, sign, flags, scale, stream);
+    case 64: return launch_pass<T, 64, PRO>(geo, f, sign, flags, scale, stream);
+    case 128: return launch_pass<T, 128, PRO>(geo, f, sign, flags, scale, stream);
+    case 256: return launch_pass<T, 256, PRO>(geo, f, sign, flags, scale, stream);
+    case 512: return launch_pass<T, 512, PRO>(geo, f, sign, flags, scale, stream);
+    case 1024: return launch_pass<T, 1024, PRO>(geo, f, sign, flags, scale, stream);
+    case 2048: return launch_pass<T, 2048, PRO>(geo, f, sign, flags, scale, stream);
+    case 4096: return launch_pass<T, 4096, PRO>(geo, f, sign, flags, scale, stream);
+    default:
+      set_error("line length " + std::to_string(geo.L) +
+                " is not supported (powers of two up to 4096)");
+      return ERR_UNSUPPORTED;
+  }
+}
+
+int run_line_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags, double scale,
+                  int prec, cudaStream_t stream, int prologue) {
+  if (f.n < 1 || f.n > kMaxFields) {
+    set_error("line pass: 1..6 fields");
+    return ERR_ARG;
+  }
+  if (geo.TA * geo.TB == 0) return OK;
+  if (prologue == PRO_CURL6) {
+    if (f.n != 6) {
+      set_error("curl prologue needs six output fields");
+      return ERR_ARG;
+    }
+    if (prec == PREC_C128)
+      return dispatch_pass<double, PRO_CURL6>(geo, f, sign, flags, scale, stream);
+    return dispatch_pass<float, PRO_CURL6>(geo, f, sign, flags, scale, stream);
+  }
+  if (prec == PREC_C128) return dispatch_pass<double, PRO_LOAD>(geo, f, sign, flags, scale, stream);
+  return dispatch_pass<float, PRO_LOAD>(geo, f, sign, flags, scale, stream);
+}
+
+static int elems_per_thread(int L) { return L >= 16 ? 16 : L; }
+
+// Choose W adjacent lines and G groups for a pass of line length L.
+static void choose_tile(LineGeo& g, int64_t adjacent, int64_t groups, int prec) {
+  const int TPL = g.L / elems_per_thread(g.L);
+  const size_t esz = prec == PREC_C128 ? 16 : 8;
+  const size_t smem_cap = 200 * 1024;
+  int W = 1;
+  const int Wmax = prec == PREC_C128 ? 8 : 16;  // 128-byte runs
+  while (W * 2 <= Wmax && adjacent % (W * 2) == 0 && W * 2 * TPL <= max_threads(prec) &&
+         (size_t)(W * 2) * row_stride(g.L) * esz <= smem_cap)
+    W *= 2;
+  int G = 1;
+  while (W * G * 2 * TPL <= 256 && groups % (G * 2) == 0 &&
+         (size_t)(W * G * 2) * row_stride(g.L) * esz <= smem_cap / 2)
+    G *= 2;
+  g.W = W;
+  g.G = G;
+}
+
+LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec) {
+  LineGeo g{};
+  g.nx = nx;
+  g.ny = ny;
+  g.nz = nz;
+  const int64_t nxy = (int64_t)nx * ny;
+  if (axis == 0) {
+    g.L = nx;
+    g.ps = 1;
+    g.gs = nx;
+    choose_tile(g, 1, (int64_t)ny * nz, prec);
+    g.TA = (int64_t)ny * nz / g.G;
+    g.TB = 1;
+    g.sa = (int64_t)g.G * nx;
+    g.sb = 0;
+  } else if (axis == 1) {
+    g.L = ny;
+    g.ps = nx;
+    g.gs = nxy;
+    choose_tile(g, nx, nz, prec);
+    g.TA = nx / g.W;
+    g.TB = nz / g.G;
+    g.sa = g.W;
+    g.sb = (int64_t)g.G * nxy;
+  } else {
+    g.L = nz;
+    g.ps = nxy;
+    g.gs = nx;
+    choose_tile(g, nx, ny, prec);
+    g.TA = nx / g.W;
+    g.TB = ny / g.G;
+    g.sa = g.W;
+    g.sb = (int64_t)g.G * nx;
+  }
+  return g;
+}
+
+int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int flags, int prec,
+          cudaStream_t stream) {
+  if (nx < 1 || ny < 1 || nz < 1 || nf < 1 || nf > kMaxFields) {
+    set_error("fft3d: bad dimensions or field count");
+    return ERR_ARG;
+  }
+  if (!line_supported(nx) || !line_supported(ny) || !line_supported(nz)) {
+    set_error("fft3d: dimensions must be powers of two up to 4096");
+    return ERR_UNSUPPORTED;
+  }
+  FieldPtrs f{};
+  f.n = nf;
+  for (int i = 0; i < nf; i++) f.in[i] = f.out[i] = fields[i];
+  const double N = (double)nx * ny * nz;
+  // axes of length 1 are identities; the epilogue rides on the last real pass
+  int axes[3], na = 0;
+  const int order_fwd[3] = {0, 1, 2}, order_inv[3] = {2, 1, 0};
+  const int* order = sign < 0 ? order_fwd : order_inv;
+  const int dims[3] = {nx, ny, nz};
+  for (int i = 0; i < 3; i++)
+    if (dims[order[i]] > 1) axes[na++] = order[i];
+  for (int i = 0; i < na; i++) {
+    LineGeo g = axis_geo(axes[i], nx, ny, nz, prec);
+    int fl = (i == na - 1) ? flags : 0;
+    int rc = run_line_pass(g, f, sign, fl, 1.0 / N, prec, stream);
+    if (rc) return rc;
+  }
+  if (na == 0 && flags) {
+    const int64_t n = (int64_t)nx * ny * nz;
+    dim3 grid((unsigned)((n + 255) / 256), nf);
+    if (prec == PREC_C128)
+      k_scale_zero<double><<<grid, 256, 0, stream>>>(f, n, nx, ny, nz, 1.0 / N, flags);
+    else
+      k_scale_zero<float><<<grid, 256, 0, stream>>>(f, n, nx, ny, nz, (float)(1.0 / N), flags);
+    SNS_CHECK_LAUNCH("k_scale_zero");
+  }
+  return OK;
+}
+
+}  // namespace sns

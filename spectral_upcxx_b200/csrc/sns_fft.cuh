@@ -1,0 +1,67 @@
+// Batched line-FFT passes over device fields (host interface).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "sns_common.cuh"
+
+namespace sns {
+
+constexpr int kMaxFields = 6;
+constexpr int kMaxLine = 4096;
+
+// Epilogue flags of a pass.
+enum PassFlags : int {
+  PASS_SCALE = 1,         // multiply the output by `scale`
+  PASS_ZERO_NYQUIST = 2,  // zero outputs on the planes x=nx/2, y=ny/2, z=nz/2
+};
+
+// How a pass forms its input tile.
+enum PassPrologue : int {
+  PRO_LOAD = 0,   // field f reads in[f]
+  PRO_CURL6 = 1,  // in[0..2] = a Fourier vector V; fields 0..2 read V, fields
+                  // 3..5 form (i k x V) on the fly (src/Vector.cpp:92-122)
+};
+
+// Geometry of a batch of lines: element p of line (w, g) of tile t sits at
+//   base(t) + w + g*gs + p*ps,  base(t) = (t % TA)*sa + (t / TA)*sb.
+// W adjacent lines (unit stride) and G line groups form one tile.
+struct LineGeo {
+  int L;       // line length (power of two)
+  int W, G;    // adjacent lines and groups per tile
+  int64_t ps, gs;
+  int64_t TA, TB, sa, sb;
+  // field dimensions, used by the Nyquist epilogue to recover (x, y, z)
+  int nx, ny, nz;
+};
+
+struct FieldPtrs {
+  void* in[kMaxFields];
+  void* out[kMaxFields];
+  int n;
+};
+
+bool is_pow2(int64_t n);
+// Validate that the batched pass supports line length L.
+bool line_supported(int64_t L);
+
+// One transform pass along the lines of `geo` over `f.n` fields.
+// sign = -1 forward, +1 inverse.  In place when in == out.
+int run_line_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags, double scale,
+                  int prec, cudaStream_t stream, int prologue = PRO_LOAD);
+
+// Geometry of the lines along `axis` (0 = x, 1 = y, 2 = z) of nx*ny*nz fields.
+LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec);
+
+// Full 3D C2C transform of nf fields in place (the Scalar::transform
+// contract, src/Scalar.cpp:400-646), with optional fused Nyquist zeroing
+// (forward) and 1/N scaling (inverse).
+int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int flags,
+          int prec, cudaStream_t stream);
+
+// Device twiddle table exp(-2 pi i m / L), m < L, generated in FP64 on the
+// host and stored as complex64 or complex128 (cached per device).
+const void* twiddles(int L, int prec);
+
+}  // namespace sns

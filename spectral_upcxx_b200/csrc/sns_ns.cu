@@ -1,0 +1,473 @@
+// Fused pseudo-spectral Navier-Stokes step (exec/ns.cpp:167-217).
+//
+// State: V (Fourier velocity, 3 fields) and C0 (Fourier V x omega of the
+// previous step, 3 fields); work: U (6 fields).  One step is five passes:
+//
+//   K1  z-inverse of (V, i k x V): the curl is formed while the tile loads
+//       (ns.cpp:206 + Vector::cross's inverse copies, src/Vector.cpp:74-77)
+//   K2  y-inverse of the 6 fields
+//   K3  x-inverse, 1/N^2-scaled complex cross product u x omega, x-forward
+//       (src/Vector.cpp:79-89), 6 fields in, 3 out
+//   K4  y-forward of the 3 fields
+//   K5  z-forward + Nyquist zeroing (cross1 complete), then per mode the AB2 /
+//       projection / Crank-Nicolson update (ns.cpp:170-187) written over V,
+//       cross1 written over C0, FP64 diagnostics (ns.cpp:206-210)
+//
+// The reference runs 9 separate 3D FFTs plus ~25 eager field sweeps and 15
+// deep copies per step; here the history copies (ns.cpp:213-217) are
+// in-place updates and every intermediate lives in U.
+#include <math.h>
+
+#include <vector>
+
+#include "sns_fft.cuh"
+#include "sns_fft_core.cuh"
+#include "sns_ns.cuh"
+#include "sns_ops.cuh"
+
+namespace sns {
+
+// ---------------------------------------------------------------------------
+// K3: x lines -- inverse 6 fields, cross product, forward 3 fields.
+template <typename T, int L>
+__global__ void __launch_bounds__(MaxThreads<T>::value)
+    k_xcross(FieldPtrs f, const cx_t<T>* __restrict__ tw, int G, T scale2) {
+  using C = cx_t<T>;
+  using P = LinePlan<L>;
+  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(L);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sm = reinterpret_cast<C*>(smem_raw);
+  const int64_t row0 = (int64_t)blockIdx.x * G;
+  const int per = G * L;
+
+  for (int q = threadIdx.x; q < 6 * per; q += blockDim.x) {
+    const int fld = q / per, rem = q - fld * per, g = rem / L, p = rem & (L - 1);
+    sm[(fld * G + g) * RS + pad_pos(p)] =
+        reinterpret_cast<const C*>(f.in[fld])[(row0 + g) * L + p];
+  }
+  __syncthreads();
+
+  const int j = threadIdx.x % TPL, line = threadIdx.x / TPL;
+  C* row = sm + line * RS;
+  C v[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
+  line_sync<TPL>();
+  line_fft<L>(v, row, j, tw, (T)1);
+#pragma unroll
+  for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
+  __syncthreads();
+
+  // c = (u/N) x (omega/N): u in rows of fields 0..2, omega in 3..5
+  for (int q = threadIdx.x; q < per; q += blockDim.x) {
+    const int g = q / L, p = q & (L - 1);
+    C u[3], w[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      u[d] = sm[(d * G + g) * RS + pad_pos(p)];
+      w[d] = sm[((3 + d) * G + g) * RS + pad_pos(p)];
+    }
+    const C c0 = csub(cmul(u[1], w[2]), cmul(u[2], w[1]));
+    const C c1 = csub(cmul(u[2], w[0]), cmul(u[0], w[2]));
+    const C c2 = csub(cmul(u[0], w[1]), cmul(u[1], w[0]));
+    sm[(0 * G + g) * RS + pad_pos(p)] = cscale(scale2, c0);
+    sm[(1 * G + g) * RS + pad_pos(p)] = cscale(scale2, c1);
+    sm[(2 * G + g) * RS + pad_pos(p)] = cscale(scale2, c2);
+  }
+  __syncthreads();
+
+  // forward x on all rows (rows of fields 3..5 are discarded; keeping every
+  // thread on the same path keeps the block-wide syncs of long lines uniform)
+#pragma unroll
+  for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
+  line_sync<TPL>();
+  line_fft<L>(v, row, j, tw, (T)-1);
+#pragma unroll
+  for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
+  __syncthreads();
+
+  for (int q = threadIdx.x; q < 3 * per; q += blockDim.x) {
+    const int fld = q / per, rem = q - fld * per, g = rem / L, p = rem & (L - 1);
+    reinterpret_cast<C*>(f.out[fld])[(row0 + g) * L + p] = sm[(fld * G + g) * RS + pad_pos(p)];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K5: z lines -- forward 3 fields + Nyquist zeroing, then the AB2 /
+// projection / CN update per mode.
+struct UpdateArgs {
+  const void* U[3];  // cross1 after x, y forward passes
+  void* V[3];        // in: V1, out: V (new)
+  void* C0[3];       // in: cross0, out: cross1
+  int nx, ny, nz;
+  int W;
+  double hK;      // K/2
+  double nuhK;    // nu*K/2
+  double* stats;  // per block: sum|div|, sum|V|^2, sum|k x V|^2, max|div|
+};
+
+template <typename T, int L>
+__global__ void __launch_bounds__(MaxThreads<T>::value)
+    k_zfwd_update(const UpdateArgs a, const cx_t<T>* __restrict__ tw) {
+  using C = cx_t<T>;
+  using P = LinePlan<L>;
+  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(L);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sm = reinterpret_cast<C*>(smem_raw);
+  __shared__ double red[4][32];
+
+  const int W = a.W;
+  const int tiles_x = a.nx / W;
+  const int x0 = (blockIdx.x % tiles_x) * W;
+  const int y = blockIdx.x / tiles_x;
+  const int64_t nxy = (int64_t)a.nx * a.ny;
+  const int64_t base = x0 + (int64_t)a.nx * y;
+  const int per = W * L;
+
+  for (int q = threadIdx.x; q < 3 * per; q += blockDim.x) {
+    const int fld = q / per, rem = q - fld * per, w = rem % W, p = rem / W;
+    sm[(fld * W + w) * RS + pad_pos(p)] =
+        reinterpret_cast<const C*>(a.U[fld])[base + w + nxy * p];
+  }
+  __syncthreads();
+
+  const int j = threadIdx.x % TPL, line = threadIdx.x / TPL;
+  C* row = sm + line * RS;
+  C v[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
+  line_sync<TPL>();
+  line_fft<L>(v, row, j, tw, (T)-1);
+#pragma unroll
+  for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
+  __syncthreads();
+
+  const T hK = (T)a.hK, nuhK = (T)a.nuhK;
+  const T ky = (T)freq_i(y, a.ny);
+  const bool ynyq = (y == (a.ny >> 1));
+  double s_div = 0, s_e = 0, s_w = 0, m_div = 0;
+  for (int q = threadIdx.x; q < per; q += blockDim.x) {
+    const int w = q % W, z = q / W;
+    const int x = x0 + w;
+    const int64_t idx = base + w + nxy * z;
+    const T kx = (T)freq_i(x, a.nx), kz = (T)freq_i(z, a.nz);
+    const bool nyq = ynyq || x == (a.nx >> 1) || z == (a.nz >> 1);
+    C c1[3], V1[3], c0[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      c1[d] = nyq ? mk((T)0, (T)0) : sm[(d * W + w) * RS + pad_pos(z)];
+      V1[d] = reinterpret_cast<const C*>(a.V[d])[idx];
+      c0[d] = reinterpret_cast<const C*>(a.C0[d])[idx];
+    }
+    const T kk[3] = {kx, ky, kz};
+    const T k2 = kx * kx + ky * ky + kz * kz;
+    const double k2d = (double)kx * kx + (double)ky * ky + (double)kz * kz;
+    // F = K/2 (3 c1 - c0)                      (ns.cpp:171)
+    // lap1 = nu K/2 (-|k|^2 V1)                (ns.cpp:174)
+    // s = V1 + lap1 + F; G = div s / (-|k|^2)  (ns.cpp:177-178)
+    C F[3], lap[3], s[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      F[d] = cscale(hK, csub(cscale((T)3, c1[d]), c0[d]));
+      lap[d] = cscale(nuhK, cscale(-k2, V1[d]));
+      s[d] = cadd(cadd(V1[d], lap[d]), F[d]);
+    }
+    C G = cadd(cadd(ikmul(kx, s[0]), ikmul(ky, s[1])), ikmul(kz, s[2]));
+    double den_cn = 1.0;
+    if (k2d != 0.0) {
+      const double den = -k2d;
+      G = mk((T)((double)G.x / den), (T)((double)G.y / den));
+      den_cn = 1.0 + a.nuhK * k2d;
+    }
+    // Vhalf = V1 + F - grad G; V = (Vhalf + lap1) / (1 + nu K/2 |k|^2)  (ns.cpp:181-187)
+    C Vn[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      C vh = csub(cadd(V1[d], F[d]), ikmul(kk[d], G));
+      C vv = cadd(vh, lap[d]);
+      if (k2d != 0.0) vv = mk((T)((double)vv.x / den_cn), (T)((double)vv.y / den_cn));
+      Vn[d] = vv;
+      reinterpret_cast<C*>(a.V[d])[idx] = vv;
+      reinterpret_cast<C*>(a.C0[d])[idx] = c1[d];
+    }
+    // FP64 diagnostics of the new velocity
+    const C dv = cadd(cadd(ikmul(kx, Vn[0]), ikmul(ky, Vn[1])), ikmul(kz, Vn[2]));
+    const double ad = hypot((double)dv.x, (double)dv.y);
+    s_div += ad;
+    m_div = fmax(m_div, ad);
+    double e2 = 0, w2 = 0;
+#pragma unroll
+    for (int d = 0; d < 3; d++) e2 += (double)Vn[d].x * Vn[d].x + (double)Vn[d].y * Vn[d].y;
+    const C om0 = csub(ikmul(ky, Vn[2]), ikmul(kz, Vn[1]));
+    const C om1 = csub(ikmul(kz, Vn[0]), ikmul(kx, Vn[2]));
+    const C om2 = csub(ikmul(kx, Vn[1]), ikmul(ky, Vn[0]));
+    w2 = (double)om0.x * om0.x + (double)om0.y * om0.y + (double)om1.x * om1.x +
+         (double)om1.y * om1.y + (double)om2.x * om2.x + (double)om2.y * om2.y;
+    s_e += e2;
+    s_w += w2;
+  }
+  // block reduction of the diagnostics
+  for (int o = 16; o > 0; o >>= 1) {
+    s_div += __shfl_xor_sync(0xffffffffu, s_div, o);
+    s_e += __shfl_xor_sync(0xffffffffu, s_e, o);
+    s_w += __shfl_xor_sync(0xffffffffu, s_w, o);
+    m_div = fmax(m_div, __shfl_xor_sync(0xffffffffu, m_div, o));
+  }
+  const int warp = threadIdx.x >> 5, nwarps = (blockDim.x + 31) >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][warp] = s_div;
+    red[1][warp] = s_e;
+    red[2][warp] = s_w;
+    red[3][warp] = m_div;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+    for (int i = 0; i < nwarps; i++) {
+      t0 += red[0][i];
+      t1 += red[1][i];
+      t2 += red[2][i];
+      t3 = fmax(t3, red[3][i]);
+    }
+    double* out = a.stats + 4 * (int64_t)blockIdx.x;
+    out[0] = t0;
+    out[1] = t1;
+    out[2] = t2;
+    out[3] = t3;
+  }
+}
+
+__global__ void k_stats_final(const double* part, int blocks, double* out) {
+  __shared__ double sm[4][256];
+  double a = 0, b = 0, c = 0, m = 0;
+  for (int i = threadIdx.x; i < blocks; i += blockDim.x) {
+    a += part[4 * i];
+    b += part[4 * i + 1];
+    c += part[4 * i + 2];
+    m = fmax(m, part[4 * i + 3]);
+  }
+  sm[0][threadIdx.x] = a;
+  sm[1][threadIdx.x] = b;
+  sm[2][threadIdx.x] = c;
+  sm[3][threadIdx.x] = m;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sm[0][threadIdx.x] += sm[0][threadIdx.x + o];
+      sm[1][threadIdx.x] += sm[1][threadIdx.x + o];
+      sm[2][threadIdx.x] += sm[2][threadIdx.x + o];
+      sm[3][threadIdx.x] = fmax(sm[3][threadIdx.x], sm[3][threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 4; k++) out[k] = sm[k][0];
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+namespace {
+
+template <typename T, int L>
+int launch_xcross(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
+  using C = cx_t<T>;
+  constexpr int TPL = LinePlan<L>::TPL;
+  const int G = pl.xG;
+  const int threads = 6 * G * TPL;
+  const size_t smem = (size_t)6 * G * row_stride(L) * sizeof(C);
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr[dev & 63]) {
+    cudaError_t e = cudaFuncSetAttribute(k_xcross<T, L>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_xcross)");
+    attr[dev & 63] = true;
+  }
+  const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
+  const double N = (double)pl.nx * pl.ny * pl.nz;
+  const int blocks = (int)((int64_t)pl.ny * pl.nz / G);
+  k_xcross<T, L><<<blocks, threads, smem, s>>>(f, tw, G, (T)(1.0 / (N * N)));
+  SNS_CHECK_LAUNCH("k_xcross");
+  return OK;
+}
+
+template <typename T, int L>
+int launch_update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
+  using C = cx_t<T>;
+  constexpr int TPL = LinePlan<L>::TPL;
+  const int threads = 3 * a.W * TPL;
+  const size_t smem = (size_t)3 * a.W * row_stride(L) * sizeof(C);
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr[dev & 63]) {
+    cudaError_t e = cudaFuncSetAttribute(k_zfwd_update<T, L>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_zfwd_update)");
+    attr[dev & 63] = true;
+  }
+  const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
+  k_zfwd_update<T, L><<<pl.update_blocks, threads, smem, s>>>(a, tw);
+  SNS_CHECK_LAUNCH("k_zfwd_update");
+  return OK;
+}
+
+template <typename T, int L>
+int launch_xcross_dispatch(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
+  return launch_xcross<T, L>(pl, f, s);
+}
+
+template <typename T>
+int xcross(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
+  switch (pl.nx) {
+    case 4: return launch_xcross<T, 4>(pl, f, s);
+    case 8: return launch_xcross<T, 8>(pl, f, s);
+    case 16: return launch_xcross<T, 16>(pl, f, s);
+    case 32: return launch_xcross<T, 32>(pl, f, s);
+    case 64: return launch_xcross<T, 64>(pl, f, s);
+    case 128: return launch_xcross<T, 128>(pl, f, s);
+    case 256: return launch_xcross<T, 256>(pl, f, s);
+    case 512: return launch_xcross<T, 512>(pl, f, s);
+    case 1024: return launch_xcross<T, 1024>(pl, f, s);
+    default: set_error("fused NS step: nx must be a power of two in [4, 1024]"); return ERR_UNSUPPORTED;
+  }
+}
+
+template <typename T>
+int update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
+  switch (pl.nz) {
+    case 4: return launch_update<T, 4>(pl, a, s);
+    case 8: return launch_update<T, 8>(pl, a, s);
+    case 16: return launch_update<T, 16>(pl, a, s);
+    case 32: return launch_update<T, 32>(pl, a, s);
+    case 64: return launch_update<T, 64>(pl, a, s);
+    case 128: return launch_update<T, 128>(pl, a, s);
+    case 256: return launch_update<T, 256>(pl, a, s);
+    case 512: return launch_update<T, 512>(pl, a, s);
+    case 1024: return launch_update<T, 1024>(pl, a, s);
+    default: set_error("fused NS step: nz must be a power of two in [4, 1024]"); return ERR_UNSUPPORTED;
+  }
+}
+
+int elems(int L) { return L >= 16 ? 16 : L; }
+
+}  // namespace
+
+int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec) {
+  pl = NSPlan{};
+  pl.nx = nx;
+  pl.ny = ny;
+  pl.nz = nz;
+  pl.prec = prec;
+  for (int n : {nx, ny, nz})
+    if (!is_pow2(n) || n < 4 || n > 1024) {
+      set_error("fused NS step: dimensions must be powers of two in [4, 1024]");
+      return ERR_UNSUPPORTED;
+    }
+  const size_t esz = prec == PREC_C128 ? 16 : 8;
+  // K3 tile: G rows of all six fields
+  {
+    const int TPL = nx / elems(nx);
+    int G = 1;
+    while (6 * (G * 2) * TPL <= 384 && ((int64_t)ny * nz) % (G * 2) == 0 &&
+           (size_t)6 * G * 2 * row_stride(nx) * esz <= 110 * 1024)
+      G *= 2;
+    if (6 * G * TPL > max_threads(prec)) {
+      set_error("fused NS step: nx too large for the x-pass tile");
+      return ERR_UNSUPPORTED;
+    }
+    pl.xG = G;
+  }
+  // K5 tile: W adjacent z lines of three fields
+  {
+    const int TPL = nz / elems(nz);
+    int W = 1;
+    const int Wmax = prec == PREC_C128 ? 8 : 16;
+    while (W * 2 <= Wmax && nx % (W * 2) == 0 && 3 * (W * 2) * TPL <= max_threads(prec) &&
+           (size_t)3 * W * 2 * row_stride(nz) * esz <= 110 * 1024)
+      W *= 2;
+    pl.zW = W;
+    pl.update_blocks = (nx / W) * ny;
+  }
+  return OK;
+}
+
+int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* const U[6],
+                 double* stats, double nu, double dt, cudaStream_t s, cudaEvent_t* ev) {
+  const int nx = pl.nx, ny = pl.ny, nz = pl.nz, prec = pl.prec;
+  int rc;
+  int pass = 0;
+  auto mark = [&]() {
+    if (ev) cudaEventRecord(ev[pass], s);
+    pass++;
+  };
+  mark();
+  // K1: z-inverse of (V, i k x V)
+  {
+    FieldPtrs f{};
+    f.n = 6;
+    for (int d = 0; d < 3; d++) f.in[d] = V[d];
+    for (int i = 0; i < 6; i++) f.out[i] = U[i];
+    LineGeo g = axis_geo(2, nx, ny, nz, prec);
+    if ((rc = run_line_pass(g, f, +1, 0, 1.0, prec, s, PRO_CURL6))) return rc;
+    mark();
+  }
+  // K2: y-inverse of the six fields
+  {
+    FieldPtrs f{};
+    f.n = 6;
+    for (int i = 0; i < 6; i++) f.in[i] = f.out[i] = U[i];
+    LineGeo g = axis_geo(1, nx, ny, nz, prec);
+    if ((rc = run_line_pass(g, f, +1, 0, 1.0, prec, s))) return rc;
+    mark();
+  }
+  // K3: x-inverse, cross product, x-forward
+  {
+    FieldPtrs f{};
+    f.n = 6;
+    for (int i = 0; i < 6; i++) f.in[i] = U[i];
+    for (int i = 0; i < 3; i++) f.out[i] = U[i];
+    rc = prec == PREC_C128 ? xcross<double>(pl, f, s) : xcross<float>(pl, f, s);
+    if (rc) return rc;
+    mark();
+  }
+  // K4: y-forward of the cross product
+  {
+    FieldPtrs f{};
+    f.n = 3;
+    for (int i = 0; i < 3; i++) f.in[i] = f.out[i] = U[i];
+    LineGeo g = axis_geo(1, nx, ny, nz, prec);
+    if ((rc = run_line_pass(g, f, -1, 0, 1.0, prec, s))) return rc;
+    mark();
+  }
+  // K5: z-forward + Nyquist zeroing + AB2/projection/CN update
+  {
+    UpdateArgs a{};
+    for (int d = 0; d < 3; d++) {
+      a.U[d] = U[d];
+      a.V[d] = V[d];
+      a.C0[d] = C0[d];
+    }
+    a.nx = nx;
+    a.ny = ny;
+    a.nz = nz;
+    a.W = pl.zW;
+    a.hK = dt / 2;
+    a.nuhK = nu * dt / 2;
+    a.stats = stats;
+    rc = prec == PREC_C128 ? update<double>(pl, a, s) : update<float>(pl, a, s);
+    if (rc) return rc;
+    mark();
+  }
+  return OK;
+}
+
+int ns_stats_final(const NSPlan& pl, const double* partials, double* out4, cudaStream_t s) {
+  k_stats_final<<<1, 256, 0, s>>>(partials, pl.update_blocks, out4);
+  SNS_CHECK_LAUNCH("k_stats_final");
+  return OK;
+}
+
+}  // namespace sns

@@ -1,0 +1,27 @@
+// Fused NS step (host interface).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace sns {
+
+struct NSPlan {
+  int nx, ny, nz, prec;
+  int xG;             // rows per CTA of the x cross pass
+  int zW;             // adjacent z lines per CTA of the update pass
+  int update_blocks;  // CTAs of the update pass (= diagnostics partials)
+};
+
+int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec);
+// One step in place on V (Fourier velocity) and C0 (previous cross product),
+// with six work fields U; per-block diagnostics go to `stats`
+// (4 doubles x update_blocks).
+// `ev`, when not null, holds kNSPasses + 1 events recorded around the passes.
+constexpr int kNSPasses = 5;
+int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* const U[6],
+                 double* stats, double nu, double dt, cudaStream_t s, cudaEvent_t* ev = nullptr);
+// Reduce the per-block diagnostics into out4 (device): sum|div|, sum|V|^2,
+// sum|i k x V|^2, max|div|.
+int ns_stats_final(const NSPlan& pl, const double* partials, double* out4, cudaStream_t s);
+
+}  // namespace sns

@@ -1,0 +1,166 @@
+"""The fused NS stepper against the oracle and the reference's golden run.
+
+Tolerances (relative L2 per field): complex128 vs the FP64 oracle <= 1e-12;
+complex64 vs the complex128 device path <= 2e-5 per field per step."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def dev(a, dtype, device):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(device=device, dtype=dtype)
+
+
+def host(t):
+    return t.detach().cpu().to(torch.complex128).numpy()
+
+
+@pytest.mark.parametrize("case,nu", [("tg", 0.01), ("vx", 1e-3)])
+def test_stepper_matches_reference_golden(sns, cuda, case, nu):
+    """16^3, ns.cpp bootstrap + 5 steps, against the reference's own run."""
+    g = np.load(os.path.join(GOLD, "ns16.npz"))
+    steps = int(g["steps"])
+    V0 = [dev(g[f"{case}_V0_{d}"], torch.complex128, cuda) for d in range(3)]
+    w0 = [dev(g[f"{case}_omega0_{d}"], torch.complex128, cuda) for d in range(3)]
+    st = sns.NSStepper((16, 16, 16), nu, 1e-3, torch.complex128)
+    st.bootstrap(V0, w0)
+    st.step(steps)
+    s = st.state()
+    scale = max(np.abs(g[f"{case}_V1_{d}"]).max() for d in range(3))
+    for d in range(3):
+        assert rel_l2(host(s["V1"][d]), g[f"{case}_V1_{d}"]) < 1e-12
+        assert rel_l2(host(s["cross0"][d]), g[f"{case}_cross0_{d}"]) < 1e-12
+    stats = st.stats()
+    assert abs(stats["div_avg"] - g[f"{case}_div_avgs"][-1]) < 1e-12 * scale
+    st.close()
+
+
+def test_config1_taylor_green_64_every_field(sns, oracle, cuda):
+    """64^3 Taylor-Green, nu = 0.01, dt = 1e-3, 100 steps: V1, omega1 and
+    cross0 against the oracle run of the ns.cpp sequence at steps 1, 10, 100."""
+    from spectral_upcxx_b200 import ic
+    n, nu, dt = 64, 0.01, 1e-3
+    V0 = [oracle.forward(c) for c in ic.taylor_green(n)]
+    w0 = oracle.curl(V0)
+    st = sns.NSStepper((n, n, n), nu, dt, torch.complex128)
+    st.bootstrap([dev(x, torch.complex128, cuda) for x in V0],
+                 [dev(x, torch.complex128, cuda) for x in w0])
+    ns = oracle.NS((n, n, n), nu, dt)
+    ns.bootstrap(V0, w0)
+    done = 0
+    for target in (1, 10, 100):
+        for _ in range(target - done):
+            ns.step()
+        st.step(target - done)
+        done = target
+        ref = ns.state()
+        got = st.state()
+        for key in ("V1", "omega1", "cross0"):
+            for d in range(3):
+                if np.linalg.norm(ref[key][d]) == 0:
+                    assert np.abs(host(got[key][d])).max() < 1e-12
+                else:
+                    assert rel_l2(host(got[key][d]), ref[key][d]) < 1e-12, (target, key, d)
+    # kinetic energy decays as exp(-2 nu |k|^2 t) = exp(-6 nu t) at early times
+    e = st.stats()["energy"]
+    e0 = 0.125  # <|u|^2>/2 of the Taylor-Green field
+    assert abs(e / (e0 * np.exp(-6 * nu * 0.101)) - 1) < 2e-3
+    st.close()
+
+
+@pytest.mark.parametrize("n", [32, 64])
+def test_fp32_tracks_fp64(sns, oracle, cuda, n):
+    """Spectrum-seeded solenoidal field: complex64 vs complex128 device paths."""
+    from spectral_upcxx_b200 import ic
+    nu, dt = 1 / 400, 2e-3
+    u = ic.solenoidal_spectrum(n, seed=3)
+    V0 = [oracle.forward(c) for c in u]
+    w0 = oracle.curl(V0)
+    runs = {}
+    for dt_ in (torch.complex128, torch.complex64):
+        s = sns.NSStepper((n, n, n), nu, dt, dt_)
+        s.bootstrap([dev(x, dt_, cuda) for x in V0], [dev(x, dt_, cuda) for x in w0])
+        runs[dt_] = s
+    worst = 0.0
+    for step in range(20):
+        for s in runs.values():
+            s.step(1)
+        a, b = runs[torch.complex64].state(), runs[torch.complex128].state()
+        for key in ("V1", "cross0"):
+            for d in range(3):
+                worst = max(worst, rel_l2(host(a[key][d]), host(b[key][d])))
+    assert worst < 2e-5, worst
+    sa, sb = runs[torch.complex64].stats(), runs[torch.complex128].stats()
+    assert abs(sa["energy"] / sb["energy"] - 1) < 1e-5
+    for s in runs.values():
+        s.close()
+
+
+def test_divergence_free_and_energy_monotone(sns, oracle, cuda):
+    from spectral_upcxx_b200 import ic
+    n = 64
+    u = ic.solenoidal_spectrum(n, seed=5)
+    V0 = [oracle.forward(c) for c in u]
+    w0 = oracle.curl(V0)
+    s = sns.NSStepper((n, n, n), 1 / 400, 2e-3, torch.complex128)
+    s.bootstrap([dev(x, torch.complex128, cuda) for x in V0],
+                [dev(x, torch.complex128, cuda) for x in w0])
+    last = None
+    for _ in range(10):
+        s.step(1)
+        st = s.stats()
+        vmax = max(torch.abs(x).max().item() for x in s.state()["V1"])
+        assert st["max_div"] < 1e-12 * vmax * n
+        if last is not None:
+            assert st["energy"] < last
+        last = st["energy"]
+    s.close()
+
+
+def test_fp32_vs_fp64_256_config3(sns, oracle, cuda):
+    """Benchmark configuration: 256^3, nu = 1/400, dt = 2e-3, 500 steps.
+    Per-field relative L2 of the complex64 path against the complex128 path,
+    checked every 50 steps; energy-decay error at the end."""
+    from spectral_upcxx_b200 import ic
+    n, nu, dt = 256, 1 / 400, 2e-3
+    u = ic.solenoidal_spectrum(n, seed=1)
+    V0 = [np.fft.fftn(c) for c in u]
+    h = n // 2
+    for c in V0:
+        c[h, :, :] = 0
+        c[:, h, :] = 0
+        c[:, :, h] = 0
+    runs = {}
+    for dt_ in (torch.complex128, torch.complex64):
+        Vd = [dev(x, dt_, cuda) for x in V0]
+        wd = sns.curl(Vd)
+        s = sns.NSStepper((n, n, n), nu, dt, dt_)
+        s.bootstrap(Vd, wd)
+        del Vd, wd
+        runs[dt_] = s
+    worst = 0.0
+    e = {}
+    for block in range(10):
+        for s in runs.values():
+            s.step(50)
+        a, b = runs[torch.complex64].state(), runs[torch.complex128].state()
+        for d in range(3):
+            va = a["V1"][d].to(torch.complex128)
+            err = (torch.linalg.vector_norm(va - b["V1"][d]) /
+                   torch.linalg.vector_norm(b["V1"][d])).item()
+            worst = max(worst, err)
+        del a, b
+        e = {k: s.stats()["energy"] for k, s in runs.items()}
+    assert worst < 2e-5, worst
+    assert abs(e[torch.complex64] / e[torch.complex128] - 1) < 1e-5
+    for s in runs.values():
+        s.close()
+    torch.cuda.empty_cache()
