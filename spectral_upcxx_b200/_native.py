@@ -91,11 +91,12 @@ def header_functions():
 
 
 def lib(build: bool = True):
-    """Load libspectral_b200.so (building it first when sources changed)."""
+    """Load libspectral_b200.so.  It is built first only when it is missing
+    (or when SNS_REBUILD=1); __graft_entry__.build() rebuilds explicitly."""
     global _LIB
     if _LIB is None:
         path = _build.LIBPATH
-        if build:
+        if build and (not os.path.exists(path) or os.environ.get("SNS_REBUILD") == "1"):
             _build.build_library()
         if not os.path.exists(path):
             raise ImportError(f"{path} is missing: run spectral_upcxx_b200.build.build_library()")
