@@ -102,7 +102,8 @@ def build_library(verbose: bool = False) -> str:
 
 def build_cpp_program(sources, out: str, extra_flags=None) -> str:
     """Link a C++ program written against the reference API headers."""
-    build_library()
+    if not os.path.exists(LIBPATH):
+        build_library()
     srcs = [sources] if isinstance(sources, str) else list(sources)
     deps = srcs + [LIBPATH]
     if _newer(out, deps):
