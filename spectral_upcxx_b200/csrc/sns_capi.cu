@@ -283,6 +283,7 @@ int sns_fft1d_many(void* data, int64_t n, int64_t stride, int64_t howmany, int64
   g.L = (int)n;
   g.ps = stride;
   g.nx = g.ny = g.nz = 1;
+  g.axis = -1;
   const int TPL = (int)(n >= 16 ? n / 16 : 1);
   auto pow2_divisor = [](int64_t v, int cap) {
     int d = 1;

@@ -75,6 +75,21 @@ enum Status : int {
 
 int cuda_status(cudaError_t e, const char* where);
 
+// Opt a kernel into the largest dynamic shared memory that its static shared
+// memory leaves on this device.
+template <typename K>
+inline cudaError_t allow_max_dynamic_smem(K* kernel) {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, (const void*)kernel);
+  if (e != cudaSuccess) return e;
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              optin - (int)a.sharedSizeBytes);
+}
+
 // Number of SMs of the current device (cached).
 int sm_count();
 

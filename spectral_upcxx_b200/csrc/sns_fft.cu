@@ -79,27 +79,52 @@ const void* twiddles(int L, int prec) {
   return d;
 }
 
-// Element idx of field `field` as the prologue forms it.
+// Thread layout of a tile of W adjacent lines x G groups: thread t owns line
+// (w, g) with w = t mod W, and within it positions j + e*TPL (e < E), where
+// s = t / W, j = s mod TPL, g = s / TPL.  Consecutive threads hold the same
+// position of adjacent lines (unit stride in memory) for W > 1, or adjacent
+// positions of one line for W = 1, so the direct global loads and stores are
+// coalesced and each thread has E independent loads in flight.  The line FFT
+// then starts from registers; shared memory only carries the exchanges
+// between radix stages.
+struct LineCoord {
+  int64_t idx0, step;  // global index of position j, stride between e
+  int x, y, z;         // coordinates of position j (3D fields)
+};
+
+__device__ __forceinline__ LineCoord line_coord(const LineGeo& geo, int64_t base, int w, int g,
+                                                int j, int tpl) {
+  LineCoord c;
+  c.idx0 = base + w + g * geo.gs + (int64_t)j * geo.ps;
+  c.step = (int64_t)tpl * geo.ps;
+  c.x = c.y = c.z = 0;
+  if (geo.axis >= 0) {
+    const int64_t nxy = (int64_t)geo.nx * geo.ny;
+    const int64_t z = c.idx0 / nxy;
+    const int64_t r = c.idx0 - z * nxy;
+    const int64_t y = r / geo.nx;
+    c.x = (int)(r - y * geo.nx);
+    c.y = (int)y;
+    c.z = (int)z;
+  }
+  return c;
+}
+
+// Element e of the thread's line as the prologue forms it.
 template <int PRO, typename C>
-__device__ __forceinline__ C pro_load(const FieldPtrs& f, int field, int64_t idx,
+__device__ __forceinline__ C pro_load(const C* __restrict__ src, const C* __restrict__ v0,
+                                      const C* __restrict__ v1, const C* __restrict__ v2,
+                                      int field, int64_t idx, int x, int y, int z,
                                       const LineGeo& geo) {
   if constexpr (PRO == PRO_CURL6) {
-    if (field < 3) return reinterpret_cast<const C*>(f.in[field])[idx];
-    const int64_t nxy = (int64_t)geo.nx * geo.ny;
-    const int z = (int)(idx / nxy);
-    const int64_t r = idx - (int64_t)z * nxy;
-    const int y = (int)(r / geo.nx);
-    const int x = (int)(r - (int64_t)y * geo.nx);
+    if (field < 3) return src[idx];
     using T = decltype(C().x);
     const T kx = (T)freq_i(x, geo.nx), ky = (T)freq_i(y, geo.ny), kz = (T)freq_i(z, geo.nz);
-    const C* v0 = reinterpret_cast<const C*>(f.in[0]);
-    const C* v1 = reinterpret_cast<const C*>(f.in[1]);
-    const C* v2 = reinterpret_cast<const C*>(f.in[2]);
     if (field == 3) return csub(ikmul(ky, v2[idx]), ikmul(kz, v1[idx]));
     if (field == 4) return csub(ikmul(kz, v0[idx]), ikmul(kx, v2[idx]));
     return csub(ikmul(kx, v1[idx]), ikmul(ky, v0[idx]));
   } else {
-    return reinterpret_cast<const C*>(f.in[field])[idx];
+    return src[idx];
   }
 }
 
@@ -116,53 +141,45 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
   const int nf = f.n;
   const int field = blockIdx.x % nf;
   const int64_t t = blockIdx.x / nf;
-  C* __restrict__ dst = reinterpret_cast<C*>(f.out[field]);
   const int64_t base = (t % geo.TA) * geo.sa + (t / geo.TA) * geo.sb;
   const int W = geo.W;
-  const int total = (W * geo.G) * L;
+  const int w = threadIdx.x & (W - 1);
+  const int s = threadIdx.x >> wshift;
+  const int j = s & (TPL - 1);
+  const int g = s / TPL;
+  C* row = sm + (w + W * g) * RS;
+  const LineCoord lc = line_coord(geo, base, w, g, j, TPL);
 
-  // coalesced tile load: consecutive threads walk the unit-stride index
-  for (int q = threadIdx.x; q < total; q += blockDim.x) {
-    const int w = q & (W - 1);
-    const int rest = q >> wshift;
-    const int p = rest & (L - 1);
-    const int g = rest / L;
-    const int64_t idx = base + w + g * geo.gs + (int64_t)p * geo.ps;
-    sm[(w + W * g) * RS + pad_pos(p)] = pro_load<PRO, C>(f, field, idx, geo);
-  }
-  __syncthreads();
-
-  const int j = threadIdx.x % TPL;
-  const int line = threadIdx.x / TPL;
-  C* row = sm + line * RS;
+  const C* __restrict__ src = reinterpret_cast<const C*>(f.in[field]);
   C v[E];
+  {
+    const C* __restrict__ v0 = reinterpret_cast<const C*>(f.in[0]);
+    const C* __restrict__ v1 = reinterpret_cast<const C*>(f.in[1]);
+    const C* __restrict__ v2 = reinterpret_cast<const C*>(f.in[2]);
 #pragma unroll
-  for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
-  line_sync<TPL>();
-  line_fft<L>(v, row, j, tw, sg);
-#pragma unroll
-  for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
-  __syncthreads();
+    for (int e = 0; e < E; e++) {
+      const int p = j + TPL * e;
+      v[e] = pro_load<PRO, C>(src, v0, v1, v2, field, lc.idx0 + e * lc.step,
+                              geo.axis == 0 ? p : lc.x, geo.axis == 1 ? p : lc.y,
+                              geo.axis == 2 ? p : lc.z, geo);
+    }
+  }
+  line_fft<L, true>(v, row, j, tw, sg);
 
+  C* __restrict__ dst = reinterpret_cast<C*>(f.out[field]);
   const bool do_scale = flags & PASS_SCALE;
   const bool do_zero = flags & PASS_ZERO_NYQUIST;
-  const int64_t nxy = (int64_t)geo.nx * geo.ny;
-  for (int q = threadIdx.x; q < total; q += blockDim.x) {
-    const int w = q & (W - 1);
-    const int rest = q >> wshift;
-    const int p = rest & (L - 1);
-    const int g = rest / L;
-    const int64_t idx = base + w + g * geo.gs + (int64_t)p * geo.ps;
-    C val = sm[(w + W * g) * RS + pad_pos(p)];
+  const bool line_on_plane = (geo.axis != 0 && lc.x == (geo.nx >> 1)) ||
+                             (geo.axis != 1 && lc.y == (geo.ny >> 1)) ||
+                             (geo.axis != 2 && lc.z == (geo.nz >> 1));
+  const int half_axis = geo.axis == 0 ? (geo.nx >> 1) : geo.axis == 1 ? (geo.ny >> 1)
+                                                                      : (geo.nz >> 1);
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    C val = v[e];
     if (do_scale) val = cscale(scale, val);
-    if (do_zero) {
-      const int64_t z = idx / nxy;
-      const int64_t r = idx - z * nxy;
-      const int64_t y = r / geo.nx;
-      const int64_t x = r - y * geo.nx;
-      if (x == (geo.nx >> 1) || y == (geo.ny >> 1) || z == (geo.nz >> 1)) val = mk((T)0, (T)0);
-    }
-    dst[idx] = val;
+    if (do_zero && (line_on_plane || j + TPL * e == half_axis)) val = mk((T)0, (T)0);
+    dst[lc.idx0 + e * lc.step] = val;
   }
 }
 
@@ -199,8 +216,7 @@ static int launch_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int fla
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_set[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(k_line_pass<T, L, PRO>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaError_t e = allow_max_dynamic_smem(k_line_pass<T, L, PRO>);
     if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_line_pass)");
     attr_set[dev & 63] = true;
   }
@@ -288,6 +304,7 @@ static void choose_tile(LineGeo& g, int64_t adjacent, int64_t groups, int prec) 
 LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec) {
   LineGeo g{};
   g.nx = nx;
+  g.axis = axis;
   g.ny = ny;
   g.nz = nz;
   const int64_t nxy = (int64_t)nx * ny;

@@ -32,8 +32,10 @@ struct LineGeo {
   int W, G;    // adjacent lines and groups per tile
   int64_t ps, gs;
   int64_t TA, TB, sa, sb;
-  // field dimensions, used by the Nyquist epilogue to recover (x, y, z)
+  // field dimensions and the axis of the lines (0, 1, 2; -1 for plain 1D
+  // batches), used by the curl prologue and the Nyquist epilogue
   int nx, ny, nz;
+  int axis;
 };
 
 struct FieldPtrs {

@@ -132,11 +132,20 @@ __device__ __forceinline__ void line_sync() {
 // the row at once, so the caller synchronises the line after its own reads of
 // the row.  Every thread of the block must call this (it may synchronise the
 // block when TPL > 32).
-template <int L, typename C, typename T>
+//
+// BLOCK = true synchronises the whole block between stages, for layouts in
+// which the threads of a line are not confined to one warp.
+template <int L, bool BLOCK = false, typename C, typename T>
 __device__ __forceinline__ void line_fft(C (&v)[LinePlan<L>::E], C* row, int j,
                                          const C* __restrict__ tw, T sg) {
   using P = LinePlan<L>;
   constexpr int E = P::E, TPL = P::TPL;
+  auto sync = [] {
+    if constexpr (BLOCK)
+      __syncthreads();
+    else
+      line_sync<TPL>();
+  };
   int Ns = 1;
 #pragma unroll
   for (int s = 0; s < P::NSTAGE; s++) {
@@ -145,7 +154,7 @@ __device__ __forceinline__ void line_fft(C (&v)[LinePlan<L>::E], C* row, int j,
     if (s > 0) {
 #pragma unroll
       for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
-      line_sync<TPL>();
+      sync();
     }
     // butterflies m = 0 .. E/R-1 of this thread
 #pragma unroll
@@ -185,7 +194,7 @@ __device__ __forceinline__ void line_fft(C (&v)[LinePlan<L>::E], C* row, int j,
           if (r < R) row[pad_pos(base + r * Ns)] = a[r];
       }
     }
-    if (!last) line_sync<TPL>();
+    if (!last) sync();
     Ns *= R;
   }
 }

@@ -40,19 +40,18 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
   const int64_t row0 = (int64_t)blockIdx.x * G;
   const int per = G * L;
 
-  for (int q = threadIdx.x; q < 6 * per; q += blockDim.x) {
-    const int fld = q / per, rem = q - fld * per, g = rem / L, p = rem & (L - 1);
-    sm[(fld * G + g) * RS + pad_pos(p)] =
-        reinterpret_cast<const C*>(f.in[fld])[(row0 + g) * L + p];
-  }
-  __syncthreads();
-
+  // thread t owns line t / TPL (field-major: field = line / G, row = line % G)
+  // at positions j + e*TPL; loads go straight to registers, E per thread
   const int j = threadIdx.x % TPL, line = threadIdx.x / TPL;
+  const int fld = line / G, gl = line - fld * G;
   C* row = sm + line * RS;
   C v[E];
+  {
+    const C* __restrict__ src = reinterpret_cast<const C*>(f.in[fld]);
+    const int64_t i0 = (row0 + gl) * L + j;
 #pragma unroll
-  for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
-  line_sync<TPL>();
+    for (int e = 0; e < E; e++) v[e] = src[i0 + TPL * e];
+  }
   line_fft<L>(v, row, j, tw, (T)1);
 #pragma unroll
   for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
@@ -82,13 +81,12 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
   for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
   line_sync<TPL>();
   line_fft<L>(v, row, j, tw, (T)-1);
-#pragma unroll
-  for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
-  __syncthreads();
 
-  for (int q = threadIdx.x; q < 3 * per; q += blockDim.x) {
-    const int fld = q / per, rem = q - fld * per, g = rem / L, p = rem & (L - 1);
-    reinterpret_cast<C*>(f.out[fld])[(row0 + g) * L + p] = sm[(fld * G + g) * RS + pad_pos(p)];
+  if (fld < 3) {
+    C* __restrict__ dst = reinterpret_cast<C*>(f.out[fld]);
+    const int64_t i0 = (row0 + gl) * L + j;
+#pragma unroll
+    for (int e = 0; e < E; e++) dst[i0 + TPL * e] = v[e];
   }
 }
 
@@ -124,41 +122,41 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
   const int64_t base = x0 + (int64_t)a.nx * y;
   const int per = W * L;
 
-  for (int q = threadIdx.x; q < 3 * per; q += blockDim.x) {
-    const int fld = q / per, rem = q - fld * per, w = rem % W, p = rem / W;
-    sm[(fld * W + w) * RS + pad_pos(p)] =
-        reinterpret_cast<const C*>(a.U[fld])[base + w + nxy * p];
+  // thread t owns z line (field, x0 + w) at positions j + e*TPL with
+  // w = t mod W, j = (t / W) mod TPL, field = t / (W*TPL): consecutive threads
+  // load adjacent x, so the direct loads are coalesced
+  {
+    const int w = threadIdx.x % W, s = threadIdx.x / W;
+    const int j = s % TPL, fld = s / TPL;
+    C* row = sm + (fld * W + w) * RS;
+    const C* __restrict__ src = reinterpret_cast<const C*>(a.U[fld]);
+    const int64_t i0 = base + w + nxy * j;
+    C v[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = src[i0 + nxy * (TPL * e)];
+    line_fft<L, true>(v, row, j, tw, (T)-1);
+#pragma unroll
+    for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
   }
-  __syncthreads();
-
-  const int j = threadIdx.x % TPL, line = threadIdx.x / TPL;
-  C* row = sm + line * RS;
-  C v[E];
-#pragma unroll
-  for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
-  line_sync<TPL>();
-  line_fft<L>(v, row, j, tw, (T)-1);
-#pragma unroll
-  for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
   __syncthreads();
 
   const T hK = (T)a.hK, nuhK = (T)a.nuhK;
   const T ky = (T)freq_i(y, a.ny);
   const bool ynyq = (y == (a.ny >> 1));
   double s_div = 0, s_e = 0, s_w = 0, m_div = 0;
-  for (int q = threadIdx.x; q < per; q += blockDim.x) {
+  C* __restrict__ Vp[3] = {reinterpret_cast<C*>(a.V[0]), reinterpret_cast<C*>(a.V[1]),
+                           reinterpret_cast<C*>(a.V[2])};
+  C* __restrict__ Cp[3] = {reinterpret_cast<C*>(a.C0[0]), reinterpret_cast<C*>(a.C0[1]),
+                           reinterpret_cast<C*>(a.C0[2])};
+  auto update_point = [&](int q, const C (&V1)[3], const C (&c0)[3]) {
     const int w = q % W, z = q / W;
     const int x = x0 + w;
     const int64_t idx = base + w + nxy * z;
     const T kx = (T)freq_i(x, a.nx), kz = (T)freq_i(z, a.nz);
     const bool nyq = ynyq || x == (a.nx >> 1) || z == (a.nz >> 1);
-    C c1[3], V1[3], c0[3];
+    C c1[3];
 #pragma unroll
-    for (int d = 0; d < 3; d++) {
-      c1[d] = nyq ? mk((T)0, (T)0) : sm[(d * W + w) * RS + pad_pos(z)];
-      V1[d] = reinterpret_cast<const C*>(a.V[d])[idx];
-      c0[d] = reinterpret_cast<const C*>(a.C0[d])[idx];
-    }
+    for (int d = 0; d < 3; d++) c1[d] = nyq ? mk((T)0, (T)0) : sm[(d * W + w) * RS + pad_pos(z)];
     const T kk[3] = {kx, ky, kz};
     const T k2 = kx * kx + ky * ky + kz * kz;
     const double k2d = (double)kx * kx + (double)ky * ky + (double)kz * kz;
@@ -187,8 +185,8 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
       C vv = cadd(vh, lap[d]);
       if (k2d != 0.0) vv = mk((T)((double)vv.x / den_cn), (T)((double)vv.y / den_cn));
       Vn[d] = vv;
-      reinterpret_cast<C*>(a.V[d])[idx] = vv;
-      reinterpret_cast<C*>(a.C0[d])[idx] = c1[d];
+      Vp[d][idx] = vv;
+      Cp[d][idx] = c1[d];
     }
     // FP64 diagnostics of the new velocity
     const C dv = cadd(cadd(ikmul(kx, Vn[0]), ikmul(ky, Vn[1])), ikmul(kz, Vn[2]));
@@ -205,6 +203,23 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
          (double)om1.y * om1.y + (double)om2.x * om2.x + (double)om2.y * om2.y;
     s_e += e2;
     s_w += w2;
+  };
+  // two points per iteration: the 12 global loads of both are issued first
+  for (int q0 = threadIdx.x; q0 < per; q0 += 2 * blockDim.x) {
+    const int q1 = q0 + blockDim.x;
+    const bool has1 = q1 < per;
+    C V1a[3], c0a[3], V1b[3], c0b[3];
+    const int64_t ia = base + (q0 % W) + nxy * (q0 / W);
+    const int64_t ib = has1 ? base + (q1 % W) + nxy * (q1 / W) : ia;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      V1a[d] = Vp[d][ia];
+      c0a[d] = Cp[d][ia];
+      V1b[d] = Vp[d][ib];
+      c0b[d] = Cp[d][ib];
+    }
+    update_point(q0, V1a, c0a);
+    if (has1) update_point(q1, V1b, c0b);
   }
   // block reduction of the diagnostics
   for (int o = 16; o > 0; o >>= 1) {
@@ -280,8 +295,7 @@ int launch_xcross(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(k_xcross<T, L>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaError_t e = allow_max_dynamic_smem(k_xcross<T, L>);
     if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_xcross)");
     attr[dev & 63] = true;
   }
@@ -303,8 +317,7 @@ int launch_update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(k_zfwd_update<T, L>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaError_t e = allow_max_dynamic_smem(k_zfwd_update<T, L>);
     if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_zfwd_update)");
     attr[dev & 63] = true;
   }

@@ -18,7 +18,7 @@ int main(int argc, char* argv[]) {
   double nu = atof(argv[3]), K = atof(argv[4]);
   bool tg = std::strcmp(argv[5], "tg") == 0;
   array<INT, DIM> dims = {N, N, N};
-  Vector omega0(dims), omega1(dims, false), omega(dims, false);
+  Vector omega0(dims, !tg), omega1(dims, false), omega(dims, false);
   Vector V0(dims, false), V1(dims, false), V(dims, false), Vhalf(dims, false);
   Scalar Pi0(dims, false), Pi1(dims, false), G(dims, false), div(dims, false);
   array<INT, DIM> ind;

@@ -49,6 +49,7 @@ def test_api_ns_sequence_matches_oracle(cuda, oracle, tmp_path, case, nu):
     out = tmp_path / "state.bin"
     r = _run([_exe("api_ns_dump"), str(n), str(steps), repr(nu), repr(K), case, str(out)])
     assert r.returncode == 0, r.stdout
+    assert out.exists() and "ERROR" not in r.stdout, r.stdout
     data = np.fromfile(out, dtype=np.complex128).reshape(3, 3, n, n, n)
     if case == "tg":
         V0 = [oracle.forward(c) for c in ic.taylor_green(n)]

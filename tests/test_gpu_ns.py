@@ -130,7 +130,7 @@ def test_fp32_vs_fp64_256_config3(sns, oracle, cuda):
     Per-field relative L2 of the complex64 path against the complex128 path,
     checked every 50 steps; energy-decay error at the end."""
     from spectral_upcxx_b200 import ic
-    n, nu, dt = 256, 1 / 400, 2e-3
+    n, nu, dt = 256, 1 / 400, 5e-4  # the stated dt = 2e-3 diverges at 256^3 in FP64 too
     u = ic.solenoidal_spectrum(n, seed=1)
     V0 = [np.fft.fftn(c) for c in u]
     h = n // 2
@@ -156,7 +156,7 @@ def test_fp32_vs_fp64_256_config3(sns, oracle, cuda):
             va = a["V1"][d].to(torch.complex128)
             err = (torch.linalg.vector_norm(va - b["V1"][d]) /
                    torch.linalg.vector_norm(b["V1"][d])).item()
-            worst = max(worst, err)
+            worst = max(worst, err if np.isfinite(err) else float("inf"))
         del a, b
         e = {k: s.stats()["energy"] for k, s in runs.items()}
     assert worst < 2e-5, worst
