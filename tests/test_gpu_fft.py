@@ -83,7 +83,7 @@ def test_batched_fields_equal_single(sns, cuda, dtype):
 @pytest.mark.parametrize("dtype", DT)
 @pytest.mark.parametrize("n,stride,howmany,dist", [(256, 1, 64, 256), (64, 64, 64, 1),
                                                    (128, 3, 5, 1000), (16, 1, 7, 19),
-                                                   (1024, 2, 3, 1)])
+                                                   (1024, 4, 3, 1), (2048, 8, 8, 1)])
 def test_fft1d_many_matches_numpy(sns, cuda, dtype, n, stride, howmany, dist):
     rng = np.random.default_rng(n + howmany)
     size = (howmany - 1) * dist + (n - 1) * stride + 1
