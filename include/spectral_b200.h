@@ -152,6 +152,10 @@ int sns_ns_get_state(sns_ns* handle, void* const V1[3], void* const omega1[3],
  * 0.5<|u|^2>, enstrophy 0.5<|omega|^2> and max |div u_hat|.  Synchronises. */
 int sns_ns_stats(sns_ns* handle, double* div_avg, double* energy, double* enstrophy,
                  double* max_div);
+/* Synchronise and report whether any step since the last check hit a bounded
+ * wait of the persistent xy pass that gave up (SNS_ERR_TIMEOUT: the results
+ * of those steps are invalid).  sns_ns_stats performs this check too. */
+int sns_ns_check(sns_ns* handle);
 /* Number of kernel launches one sns_ns_step(h, 1) issues. */
 int sns_ns_launches_per_step(sns_ns* handle);
 /* Per-pass timing (no reference counterpart; the reference times phases with

@@ -68,6 +68,7 @@ SIGNATURES = {
     "sns_ns_get_state": ([_vp, _vp3, _vp3, _vp3], _int),
     "sns_ns_stats": ([_vp, C.POINTER(_dbl), C.POINTER(_dbl), C.POINTER(_dbl), C.POINTER(_dbl)],
                      _int),
+    "sns_ns_check": ([_vp], _int),
     "sns_ns_launches_per_step": ([_vp], _int),
     "sns_ns_profile": ([_vp, _int], _int),
     "sns_ns_pass_times": ([_vp, C.POINTER(_dbl), C.POINTER(_int), _int], _int),

@@ -172,6 +172,7 @@ struct sns_ns {
   void* U[6];
   double* stats_part;
   double* stats_out;
+  int* sync_words;  // dataflow xy pass: ticket, per-plane counters, error word
   bool stepped;
   // per-pass profiling
   bool profiling = false;
@@ -453,6 +454,10 @@ int sns_ns_create(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double nu
   for (int i = 0; i < 12 && rc == OK; i++) rc = pool_malloc(all[i], bytes);
   if (rc == OK) rc = pool_malloc((void**)&h->stats_part, sizeof(double) * 4 * h->pl.update_blocks);
   if (rc == OK) rc = pool_malloc((void**)&h->stats_out, sizeof(double) * 4);
+  if (rc == OK) rc = pool_malloc((void**)&h->sync_words, sizeof(int) * xy_sync_words((int)nz));
+  if (rc == OK)
+    rc = cuda_status(cudaMemsetAsync(h->sync_words, 0, sizeof(int) * xy_sync_words((int)nz), h->s),
+                     "sns_ns_create");
   if (rc == OK) {
     for (int i = 0; i < 6 && rc == OK; i++)
       rc = cuda_status(cudaMemsetAsync(*all[i], 0, bytes, h->s), "sns_ns_create");
@@ -476,6 +481,7 @@ int sns_ns_destroy(sns_ns* h) {
   for (int i = 0; i < 6; i++) pool_free(h->U[i]);
   pool_free(h->stats_part);
   pool_free(h->stats_out);
+  pool_free(h->sync_words);
   for (cudaEvent_t e : h->events) cudaEventDestroy(e);
   delete h;
   return OK;
@@ -548,7 +554,8 @@ int sns_ns_step(sns_ns* h, int nsteps) {
       }
       ev = &h->events[(size_t)h->recorded * (kNSPasses + 1)];
     }
-    int rc = ns_step_once(h->pl, h->V, h->C0, h->U, h->stats_part, h->nu, h->dt, h->s, ev);
+    int rc = ns_step_once(h->pl, h->V, h->C0, h->U, h->stats_part, h->sync_words, h->nu, h->dt,
+                          h->s, ev);
     if (rc) return rc;
     if (ev) h->recorded++;
     h->stepped = true;
@@ -575,7 +582,7 @@ int sns_ns_pass_times(sns_ns* h, double* total_ms, int* launches, int max) {
   }
   for (int t = 0; t < h->recorded; t++) {
     cudaEvent_t* ev = &h->events[(size_t)t * (kNSPasses + 1)];
-    for (int p = 0; p < kNSPasses && p < max; p++) {
+    for (int p = 0; p < h->pl.passes && p < max; p++) {
       float ms = 0;
       if ((rc = cuda_status(cudaEventElapsedTime(&ms, ev[p], ev[p + 1]), "sns_ns_pass_times")))
         return rc;
@@ -583,7 +590,7 @@ int sns_ns_pass_times(sns_ns* h, double* total_ms, int* launches, int max) {
       launches[p] += 1;
     }
   }
-  return kNSPasses;
+  return h->pl.passes;
 }
 
 int sns_ns_get_state(sns_ns* h, void* const V1[3], void* const omega1[3], void* const cross0[3]) {
@@ -610,13 +617,32 @@ int sns_ns_get_state(sns_ns* h, void* const V1[3], void* const omega1[3], void* 
   return OK;
 }
 
+int sns_ns_check(sns_ns* h) {
+  if (!nonnull(h, "sns_ns_check")) return ERR_ARG;
+  const size_t err_index = xy_sync_words(h->pl.nz) - 1;
+  int err = 0;
+  int rc = cuda_status(cudaMemcpyAsync(&err, h->sync_words + err_index, sizeof(int),
+                                       cudaMemcpyDeviceToHost, h->s),
+                       "sns_ns_check");
+  if (rc) return rc;
+  if ((rc = cuda_status(cudaStreamSynchronize(h->s), "sns_ns_check"))) return rc;
+  if (err) {
+    cudaMemsetAsync(h->sync_words + err_index, 0, sizeof(int), h->s);
+    set_error("sns_ns_step: a wait of the xy dataflow pass gave up; results are invalid");
+    return ERR_TIMEOUT;
+  }
+  return OK;
+}
+
 int sns_ns_stats(sns_ns* h, double* div_avg, double* energy, double* enstrophy, double* max_div) {
   if (!nonnull(h, "sns_ns_stats")) return ERR_ARG;
   if (!h->stepped) {
     set_error("sns_ns_stats: no step has run since the state was set");
     return ERR_ARG;
   }
-  int rc = ns_stats_final(h->pl, h->stats_part, h->stats_out, h->s);
+  int rc = sns_ns_check(h);
+  if (rc) return rc;
+  rc = ns_stats_final(h->pl, h->stats_part, h->stats_out, h->s);
   if (rc) return rc;
   double v[4];
   if ((rc = cuda_status(cudaMemcpyAsync(v, h->stats_out, sizeof(v), cudaMemcpyDeviceToHost, h->s),
@@ -633,7 +659,7 @@ int sns_ns_stats(sns_ns* h, double* div_avg, double* energy, double* enstrophy, 
 
 int sns_ns_launches_per_step(sns_ns* h) {
   (void)h;
-  return kNSPasses;
+  return h->pl.passes;
 }
 
 }  // extern "C"

@@ -17,6 +17,7 @@
 // deep copies per step; here the history copies (ns.cpp:213-217) are
 // in-place updates and every intermediate lives in U.
 #include <math.h>
+#include <stdlib.h>
 
 #include <vector>
 
@@ -171,11 +172,20 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
       s[d] = cadd(cadd(V1[d], lap[d]), F[d]);
     }
     C G = cadd(cadd(ikmul(kx, s[0]), ikmul(ky, s[1])), ikmul(kz, s[2]));
-    double den_cn = 1.0;
-    if (k2d != 0.0) {
-      const double den = -k2d;
-      G = mk((T)((double)G.x / den), (T)((double)G.y / den));
-      den_cn = 1.0 + a.nuhK * k2d;
+    // The divisors -|k|^2 (projection) and 1 + nu K/2 |k|^2 (Crank-Nicolson)
+    // are formed in FP64.  complex128 divides as the reference does; complex64
+    // multiplies by the FP64 reciprocals rounded once to FP32.
+    const bool nonzero = k2d != 0.0;
+    const double den_cn = 1.0 + a.nuhK * k2d;
+    T r_p = (T)1, r_cn = (T)1;
+    if constexpr (sizeof(T) == 4) {
+      if (nonzero) {
+        r_p = (T)(-1.0 / k2d);
+        r_cn = (T)(1.0 / den_cn);
+      }
+      G = cscale(r_p, G);
+    } else {
+      if (nonzero) G = mk(G.x / -k2d, G.y / -k2d);
     }
     // Vhalf = V1 + F - grad G; V = (Vhalf + lap1) / (1 + nu K/2 |k|^2)  (ns.cpp:181-187)
     C Vn[3];
@@ -183,26 +193,30 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
     for (int d = 0; d < 3; d++) {
       C vh = csub(cadd(V1[d], F[d]), ikmul(kk[d], G));
       C vv = cadd(vh, lap[d]);
-      if (k2d != 0.0) vv = mk((T)((double)vv.x / den_cn), (T)((double)vv.y / den_cn));
+      if constexpr (sizeof(T) == 4) {
+        vv = cscale(r_cn, vv);
+      } else {
+        if (nonzero) vv = mk(vv.x / den_cn, vv.y / den_cn);
+      }
       Vn[d] = vv;
       Vp[d][idx] = vv;
       Cp[d][idx] = c1[d];
     }
-    // FP64 diagnostics of the new velocity
+    // diagnostics of the new velocity: per-mode terms in T, sums in FP64
     const C dv = cadd(cadd(ikmul(kx, Vn[0]), ikmul(ky, Vn[1])), ikmul(kz, Vn[2]));
-    const double ad = hypot((double)dv.x, (double)dv.y);
+    const double ad = (double)sqrt(dv.x * dv.x + dv.y * dv.y);
     s_div += ad;
     m_div = fmax(m_div, ad);
-    double e2 = 0, w2 = 0;
+    T e2 = 0;
 #pragma unroll
-    for (int d = 0; d < 3; d++) e2 += (double)Vn[d].x * Vn[d].x + (double)Vn[d].y * Vn[d].y;
+    for (int d = 0; d < 3; d++) e2 += Vn[d].x * Vn[d].x + Vn[d].y * Vn[d].y;
     const C om0 = csub(ikmul(ky, Vn[2]), ikmul(kz, Vn[1]));
     const C om1 = csub(ikmul(kz, Vn[0]), ikmul(kx, Vn[2]));
     const C om2 = csub(ikmul(kx, Vn[1]), ikmul(ky, Vn[0]));
-    w2 = (double)om0.x * om0.x + (double)om0.y * om0.y + (double)om1.x * om1.x +
-         (double)om1.y * om1.y + (double)om2.x * om2.x + (double)om2.y * om2.y;
-    s_e += e2;
-    s_w += w2;
+    const T w2 = om0.x * om0.x + om0.y * om0.y + om1.x * om1.x + om1.y * om1.y +
+                 om2.x * om2.x + om2.y * om2.y;
+    s_e += (double)e2;
+    s_w += (double)w2;
   };
   // two points per iteration: the 12 global loads of both are issued first
   for (int q0 = threadIdx.x; q0 < per; q0 += 2 * blockDim.x) {
@@ -285,7 +299,7 @@ __global__ void k_stats_final(const double* part, int blocks, double* out) {
 namespace {
 
 template <typename T, int L>
-int launch_xcross(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
+int launch_xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream_t s) {
   using C = cx_t<T>;
   constexpr int TPL = LinePlan<L>::TPL;
   const int G = pl.xG;
@@ -301,7 +315,7 @@ int launch_xcross(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
   }
   const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
   const double N = (double)pl.nx * pl.ny * pl.nz;
-  const int blocks = (int)((int64_t)pl.ny * pl.nz / G);
+  const int blocks = (int)(rows / G);
   k_xcross<T, L><<<blocks, threads, smem, s>>>(f, tw, G, (T)(1.0 / (N * N)));
   SNS_CHECK_LAUNCH("k_xcross");
   return OK;
@@ -327,23 +341,18 @@ int launch_update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
   return OK;
 }
 
-template <typename T, int L>
-int launch_xcross_dispatch(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
-  return launch_xcross<T, L>(pl, f, s);
-}
-
 template <typename T>
-int xcross(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
+int xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream_t s) {
   switch (pl.nx) {
-    case 4: return launch_xcross<T, 4>(pl, f, s);
-    case 8: return launch_xcross<T, 8>(pl, f, s);
-    case 16: return launch_xcross<T, 16>(pl, f, s);
-    case 32: return launch_xcross<T, 32>(pl, f, s);
-    case 64: return launch_xcross<T, 64>(pl, f, s);
-    case 128: return launch_xcross<T, 128>(pl, f, s);
-    case 256: return launch_xcross<T, 256>(pl, f, s);
-    case 512: return launch_xcross<T, 512>(pl, f, s);
-    case 1024: return launch_xcross<T, 1024>(pl, f, s);
+    case 4: return launch_xcross<T, 4>(pl, f, rows, s);
+    case 8: return launch_xcross<T, 8>(pl, f, rows, s);
+    case 16: return launch_xcross<T, 16>(pl, f, rows, s);
+    case 32: return launch_xcross<T, 32>(pl, f, rows, s);
+    case 64: return launch_xcross<T, 64>(pl, f, rows, s);
+    case 128: return launch_xcross<T, 128>(pl, f, rows, s);
+    case 256: return launch_xcross<T, 256>(pl, f, rows, s);
+    case 512: return launch_xcross<T, 512>(pl, f, rows, s);
+    case 1024: return launch_xcross<T, 1024>(pl, f, rows, s);
     default: set_error("fused NS step: nx must be a power of two in [4, 1024]"); return ERR_UNSUPPORTED;
   }
 }
@@ -397,18 +406,35 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec) {
   {
     const int TPL = nz / elems(nz);
     int W = 1;
-    const int Wmax = prec == PREC_C128 ? 8 : 16;
+    int Wmax = prec == PREC_C128 ? 8 : 16;
+    // tile width override for tuning sweeps (SNS_Z_W, a power of two)
+    if (const char* e = getenv("SNS_Z_W")) {
+      const int v = atoi(e);
+      if (v >= 1 && (v & (v - 1)) == 0) Wmax = v;
+    }
     while (W * 2 <= Wmax && nx % (W * 2) == 0 && 3 * (W * 2) * TPL <= max_threads(prec) &&
            (size_t)3 * W * 2 * row_stride(nz) * esz <= 110 * 1024)
       W *= 2;
     pl.zW = W;
     pl.update_blocks = (nx / W) * ny;
   }
+  // xy phase: three separate full-domain passes by default.  SNS_XY_PASSES=1
+  // selects the persistent dataflow launch (sns_xy.cu), which moves a third of
+  // the HBM bytes of the separate passes but measured slower on B200 at 256^3
+  // (1.09 vs 0.79 ms): these passes are bound by issue and latency, not HBM.
+  const char* env = getenv("SNS_XY_PASSES");
+  const bool dataflow = env && env[0] == '1';
+  pl.use_xy = dataflow && xy_supported(nx, ny, prec) && xy_plan(pl.xy, nx, ny, nz, prec) == OK;
+  // separate passes run in slabs of xy_chunk planes (SNS_XY_CHUNK; 0 = one slab)
+  pl.xy_chunk = 0;
+  if (const char* e = getenv("SNS_XY_CHUNK")) pl.xy_chunk = atoi(e);
+  pl.passes = (pl.use_xy || (pl.xy_chunk > 0 && pl.xy_chunk < nz)) ? 3 : 5;
   return OK;
 }
 
 int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* const U[6],
-                 double* stats, double nu, double dt, cudaStream_t s, cudaEvent_t* ev) {
+                 double* stats, int* sync_words, double nu, double dt, cudaStream_t s,
+                 cudaEvent_t* ev) {
   const int nx = pl.nx, ny = pl.ny, nz = pl.nz, prec = pl.prec;
   int rc;
   int pass = 0;
@@ -427,32 +453,55 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     if ((rc = run_line_pass(g, f, +1, 0, 1.0, prec, s, PRO_CURL6))) return rc;
     mark();
   }
-  // K2: y-inverse of the six fields
-  {
-    FieldPtrs f{};
-    f.n = 6;
-    for (int i = 0; i < 6; i++) f.in[i] = f.out[i] = U[i];
-    LineGeo g = axis_geo(1, nx, ny, nz, prec);
-    if ((rc = run_line_pass(g, f, +1, 0, 1.0, prec, s))) return rc;
+  if (pl.use_xy) {
+    // K2 + K3 + K4 as one persistent dataflow launch (sns_xy.cu)
+    if ((rc = xy_run(pl.xy, U, sync_words, s))) return rc;
     mark();
   }
-  // K3: x-inverse, cross product, x-forward
-  {
-    FieldPtrs f{};
-    f.n = 6;
-    for (int i = 0; i < 6; i++) f.in[i] = U[i];
-    for (int i = 0; i < 3; i++) f.out[i] = U[i];
-    rc = prec == PREC_C128 ? xcross<double>(pl, f, s) : xcross<float>(pl, f, s);
-    if (rc) return rc;
-    mark();
-  }
-  // K4: y-forward of the cross product
-  {
-    FieldPtrs f{};
-    f.n = 3;
-    for (int i = 0; i < 3; i++) f.in[i] = f.out[i] = U[i];
-    LineGeo g = axis_geo(1, nx, ny, nz, prec);
-    if ((rc = run_line_pass(g, f, -1, 0, 1.0, prec, s))) return rc;
+  // K2, K3, K4 on the planes [z0, z0 + pz): the passes treat the slab as an
+  // nx*ny*pz field at an offset pointer (the 1/N^2 scale keeps the full N)
+  const size_t esz = prec == PREC_C128 ? 16 : 8;
+  auto xy_range = [&](int z0, int pz, bool marks) -> int {
+    const size_t off = esz * (size_t)z0 * nx * ny;
+    void* Uc[6];
+    for (int i = 0; i < 6; i++) Uc[i] = static_cast<char*>(U[i]) + off;
+    {  // K2: y-inverse of the six fields
+      FieldPtrs f{};
+      f.n = 6;
+      for (int i = 0; i < 6; i++) f.in[i] = f.out[i] = Uc[i];
+      LineGeo g = axis_geo(1, nx, ny, pz, prec);
+      int r = run_line_pass(g, f, +1, 0, 1.0, prec, s);
+      if (r) return r;
+      if (marks) mark();
+    }
+    {  // K3: x-inverse, cross product, x-forward
+      FieldPtrs f{};
+      f.n = 6;
+      for (int i = 0; i < 6; i++) f.in[i] = Uc[i];
+      for (int i = 0; i < 3; i++) f.out[i] = Uc[i];
+      const int64_t rows = (int64_t)ny * pz;
+      int r = prec == PREC_C128 ? xcross<double>(pl, f, rows, s) : xcross<float>(pl, f, rows, s);
+      if (r) return r;
+      if (marks) mark();
+    }
+    {  // K4: y-forward of the cross product
+      FieldPtrs f{};
+      f.n = 3;
+      for (int i = 0; i < 3; i++) f.in[i] = f.out[i] = Uc[i];
+      LineGeo g = axis_geo(1, nx, ny, pz, prec);
+      int r = run_line_pass(g, f, -1, 0, 1.0, prec, s);
+      if (r) return r;
+    }
+    return OK;
+  };
+  if (!pl.use_xy) {
+    if (pl.xy_chunk > 0 && pl.xy_chunk < nz) {
+      // slabs of xy_chunk planes, so each slab's intermediates stay in L2
+      for (int z0 = 0; z0 < nz; z0 += pl.xy_chunk)
+        if ((rc = xy_range(z0, std::min(pl.xy_chunk, nz - z0), false))) return rc;
+    } else if ((rc = xy_range(0, nz, true))) {
+      return rc;
+    }
     mark();
   }
   // K5: z-forward + Nyquist zeroing + AB2/projection/CN update

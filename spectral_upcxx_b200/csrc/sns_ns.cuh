@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include "sns_xy.cuh"
+
 namespace sns {
 
 struct NSPlan {
@@ -10,6 +12,10 @@ struct NSPlan {
   int xG;             // rows per CTA of the x cross pass
   int zW;             // adjacent z lines per CTA of the update pass
   int update_blocks;  // CTAs of the update pass (= diagnostics partials)
+  bool use_xy;        // xy phase as one persistent dataflow launch
+  XYPlan xy;
+  int xy_chunk;       // planes per slab of the separate xy passes (0 = all)
+  int passes;         // timed phases per step: z-inverse, xy, z-forward+update
 };
 
 int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec);
@@ -17,9 +23,11 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec);
 // with six work fields U; per-block diagnostics go to `stats`
 // (4 doubles x update_blocks).
 // `ev`, when not null, holds kNSPasses + 1 events recorded around the passes.
+// `sync_words` (xy_sync_words(nz) ints) serves the dataflow xy pass.
 constexpr int kNSPasses = 5;
 int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* const U[6],
-                 double* stats, double nu, double dt, cudaStream_t s, cudaEvent_t* ev = nullptr);
+                 double* stats, int* sync_words, double nu, double dt, cudaStream_t s,
+                 cudaEvent_t* ev = nullptr);
 // Reduce the per-block diagnostics into out4 (device): sum|div|, sum|V|^2,
 // sum|i k x V|^2, max|div|.
 int ns_stats_final(const NSPlan& pl, const double* partials, double* out4, cudaStream_t s);

@@ -126,7 +126,7 @@ def test_divergence_free_and_energy_monotone(sns, oracle, cuda):
 
 
 def test_fp32_vs_fp64_256_config3(sns, oracle, cuda):
-    """Benchmark configuration: 256^3, nu = 1/400, dt = 2e-3, 500 steps.
+    """Benchmark configuration: 256^3, nu = 1/400, 500 steps at dt = 5e-4.
     Per-field relative L2 of the complex64 path against the complex128 path,
     checked every 50 steps; energy-decay error at the end."""
     from spectral_upcxx_b200 import ic
@@ -164,3 +164,30 @@ def test_fp32_vs_fp64_256_config3(sns, oracle, cuda):
     for s in runs.values():
         s.close()
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+def test_xy_dataflow_and_slabs_match_separate_passes(sns, cuda, dtype, monkeypatch):
+    """The persistent dataflow xy launch and the slab-chunked passes give the
+    same step as the three separate passes (to rounding)."""
+    from spectral_upcxx_b200 import ic
+    n = 64
+    V0 = [np.fft.fftn(c) for c in ic.solenoidal_spectrum(n, seed=9)]
+    out = {}
+    for name, env in (("separate", {}), ("dataflow", {"SNS_XY_PASSES": "1"}),
+                      ("slabs", {"SNS_XY_CHUNK": "16"})):
+        for k in ("SNS_XY_PASSES", "SNS_XY_CHUNK"):
+            monkeypatch.delenv(k, raising=False)
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        Vd = [dev(x, dtype, cuda) for x in V0]
+        st = sns.NSStepper((n, n, n), 1 / 400, 5e-4, dtype)
+        st.bootstrap(Vd, sns.curl(Vd))
+        st.step(4)
+        assert sns._native.lib().sns_ns_check(st.h) == 0
+        out[name] = [host(x) for x in st.state()["V1"]]
+        st.close()
+    tol = 1e-14 if dtype == torch.complex128 else 1e-6
+    for name in ("dataflow", "slabs"):
+        for a, b in zip(out[name], out["separate"]):
+            assert rel_l2(a, b) < tol, name
