@@ -115,6 +115,20 @@ int sns_vector_laplacian(const void* const v[3], void* const out[3], int64_t nx,
  * zeroing.  out may alias neither input.  Uses 6 fields of pooled scratch. */
 int sns_cross(const void* const a[3], const void* const b[3], void* const out[3], int64_t nx,
               int64_t ny, int64_t nz, int prec, void* stream);
+/* Vector::cross without any device allocation (no counterpart in the
+ * reference).  For callers that cannot let the library call cudaMalloc --
+ * device memory fully reserved by another allocator, or a loop that must not
+ * enter the driver's allocation path -- the six work fields and the twiddle
+ * tables live in a static array of the library (24 MiB of work space plus
+ * 192 KiB of tables), which each GPU that uses this function holds until the
+ * process exits.  Boxes of at most 262144 complex128 or 524288 complex64
+ * points (64^3 / 64^2*128) are accepted; larger ones return SNS_ERR_ARG.
+ * The first call on a device looks up the array's device address, so make it
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU (different streams at once) race, so serialise them.  Results
+ * equal sns_cross's. */
+int sns_cross_noalloc(const void* const a[3], const void* const b[3], void* const out[3],
+                      int64_t nx, int64_t ny, int64_t nz, int prec, void* stream);
 /* Scalar::average: mean of |f_i| over n values, accumulated in FP64
  * (src/Scalar.cpp:15-22).  Synchronises `stream`; the result is written to
  * the host double *out. */

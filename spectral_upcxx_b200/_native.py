@@ -57,6 +57,7 @@ SIGNATURES = {
     "sns_divergence": ([_vp3, _vp, _i64, _i64, _i64, _int, _vp], _int),
     "sns_vector_laplacian": ([_vp3, _vp3, _i64, _i64, _i64, _int, _vp], _int),
     "sns_cross": ([_vp3, _vp3, _vp3, _i64, _i64, _i64, _int, _vp], _int),
+    "sns_cross_noalloc": ([_vp3, _vp3, _vp3, _i64, _i64, _i64, _int, _vp], _int),
     "sns_average_abs": ([_vp, _i64, _int, C.POINTER(_dbl), _vp], _int),
     "sns_axpby": ([_dbl, _vp, _dbl, _vp, _vp, _i64, _int, _vp], _int),
     "sns_mul": ([_vp, _vp, _vp, _i64, _int, _vp], _int),

@@ -139,7 +139,7 @@ static bool nonnull(const void* p, const char* what) {
 
 // Vector::cross on device fields (src/Vector.cpp:66-90), scratch = 6 fields.
 int vector_cross(const void* const a[3], const void* const b[3], void* const out[3], Dims d,
-                 int prec, void* const scratch[6], cudaStream_t s) {
+                 int prec, void* const scratch[6], cudaStream_t s, const void* const* tw_axes) {
   const size_t bytes = esize(prec) * d.n();
   int rc;
   for (int i = 0; i < 3; i++) {
@@ -151,11 +151,11 @@ int vector_cross(const void* const a[3], const void* const b[3], void* const out
              "cross copy")))
       return rc;
   }
-  if ((rc = fft3d(scratch, 6, d.nx, d.ny, d.nz, +1, PASS_SCALE, prec, s))) return rc;
+  if ((rc = fft3d(scratch, 6, d.nx, d.ny, d.nz, +1, PASS_SCALE, prec, s, tw_axes))) return rc;
   const void* u[3] = {scratch[0], scratch[1], scratch[2]};
   const void* w[3] = {scratch[3], scratch[4], scratch[5]};
   if ((rc = op_cross_pointwise(u, w, out, d.n(), prec, s))) return rc;
-  return fft3d(out, 3, d.nx, d.ny, d.nz, -1, PASS_ZERO_NYQUIST, prec, s);
+  return fft3d(out, 3, d.nx, d.ny, d.nz, -1, PASS_ZERO_NYQUIST, prec, s, tw_axes);
 }
 
 }  // namespace sns

@@ -8,6 +8,7 @@
 // applied.  Tiles are disjoint, so passes run in place; the reference's
 // transpose buffer (`tmp`, src/Scalar.cpp:113-122) is not needed.
 #include <math.h>
+#include <string.h>
 
 #include <map>
 #include <mutex>
@@ -46,6 +47,25 @@ static void cis_octant(int64_t m, int64_t n, double* c, double* s) {
   *s = y;
 }
 
+void twiddle_host_table(int L, int prec, std::vector<unsigned char>& out) {
+  std::vector<double> tab(2 * (size_t)L);
+  for (int m = 0; m < L; m++) {
+    double c, s;
+    cis_octant(m, L, &c, &s);
+    tab[2 * m] = c;
+    tab[2 * m + 1] = -s;  // exp(-i 2 pi m / L)
+  }
+  if (prec == PREC_C128) {
+    out.resize(sizeof(double) * tab.size());
+    memcpy(out.data(), tab.data(), out.size());
+  } else {
+    std::vector<float> f(tab.size());
+    for (size_t i = 0; i < tab.size(); i++) f[i] = (float)tab[i];
+    out.resize(sizeof(float) * f.size());
+    memcpy(out.data(), f.data(), out.size());
+  }
+}
+
 const void* twiddles(int L, int prec) {
   static std::mutex mu;
   static std::map<std::tuple<int, int, int>, void*> cache;
@@ -55,26 +75,11 @@ const void* twiddles(int L, int prec) {
   auto key = std::make_tuple(dev, L, prec);
   auto it = cache.find(key);
   if (it != cache.end()) return it->second;
-  std::vector<double> tab(2 * (size_t)L);
-  for (int m = 0; m < L; m++) {
-    double c, s;
-    cis_octant(m, L, &c, &s);
-    tab[2 * m] = c;
-    tab[2 * m + 1] = -s;  // exp(-i 2 pi m / L)
-  }
+  std::vector<unsigned char> tab;
+  twiddle_host_table(L, prec, tab);
   void* d = nullptr;
-  size_t bytes;
-  if (prec == PREC_C128) {
-    bytes = sizeof(double) * tab.size();
-    if (cudaMalloc(&d, bytes) != cudaSuccess) return nullptr;
-    cudaMemcpy(d, tab.data(), bytes, cudaMemcpyHostToDevice);
-  } else {
-    std::vector<float> f(tab.size());
-    for (size_t i = 0; i < tab.size(); i++) f[i] = (float)tab[i];
-    bytes = sizeof(float) * f.size();
-    if (cudaMalloc(&d, bytes) != cudaSuccess) return nullptr;
-    cudaMemcpy(d, f.data(), bytes, cudaMemcpyHostToDevice);
-  }
+  if (cudaMalloc(&d, tab.size()) != cudaSuccess) return nullptr;
+  cudaMemcpy(d, tab.data(), tab.size(), cudaMemcpyHostToDevice);
   cache[key] = d;
   return d;
 }
@@ -220,7 +225,8 @@ static int launch_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int fla
     if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_line_pass)");
     attr_set[dev & 63] = true;
   }
-  const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
+  const C* tw = reinterpret_cast<const C*>(
+      geo.tw ? geo.tw : twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
   if (!tw) {
     set_error("twiddle table allocation failed");
     return ERR_ALLOC;
@@ -340,7 +346,7 @@ LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec) {
 }
 
 int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int flags, int prec,
-          cudaStream_t stream) {
+          cudaStream_t stream, const void* const* tw_axes) {
   if (nx < 1 || ny < 1 || nz < 1 || nf < 1 || nf > kMaxFields) {
     set_error("fft3d: bad dimensions or field count");
     return ERR_ARG;
@@ -362,6 +368,7 @@ int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int fla
     if (dims[order[i]] > 1) axes[na++] = order[i];
   for (int i = 0; i < na; i++) {
     LineGeo g = axis_geo(axes[i], nx, ny, nz, prec);
+    if (tw_axes) g.tw = tw_axes[axes[i]];
     int fl = (i == na - 1) ? flags : 0;
     int rc = run_line_pass(g, f, sign, fl, 1.0 / N, prec, stream);
     if (rc) return rc;

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "sns_common.cuh"
 
 namespace sns {
@@ -36,6 +38,8 @@ struct LineGeo {
   // batches), used by the curl prologue and the Nyquist epilogue
   int nx, ny, nz;
   int axis;
+  // twiddle table to use instead of the cached one (null: cached table)
+  const void* tw;
 };
 
 struct FieldPtrs {
@@ -59,11 +63,15 @@ LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec);
 // Full 3D C2C transform of nf fields in place (the Scalar::transform
 // contract, src/Scalar.cpp:400-646), with optional fused Nyquist zeroing
 // (forward) and 1/N scaling (inverse).
+// tw_axes, when given, holds the twiddle table of each axis (x, y, z) to use
+// instead of the cached tables.
 int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int flags,
-          int prec, cudaStream_t stream);
+          int prec, cudaStream_t stream, const void* const* tw_axes = nullptr);
 
 // Device twiddle table exp(-2 pi i m / L), m < L, generated in FP64 on the
 // host and stored as complex64 or complex128 (cached per device).
 const void* twiddles(int L, int prec);
+// The same table as host bytes (L complex values of the precision).
+void twiddle_host_table(int L, int prec, std::vector<unsigned char>& out);
 
 }  // namespace sns

@@ -36,4 +36,10 @@ int op_average_abs(const void* f, int64_t n, int prec, double* partials, double*
                    cudaStream_t s);
 int reduce_partials_count();
 
+// Vector::cross on device fields (src/Vector.cpp:66-90) with six caller-given
+// work fields; tw_axes optionally supplies the twiddle table of each axis.
+int vector_cross(const void* const a[3], const void* const b[3], void* const out[3], Dims d,
+                 int prec, void* const scratch[6], cudaStream_t s,
+                 const void* const* tw_axes = nullptr);
+
 }  // namespace sns
