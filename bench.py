@@ -46,7 +46,17 @@ PASSES = {
     3: (["K1 z-inverse+curl", "K234 xy dataflow (y-inv x6, x cross, y-fwd x3)",
          "K5 z-forward+update"], [3 + 6, 6 + 3, 9 + 6]),
 }
-STEP_FIELDS = 30  # 9 FFTs x 2 + 12 for the spectral update
+STEP_FIELDS = 30  # 9 FFTs x 2 + 12 for the spectral update: 30 N^3 S per step
+
+# DRAM bytes (read + write) per launch of each pass at 256^3 complex64, from the
+# one-pass ncu capture summarised in profiles/ns_step_256_c64_launches.md.
+NCU_TRAFFIC = {
+    ("ns256_fp32", "K1 z-inverse+curl"): (403 + 790) * 1e6,
+    ("ns256_fp32", "K2 y-inverse x6"): (806 + 809) * 1e6,
+    ("ns256_fp32", "K3 x-inv+cross+x-fwd"): (805 + 365) * 1e6,
+    ("ns256_fp32", "K4 y-forward x3"): (403 + 374) * 1e6,
+    ("ns256_fp32", "K5 z-forward+update"): (1208 + 851) * 1e6,
+}
 
 WORKLOADS = {
     "ns256_fp32": dict(kind="ns", n=256, prec="c64"),
@@ -364,7 +374,8 @@ def run_b200(args, rank, world, local):
             metric=METRIC, value=value, unit="steps/s", ms_per_step=step_ms,
             dtype="fp32 bulk + fp64 reductions" if esz == 8 else "fp64",
             roofline={"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                      "frac": achieved / hbm, "traffic": None,
+                      "frac": achieved / hbm,
+                      "traffic": NCU_TRAFFIC.get((args.workload, PASS_NAMES[top])),
                       "kernel": PASS_NAMES[top],
                       "algorithmic_bytes_per_launch": alg,
                       "peak_source": f"{peak_src} hbm_gbs",
@@ -555,6 +566,17 @@ def secondary(S, torch, dev, stream, n, hbm):
         stream.synchronize()
         ms = e0.elapsed_time(e1) / 10
         out[f"fft{n}_{prec}_fwd_inv_gbs"] = 4 * n ** 3 * esz / (ms / 1e3) / 1e9
+        # comparison row only: the same transform pair through cuFFT (torch.fft)
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                x = torch.fft.ifftn(torch.fft.fftn(x))
+            e0.record(stream)
+            for _ in range(10):
+                x = torch.fft.ifftn(torch.fft.fftn(x))
+            e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1) / 10
+        out[f"cufft{n}_{prec}_fwd_inv_gbs_comparison"] = 4 * n ** 3 * esz / (ms / 1e3) / 1e9
         del x
     torch.cuda.empty_cache()
     return out

@@ -2,12 +2,13 @@
 // (src/FFT1D.cpp:95-101) and for the three 1D phases of Scalar::transform
 // (src/Scalar.cpp:419-566).  One kernel launch transforms every line along
 // one axis of up to six fields.  A CTA owns a tile of W adjacent lines x G
-// groups: it loads the tile with unit-stride (coalesced) global reads into
-// padded shared-memory rows, runs the register/shared Stockham line FFT, and
-// stores the tile back with the epilogue (1/N scaling, Nyquist zeroing)
-// applied.  Tiles are disjoint, so passes run in place; the reference's
-// transpose buffer (`tmp`, src/Scalar.cpp:113-122) is not needed.
+// groups: its threads load the tile straight into registers with coalesced
+// reads, run the register/shared-memory Stockham line FFT, and store the
+// tile back with the epilogue (1/N scaling, Nyquist zeroing) applied.  Tiles
+// are disjoint, so passes run in place; the reference's transpose buffer
+// (`tmp`, src/Scalar.cpp:113-122) is not needed.
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <map>
@@ -116,15 +117,12 @@ __device__ __forceinline__ LineCoord line_coord(const LineGeo& geo, int64_t base
 }
 
 // Element e of the thread's line as the prologue forms it.
-template <int PRO, typename C>
+template <int PRO, typename C, typename T>
 __device__ __forceinline__ C pro_load(const C* __restrict__ src, const C* __restrict__ v0,
                                       const C* __restrict__ v1, const C* __restrict__ v2,
-                                      int field, int64_t idx, int x, int y, int z,
-                                      const LineGeo& geo) {
+                                      int field, int64_t idx, T kx, T ky, T kz) {
   if constexpr (PRO == PRO_CURL6) {
     if (field < 3) return src[idx];
-    using T = decltype(C().x);
-    const T kx = (T)freq_i(x, geo.nx), ky = (T)freq_i(y, geo.ny), kz = (T)freq_i(z, geo.nz);
     if (field == 3) return csub(ikmul(ky, v2[idx]), ikmul(kz, v1[idx]));
     if (field == 4) return csub(ikmul(kz, v0[idx]), ikmul(kx, v2[idx]));
     return csub(ikmul(kx, v1[idx]), ikmul(ky, v0[idx]));
@@ -161,12 +159,16 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
     const C* __restrict__ v0 = reinterpret_cast<const C*>(f.in[0]);
     const C* __restrict__ v1 = reinterpret_cast<const C*>(f.in[1]);
     const C* __restrict__ v2 = reinterpret_cast<const C*>(f.in[2]);
+    // wavenumbers of the line: two are fixed, the one along the axis varies
+    const T kx0 = (T)freq_i(lc.x, geo.nx), ky0 = (T)freq_i(lc.y, geo.ny),
+            kz0 = (T)freq_i(lc.z, geo.nz);
+    const int naxis = geo.axis == 0 ? geo.nx : geo.axis == 1 ? geo.ny : geo.nz;
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const int p = j + TPL * e;
+      const T kp = (T)freq_i(j + TPL * e, naxis);
       v[e] = pro_load<PRO, C>(src, v0, v1, v2, field, lc.idx0 + e * lc.step,
-                              geo.axis == 0 ? p : lc.x, geo.axis == 1 ? p : lc.y,
-                              geo.axis == 2 ? p : lc.z, geo);
+                              geo.axis == 0 ? kp : kx0, geo.axis == 1 ? kp : ky0,
+                              geo.axis == 2 ? kp : kz0);
     }
   }
   line_fft<L, true>(v, row, j, tw, sg);
@@ -295,7 +297,12 @@ static void choose_tile(LineGeo& g, int64_t adjacent, int64_t groups, int prec) 
   const size_t esz = prec == PREC_C128 ? 16 : 8;
   const size_t smem_cap = 200 * 1024;
   int W = 1;
-  const int Wmax = prec == PREC_C128 ? 8 : 16;  // 128-byte runs
+  int Wmax = prec == PREC_C128 ? 8 : 16;  // 128-byte runs
+  // run-width override for tuning sweeps (SNS_LINE_W, a power of two)
+  if (const char* e = getenv("SNS_LINE_W")) {
+    const int v = atoi(e);
+    if (v >= 1 && (v & (v - 1)) == 0) Wmax = v;
+  }
   while (W * 2 <= Wmax && adjacent % (W * 2) == 0 && W * 2 * TPL <= max_threads(prec) &&
          (size_t)(W * 2) * row_stride(g.L) * esz <= smem_cap)
     W *= 2;

@@ -76,12 +76,18 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
   }
   __syncthreads();
 
-  // forward x on all rows (rows of fields 3..5 are discarded; keeping every
-  // thread on the same path keeps the block-wide syncs of long lines uniform)
+  // forward x of the three products.  Lines of up to 32 threads synchronise
+  // within their warp, so warps that hold only omega rows (every warp when G
+  // is a multiple of the lines per warp) skip it; longer lines synchronise the
+  // block and every thread takes part.
+  constexpr int kLinesPerWarp = TPL <= 32 ? 32 / TPL : 1;
+  const bool skip = (TPL <= 32) && (G % kLinesPerWarp == 0) && fld >= 3;
+  if (!skip) {
 #pragma unroll
-  for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
-  line_sync<TPL>();
-  line_fft<L>(v, row, j, tw, (T)-1);
+    for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
+    line_sync<TPL>();
+    line_fft<L>(v, row, j, tw, (T)-1);
+  }
 
   if (fld < 3) {
     C* __restrict__ dst = reinterpret_cast<C*>(f.out[fld]);
