@@ -69,7 +69,18 @@ WORKLOADS = {
     "fft128_c128": dict(kind="fft", n=128, prec="c128"),
     "fft256_c128": dict(kind="fft", n=256, prec="c128"),
     "fft512_c128": dict(kind="fft", n=512, prec="c128"),
+    "ens_config4": dict(kind="ens", n=128, prec="c64"),
 }
+# batched ensemble: 32 boxes of 32^3, 24 of 64^3 and 8 of 128^3, each with its
+# own spectrum-seeded field and nu log-uniform in [1/800, 1/100].  dt = 1e-3:
+# at the stated 2e-3 the AB2/CN scheme blows up in the 128^3 boxes of smallest
+# nu within about 200 steps (3 of 64 boxes non-finite after 205 steps), as it
+# does in FP64 at 128^3 and 256^3
+ENS_BOXES = [(32, 32), (64, 24), (128, 8)]
+ENS_DT = 1e-3
+ENS_NU_RANGE = (1.0 / 800, 1.0 / 100)
+ENS_STAGES = ["S1 z-inverse+curl", "S2 y-inverse x6", "S3 x-inv+cross+x-fwd", "S4 y-forward x3",
+              "S5 z-forward+update"]
 # config 3: nu = 1/400; dt = 5e-4 because the stated dt = 2e-3 makes the reference's
 # AB2/CN scheme diverge at 256^3 (FP64 energy -> NaN within 75 steps)
 NU, DT = 1.0 / 400, 5e-4
@@ -227,6 +238,41 @@ def cpu_fft_sample(n, budget_s=20.0):
                       f"{secs:.2f} s"}
 
 
+def _curl_np(Vh, n):
+    k = _k1d(n)
+    KZ, KY, KX = np.meshgrid(k, k, k, indexing="ij")
+    return [1j * (KY * Vh[2] - KZ * Vh[1]), 1j * (KZ * Vh[0] - KX * Vh[2]),
+            1j * (KX * Vh[1] - KY * Vh[0])]
+
+
+def cpu_ens_sample():
+    """The reference's ns.cpp loop body on the host cores, one warm-up and one
+    timed step per box size, weighted by the ensemble's box counts."""
+    from oracle import pyoracle as O
+    cores = os.cpu_count() or 1
+    have = O.have_ref()
+    if have:
+        O.ref(True).ref_set_threads(cores)
+    else:
+        os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    per = {}
+    for n, _ in ENS_BOXES:
+        Vh = initial_velocity_hat(n, 1)
+        w = _curl_np(Vh, n)
+        c0 = [np.zeros_like(Vh[0]) for _ in range(3)]
+        run = (lambda: O.ref_ns_steps(Vh, w, c0, NU, ENS_DT, 1)) if have else \
+            (lambda: O.port_ns_seconds(Vh, w, c0, NU, ENS_DT, 1))
+        run()
+        per[n] = run()
+    boxes = sum(c for _, c in ENS_BOXES)
+    secs = sum(c * per[n] for n, c in ENS_BOXES)
+    return {"value": boxes / secs, "unit": "box-steps/s", "cores": cores,
+            "kind": "reference" if have else "port",
+            "sample": "1 timed complex128 exec/ns.cpp loop-body step per box size (" +
+                      ", ".join(f"{n}^3: {per[n]:.3f} s" for n, _ in ENS_BOXES) +
+                      f") after 1 warm-up, weighted by the box counts, {cores} host threads"}
+
+
 # ---------------------------------------------------------------- reference arm
 def run_reference(args, rank, world):
     if rank != 0:
@@ -235,6 +281,22 @@ def run_reference(args, rank, world):
     wl = WORKLOADS[args.workload]
     n = wl["n"]
     cores = os.cpu_count() or 1
+    if wl["kind"] == "ens":
+        cb = cpu_ens_sample()
+        line = {
+            "impl": "reference", "metric": "NS ensemble box-steps/s (32x32^3 + 24x64^3 + 8x128^3)",
+            "value": cb["value"], "unit": cb["unit"], "n_gpus": world, "steps": 1, "warmup": 1,
+            "ms_per_step": 1000.0 * sum(c for _, c in ENS_BOXES) / cb["value"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": "ens_config4: boxes run one after another by the reference "
+                                   "loop body", "dt": ENS_DT},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return 0
     if wl["kind"] == "ns":
         Vh = initial_velocity_hat(n, 1)
         k = _k1d(n)
@@ -443,6 +505,19 @@ def run_b200(args, rank, world, local):
                "grid": f"{n}^3", "precision": wl["prec"], "parallelism": f"replicas x{world}",
                "l2": "no flush: 12 resident fields (%.2f GB) exceed the 126 MB L2" % (
                    12 * field_bytes / 1e9)}
+    elif wl["kind"] == "ens":
+        result.update(ens_bench(S, torch, dev, stream, args, world, rank, hbm, peak_src, clocks,
+                                barrier, max_over_ranks))
+        if rank == 0 and world == 1 and not args.no_cpu:
+            result["cpu_baseline"] = cpu_ens_sample()
+        cfg = {"workload": "ens_config4: 32 boxes of 32^3 + 24 of 64^3 + 8 of 128^3 "
+                           "(24,117,248 points), spectrum-seeded solenoidal field per box "
+                           "(distinct seeds), nu log-uniform in [1/800, 1/100], dt=1e-3 (2e-3 blows up "
+                           "in the 128^3 boxes of smallest nu), complex64",
+               "boxes": {f"{n}^3": c for n, c in ENS_BOXES}, "precision": "c64",
+               "parallelism": f"replicas x{world}",
+               "l2": "no flush: 12 resident fields per box (%.2f GB) exceed the 126 MB L2" % (
+                   12 * result["points"] * 8 / 1e9)}
     else:
         result.update(fft_bench(S, torch, dev, stream, n, dtype, esz, args, world, hbm, peak_src,
                                 clocks, barrier, max_over_ranks))
@@ -525,6 +600,124 @@ def fft_bench(S, torch, dev, stream, n, dtype, esz, args, world, hbm, peak_src, 
             "gpu_launches": 6 * args.steps,
             "e2e": {"value": world * alg * args.steps / (e2e_ms / 1e3) / 1e9, "unit": "GB/s",
                     "h2d_bytes_per_step": n ** 3 * esz, "d2h_bytes_per_step": n ** 3 * esz}}
+
+
+def ens_bench(S, torch, dev, stream, args, world, rank, hbm, peak_src, clocks, barrier,
+              max_over_ranks):
+    """Batched ensemble: one graph replay per ensemble step (five launches over
+    all boxes).  value = box-steps/s of all ranks; the sequential per-box
+    stepping of the same ensemble is timed beside it."""
+    from spectral_upcxx_b200 import ic
+    r = np.random.default_rng(4 + rank)
+    shapes = [(n, n, n) for n, c in ENS_BOXES for _ in range(c)]
+    lo, hi = np.log(ENS_NU_RANGE[0]), np.log(ENS_NU_RANGE[1])
+    nus = list(np.exp(r.uniform(lo, hi, len(shapes))))
+    points = int(sum(np.prod(s) for s in shapes))
+    esz = 8
+    host_ic = []
+    with torch.cuda.stream(stream):
+        ens = S.NSEnsemble(shapes, nus, ENS_DT, torch.complex64, tune=True, device=dev)
+        for b, s in enumerate(shapes):
+            Vd = [x.to(torch.complex64) for x in
+                  ic.solenoidal_spectrum_hat(s[0], 1000 * (rank + 1) + b, dev)]
+            wd = S.curl(Vd)
+            ens.bootstrap(b, Vd, wd)
+            host_ic.append(([x.cpu().pin_memory() for x in Vd], [x.cpu().pin_memory() for x in wd]))
+        ens.step(args.warmup)
+    stream.synchronize()
+    nb = len(shapes)
+    clocks.start()
+    time.sleep(0.3)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.time()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        ens.step(args.steps, S.ENS_GRAPH)
+        e1.record(stream)
+    stream.synchronize()
+    t1 = time.time()
+    barrier()
+    clocks.window(t0, t1)
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    time.sleep(0.2)
+    clocks.stop()
+    stats = ens.stats()
+    finite = sum(1 for s in stats if np.isfinite(s["energy"]))
+    # the same ensemble launched stage by stage, and box by box with the single-box kernels
+    alt = {}
+    k_alt = max(10, args.steps // 10)
+    for name, mode in (("eager", S.ENS_EAGER), ("sequential", S.ENS_SEQUENTIAL)):
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            ens.step(2, mode)
+            a0.record(stream)
+            ens.step(k_alt, mode)
+            a1.record(stream)
+        stream.synchronize()
+        alt[name] = max_over_ranks(a0.elapsed_time(a1)) / k_alt
+    stage_ms = ens.stage_times(20)
+    top = int(np.argmax(stage_ms))
+    fields = PASSES[5][1]
+    alg = fields[top] * points * esz
+    achieved = alg / (stage_ms[top] / 1e3) / 1e9
+    step_ms = ms / args.steps
+    step_bytes = STEP_FIELDS * points * esz
+    # e2e through the public API: upload every box's V0/omega0 from pinned host,
+    # bootstrap, K steps each followed by the per-box diagnostics read, download V1
+    out_V = [[torch.empty(s, dtype=torch.complex64).pin_memory() for _ in range(3)]
+             for s in shapes]
+    dev_ic = [([torch.empty(s, dtype=torch.complex64, device=dev) for _ in range(3)],
+               [torch.empty(s, dtype=torch.complex64, device=dev) for _ in range(3)])
+              for s in shapes]
+    barrier()
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        s0.record(stream)
+        for b in range(nb):
+            for a, h in zip(dev_ic[b][0] + dev_ic[b][1], host_ic[b][0] + host_ic[b][1]):
+                a.copy_(h, non_blocking=True)
+            ens.bootstrap(b, dev_ic[b][0], dev_ic[b][1])
+        for _ in range(args.steps):
+            ens.step(1, S.ENS_GRAPH)
+            ens.stats()  # per-box div.average() monitor (ns.cpp:210), D2H + sync
+        for b in range(nb):
+            for a, v in zip(out_V[b], ens.state(b)["V1"]):
+                a.copy_(v, non_blocking=True)
+        s1.record(stream)
+    stream.synchronize()
+    e2e_ms = max_over_ranks(s0.elapsed_time(s1))
+    tuning = ens.tuning()
+    ens.close()
+    del dev_ic
+    torch.cuda.empty_cache()
+    return {
+        "metric": "NS ensemble box-steps/s (32x32^3 + 24x64^3 + 8x128^3)",
+        "value": world * nb * args.steps / (ms / 1e3), "unit": "box-steps/s",
+        "ms_per_step": step_ms, "dtype": "fp32 bulk + fp64 reductions", "points": points,
+        "ensemble_steps_per_s": world * args.steps / (ms / 1e3),
+        "modes_ms_per_ensemble_step": {"graph": step_ms, **alt},
+        "speedup_vs_sequential": alt["sequential"] / step_ms,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None, "kernel": ENS_STAGES[top],
+                     "algorithmic_bytes_per_launch": alg, "peak_source": f"{peak_src} hbm_gbs",
+                     "step": {"algorithmic_bytes": step_bytes,
+                              "achieved_gbs": step_bytes / (step_ms / 1e3) / 1e9,
+                              "frac": step_bytes / (step_ms / 1e3) / 1e9 / hbm},
+                     "stages": [{"name": nm, "ms": t, "gbs": fields[i] * points * esz / (t / 1e3) / 1e9}
+                                for i, (nm, t) in enumerate(zip(ENS_STAGES, stage_ms))]},
+        "tuning": [{"threads": t, "line_run_cap": w, "persistent": p} for t, w, p in tuning],
+        "gpu_launches": args.steps * 5,
+        "diagnostics": {"boxes_finite": finite, "boxes": nb,
+                        "energy_min": min(s["energy"] for s in stats),
+                        "energy_max": max(s["energy"] for s in stats)},
+        "e2e": {"value": world * nb * args.steps / (e2e_ms / 1e3), "unit": "box-steps/s",
+                "h2d_bytes_per_step": 6 * points * esz / args.steps,
+                "d2h_bytes_per_step": (3 * points * esz + 32 * nb * args.steps) / args.steps,
+                "includes": "upload of V0/omega0 of every box from pinned host, bootstrap, K graph "
+                            "steps each with the per-box diagnostics read, download of every V1"},
+    }
 
 
 def secondary(S, torch, dev, stream, n, hbm):

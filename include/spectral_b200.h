@@ -181,6 +181,50 @@ int sns_ns_launches_per_step(sns_ns* handle);
 int sns_ns_profile(sns_ns* handle, int enable);
 int sns_ns_pass_times(sns_ns* handle, double* total_ms, int* launches, int max);
 
+/* ---- batched ensemble of NS boxes ----------------------------------------
+ * No reference counterpart: the reference runs one box per process
+ * (exec/ns.cpp).  An ensemble holds independent boxes of up to 8 distinct
+ * sizes (powers of two in [16, 256] per axis), each with its own viscosity,
+ * sharing dt and precision; every box follows the ns.cpp:132-217 sequence
+ * exactly as sns_ns does.  One ensemble step is five launches, one per stage,
+ * each over every box; SNS_ENS_GRAPH replays them as one captured CUDA graph,
+ * SNS_ENS_EAGER launches them directly, SNS_ENS_SEQUENTIAL steps the boxes one
+ * after another with the single-box stepper's kernels (a baseline). */
+typedef struct sns_ens sns_ens;
+#define SNS_ENS_GRAPH 0
+#define SNS_ENS_EAGER 1
+#define SNS_ENS_SEQUENTIAL 2
+/* dims: 3 per box (nx, ny, nz); nu: one per box.  tune != 0 times the
+ * candidate tile configurations of every stage on the ensemble (zeroed
+ * fields) and keeps the fastest; tune = 0 takes the first that fits. */
+int sns_ens_create(sns_ens** handle, int nboxes, const int64_t* dims, const double* nu, double dt,
+                   int prec, int tune, void* stream);
+int sns_ens_destroy(sns_ens* handle);
+/* Number of boxes. */
+int sns_ens_boxes(sns_ens* handle);
+/* Per-box counterparts of sns_ns_bootstrap / set_state / get_state. */
+int sns_ens_bootstrap(sns_ens* handle, int box, const void* const V0[3],
+                      const void* const omega0[3]);
+int sns_ens_set_state(sns_ens* handle, int box, const void* const V1[3],
+                      const void* const cross0[3]);
+int sns_ens_get_state(sns_ens* handle, int box, void* const V1[3], void* const omega1[3],
+                      void* const cross0[3]);
+/* Advance every box nsteps steps (mode: SNS_ENS_GRAPH, _EAGER, _SEQUENTIAL),
+ * queued on the ensemble's stream. */
+int sns_ens_step(sns_ens* handle, int nsteps, int mode);
+/* Diagnostics of every box after the last step, 4 doubles per box in the
+ * order of sns_ns_stats (div_avg, energy, enstrophy, max_div).  Synchronises. */
+int sns_ens_stats(sns_ens* handle, double* out);
+/* The configuration of each stage: threads per CTA, line-run cap, persistent
+ * grid (3 ints per stage into out[max]).  Returns the number of stages. */
+int sns_ens_tuning(sns_ens* handle, int* out, int max);
+/* Run nsteps ensemble steps with CUDA events between the stages (the state
+ * advances); ms[5] receives the mean milliseconds of each stage.  Synchronises
+ * and returns the number of stages. */
+int sns_ens_stage_times(sns_ens* handle, int nsteps, double* ms);
+/* Kernel launches per ensemble step in the given mode. */
+int sns_ens_launches_per_step(sns_ens* handle, int mode);
+
 #ifdef __cplusplus
 }
 #endif

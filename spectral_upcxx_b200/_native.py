@@ -73,6 +73,18 @@ SIGNATURES = {
     "sns_ns_launches_per_step": ([_vp], _int),
     "sns_ns_profile": ([_vp, _int], _int),
     "sns_ns_pass_times": ([_vp, C.POINTER(_dbl), C.POINTER(_int), _int], _int),
+    "sns_ens_create": ([C.POINTER(_vp), _int, C.POINTER(_i64), C.POINTER(_dbl), _dbl, _int, _int,
+                        _vp], _int),
+    "sns_ens_destroy": ([_vp], _int),
+    "sns_ens_boxes": ([_vp], _int),
+    "sns_ens_bootstrap": ([_vp, _int, _vp3, _vp3], _int),
+    "sns_ens_set_state": ([_vp, _int, _vp3, _vp3], _int),
+    "sns_ens_get_state": ([_vp, _int, _vp3, _vp3, _vp3], _int),
+    "sns_ens_step": ([_vp, _int, _int], _int),
+    "sns_ens_stats": ([_vp, C.POINTER(_dbl)], _int),
+    "sns_ens_tuning": ([_vp, C.POINTER(_int), _int], _int),
+    "sns_ens_launches_per_step": ([_vp, _int], _int),
+    "sns_ens_stage_times": ([_vp, _int, C.POINTER(_dbl)], _int),
 }
 
 _LIB = None

@@ -12,6 +12,7 @@
 #include "sns_common.cuh"
 #include "sns_fft.cuh"
 #include "sns_ns.cuh"
+#include "sns_ens.cuh"
 #include "sns_ops.cuh"
 
 namespace sns {
@@ -156,6 +157,34 @@ int vector_cross(const void* const a[3], const void* const b[3], void* const out
   const void* w[3] = {scratch[3], scratch[4], scratch[5]};
   if ((rc = op_cross_pointwise(u, w, out, d.n(), prec, s))) return rc;
   return fft3d(out, 3, d.nx, d.ny, d.nz, -1, PASS_ZERO_NYQUIST, prec, s, tw_axes);
+}
+
+// The bootstrap of ns.cpp:132-153 into V (-> V1) and C0 (-> cross0), with six
+// work fields U.
+int ns_bootstrap_fields(Dims d, int prec, double nu, double dt, const void* const V0[3],
+                        const void* const omega0[3], void* const V[3], void* const C0[3],
+                        void* const U[6], cudaStream_t s) {
+  const int64_t n = d.n();
+  int rc;
+  // cross0 = V0 x omega0 (ns.cpp:133, 137, 153)
+  if ((rc = vector_cross(V0, omega0, C0, d, prec, U, s))) return rc;
+  // t = cross0 + nu * laplacian(V0), held in V
+  if ((rc = op_vlaplacian(V0, V, d, prec, s))) return rc;
+  for (int i = 0; i < 3; i++) {
+    if ((rc = op_axpby(nu, V[i], 0.0, nullptr, V[i], n, prec, s))) return rc;
+    if ((rc = op_axpby(1.0, C0[i], 1.0, V[i], V[i], n, prec, s))) return rc;
+  }
+  // Pi0 = ilap(div t) (ns.cpp:133-134) in U[0]; grad Pi0 in U[1..3]
+  const void* t[3] = {V[0], V[1], V[2]};
+  if ((rc = op_divergence(t, U[0], d, prec, s))) return rc;
+  if ((rc = op_laplacian_inverse(U[0], 0.0, 1.0, d, prec, s))) return rc;
+  if ((rc = op_gradient(U[0], U[1], U[2], U[3], d, prec, s))) return rc;
+  // V1 = V0 + K (t - grad Pi0)  (ns.cpp:137)
+  for (int i = 0; i < 3; i++) {
+    if ((rc = op_axpby(1.0, V[i], -1.0, U[1 + i], V[i], n, prec, s))) return rc;
+    if ((rc = op_axpby(1.0, V0[i], dt, V[i], V[i], n, prec, s))) return rc;
+  }
+  return OK;
 }
 
 }  // namespace sns
@@ -432,11 +461,19 @@ int sns_mul(const void* a, const void* b, void* out, int64_t n, int prec, void* 
 // ---- fused stepper -------------------------------------------------------------
 int sns_ns_create(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double nu, double dt,
                   int prec, void* stream) {
+  return sns::ns_create_tuned(handle, nx, ny, nz, nu, dt, prec, stream, 0, 0);
+}
+
+}  // extern "C"
+
+// sns_ns_create with tile widths chosen by the ensemble's autotuner (0 = defaults).
+int sns::ns_create_tuned(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double nu,
+                         double dt, int prec, void* stream, int zW, int lineW) {
   if (!nonnull(handle, "sns_ns_create")) return ERR_ARG;
   *handle = nullptr;
   if (!check_prec(prec) || !check_dims(nx, ny, nz)) return ERR_ARG;
   sns_ns* h = new sns_ns();
-  int rc = ns_plan(h->pl, (int)nx, (int)ny, (int)nz, prec);
+  int rc = ns_plan(h->pl, (int)nx, (int)ny, (int)nz, prec, zW, lineW);
   if (rc) {
     delete h;
     return rc;
@@ -470,6 +507,8 @@ int sns_ns_create(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double nu
   *handle = h;
   return OK;
 }
+
+extern "C" {
 
 int sns_ns_destroy(sns_ns* h) {
   if (!h) return OK;
@@ -511,27 +550,8 @@ int sns_ns_bootstrap(sns_ns* h, const void* const V0[3], const void* const omega
       !vec_ok(omega0, "sns_ns_bootstrap"))
     return ERR_ARG;
   const Dims d{h->pl.nx, h->pl.ny, h->pl.nz};
-  const int prec = h->pl.prec;
-  const int64_t n = d.n();
-  int rc;
-  // cross0 = V0 x omega0 (ns.cpp:133, 137, 153)
-  if ((rc = vector_cross(V0, omega0, h->C0, d, prec, h->U, h->s))) return rc;
-  // t = cross0 + nu * laplacian(V0), held in V
-  if ((rc = op_vlaplacian(V0, h->V, d, prec, h->s))) return rc;
-  for (int i = 0; i < 3; i++) {
-    if ((rc = op_axpby(h->nu, h->V[i], 0.0, nullptr, h->V[i], n, prec, h->s))) return rc;
-    if ((rc = op_axpby(1.0, h->C0[i], 1.0, h->V[i], h->V[i], n, prec, h->s))) return rc;
-  }
-  // Pi0 = ilap(div t) (ns.cpp:133-134) in U[0]; grad Pi0 in U[1..3]
-  const void* t[3] = {h->V[0], h->V[1], h->V[2]};
-  if ((rc = op_divergence(t, h->U[0], d, prec, h->s))) return rc;
-  if ((rc = op_laplacian_inverse(h->U[0], 0.0, 1.0, d, prec, h->s))) return rc;
-  if ((rc = op_gradient(h->U[0], h->U[1], h->U[2], h->U[3], d, prec, h->s))) return rc;
-  // V1 = V0 + K (t - grad Pi0)  (ns.cpp:137)
-  for (int i = 0; i < 3; i++) {
-    if ((rc = op_axpby(1.0, h->V[i], -1.0, h->U[1 + i], h->V[i], n, prec, h->s))) return rc;
-    if ((rc = op_axpby(1.0, V0[i], h->dt, h->V[i], h->V[i], n, prec, h->s))) return rc;
-  }
+  int rc = ns_bootstrap_fields(d, h->pl.prec, h->nu, h->dt, V0, omega0, h->V, h->C0, h->U, h->s);
+  if (rc) return rc;
   h->stepped = false;
   return OK;
 }

@@ -17,6 +17,7 @@
 
 #include "sns_fft.cuh"
 #include "sns_fft_core.cuh"
+#include "sns_tiles.cuh"
 
 namespace sns {
 
@@ -85,109 +86,14 @@ const void* twiddles(int L, int prec) {
   return d;
 }
 
-// Thread layout of a tile of W adjacent lines x G groups: thread t owns line
-// (w, g) with w = t mod W, and within it positions j + e*TPL (e < E), where
-// s = t / W, j = s mod TPL, g = s / TPL.  Consecutive threads hold the same
-// position of adjacent lines (unit stride in memory) for W > 1, or adjacent
-// positions of one line for W = 1, so the direct global loads and stores are
-// coalesced and each thread has E independent loads in flight.  The line FFT
-// then starts from registers; shared memory only carries the exchanges
-// between radix stages.
-struct LineCoord {
-  int64_t idx0, step;  // global index of position j, stride between e
-  int x, y, z;         // coordinates of position j (3D fields)
-};
-
-__device__ __forceinline__ LineCoord line_coord(const LineGeo& geo, int64_t base, int w, int g,
-                                                int j, int tpl) {
-  LineCoord c;
-  c.idx0 = base + w + g * geo.gs + (int64_t)j * geo.ps;
-  c.step = (int64_t)tpl * geo.ps;
-  c.x = c.y = c.z = 0;
-  if (geo.axis >= 0) {
-    const int64_t nxy = (int64_t)geo.nx * geo.ny;
-    const int64_t z = c.idx0 / nxy;
-    const int64_t r = c.idx0 - z * nxy;
-    const int64_t y = r / geo.nx;
-    c.x = (int)(r - y * geo.nx);
-    c.y = (int)y;
-    c.z = (int)z;
-  }
-  return c;
-}
-
-// Element e of the thread's line as the prologue forms it.
-template <int PRO, typename C, typename T>
-__device__ __forceinline__ C pro_load(const C* __restrict__ src, const C* __restrict__ v0,
-                                      const C* __restrict__ v1, const C* __restrict__ v2,
-                                      int field, int64_t idx, T kx, T ky, T kz) {
-  if constexpr (PRO == PRO_CURL6) {
-    if (field < 3) return src[idx];
-    if (field == 3) return csub(ikmul(ky, v2[idx]), ikmul(kz, v1[idx]));
-    if (field == 4) return csub(ikmul(kz, v0[idx]), ikmul(kx, v2[idx]));
-    return csub(ikmul(kx, v1[idx]), ikmul(ky, v0[idx]));
-  } else {
-    return src[idx];
-  }
-}
-
+// One CTA per (field, tile); the tile body is in sns_tiles.cuh.
 template <typename T, int L, int PRO>
 __global__ void __launch_bounds__(MaxThreads<T>::value)
     k_line_pass(const LineGeo geo, const FieldPtrs f, const cx_t<T>* __restrict__ tw, T sg,
                 T scale, int flags, int wshift) {
-  using C = cx_t<T>;
-  using P = LinePlan<L>;
-  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(L);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* sm = reinterpret_cast<C*>(smem_raw);
-
-  const int nf = f.n;
-  const int field = blockIdx.x % nf;
-  const int64_t t = blockIdx.x / nf;
-  const int64_t base = (t % geo.TA) * geo.sa + (t / geo.TA) * geo.sb;
-  const int W = geo.W;
-  const int w = threadIdx.x & (W - 1);
-  const int s = threadIdx.x >> wshift;
-  const int j = s & (TPL - 1);
-  const int g = s / TPL;
-  C* row = sm + (w + W * g) * RS;
-  const LineCoord lc = line_coord(geo, base, w, g, j, TPL);
-
-  const C* __restrict__ src = reinterpret_cast<const C*>(f.in[field]);
-  C v[E];
-  {
-    const C* __restrict__ v0 = reinterpret_cast<const C*>(f.in[0]);
-    const C* __restrict__ v1 = reinterpret_cast<const C*>(f.in[1]);
-    const C* __restrict__ v2 = reinterpret_cast<const C*>(f.in[2]);
-    // wavenumbers of the line: two are fixed, the one along the axis varies
-    const T kx0 = (T)freq_i(lc.x, geo.nx), ky0 = (T)freq_i(lc.y, geo.ny),
-            kz0 = (T)freq_i(lc.z, geo.nz);
-    const int naxis = geo.axis == 0 ? geo.nx : geo.axis == 1 ? geo.ny : geo.nz;
-#pragma unroll
-    for (int e = 0; e < E; e++) {
-      const T kp = (T)freq_i(j + TPL * e, naxis);
-      v[e] = pro_load<PRO, C>(src, v0, v1, v2, field, lc.idx0 + e * lc.step,
-                              geo.axis == 0 ? kp : kx0, geo.axis == 1 ? kp : ky0,
-                              geo.axis == 2 ? kp : kz0);
-    }
-  }
-  line_fft<L, true>(v, row, j, tw, sg);
-
-  C* __restrict__ dst = reinterpret_cast<C*>(f.out[field]);
-  const bool do_scale = flags & PASS_SCALE;
-  const bool do_zero = flags & PASS_ZERO_NYQUIST;
-  const bool line_on_plane = (geo.axis != 0 && lc.x == (geo.nx >> 1)) ||
-                             (geo.axis != 1 && lc.y == (geo.ny >> 1)) ||
-                             (geo.axis != 2 && lc.z == (geo.nz >> 1));
-  const int half_axis = geo.axis == 0 ? (geo.nx >> 1) : geo.axis == 1 ? (geo.ny >> 1)
-                                                                      : (geo.nz >> 1);
-#pragma unroll
-  for (int e = 0; e < E; e++) {
-    C val = v[e];
-    if (do_scale) val = cscale(scale, val);
-    if (do_zero && (line_on_plane || j + TPL * e == half_axis)) val = mk((T)0, (T)0);
-    dst[lc.idx0 + e * lc.step] = val;
-  }
+  line_pass_tile<T, L, PRO>(geo, ParamFields{f}, f.n, tw, sg, scale, flags, wshift,
+                            (int64_t)blockIdx.x, reinterpret_cast<cx_t<T>*>(smem_raw));
 }
 
 // epilogue-only pass (used when every axis has length 1)
@@ -292,14 +198,15 @@ int run_line_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags, d
 static int elems_per_thread(int L) { return L >= 16 ? 16 : L; }
 
 // Choose W adjacent lines and G groups for a pass of line length L.
-static void choose_tile(LineGeo& g, int64_t adjacent, int64_t groups, int prec) {
+static void choose_tile(LineGeo& g, int64_t adjacent, int64_t groups, int prec, int wmax) {
   const int TPL = g.L / elems_per_thread(g.L);
   const size_t esz = prec == PREC_C128 ? 16 : 8;
   const size_t smem_cap = 200 * 1024;
   int W = 1;
   int Wmax = prec == PREC_C128 ? 8 : 16;  // 128-byte runs
+  if (wmax > 0) Wmax = wmax;  // a tuned width
   // run-width override for tuning sweeps (SNS_LINE_W, a power of two)
-  if (const char* e = getenv("SNS_LINE_W")) {
+  if (const char* e = wmax > 0 ? nullptr : getenv("SNS_LINE_W")) {
     const int v = atoi(e);
     if (v >= 1 && (v & (v - 1)) == 0) Wmax = v;
   }
@@ -314,7 +221,7 @@ static void choose_tile(LineGeo& g, int64_t adjacent, int64_t groups, int prec) 
   g.G = G;
 }
 
-LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec) {
+LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec, int wmax) {
   LineGeo g{};
   g.nx = nx;
   g.axis = axis;
@@ -325,7 +232,7 @@ LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec) {
     g.L = nx;
     g.ps = 1;
     g.gs = nx;
-    choose_tile(g, 1, (int64_t)ny * nz, prec);
+    choose_tile(g, 1, (int64_t)ny * nz, prec, wmax);
     g.TA = (int64_t)ny * nz / g.G;
     g.TB = 1;
     g.sa = (int64_t)g.G * nx;
@@ -334,7 +241,7 @@ LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec) {
     g.L = ny;
     g.ps = nx;
     g.gs = nxy;
-    choose_tile(g, nx, nz, prec);
+    choose_tile(g, nx, nz, prec, wmax);
     g.TA = nx / g.W;
     g.TB = nz / g.G;
     g.sa = g.W;
@@ -343,7 +250,7 @@ LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec) {
     g.L = nz;
     g.ps = nxy;
     g.gs = nx;
-    choose_tile(g, nx, ny, prec);
+    choose_tile(g, nx, ny, prec, wmax);
     g.TA = nx / g.W;
     g.TB = ny / g.G;
     g.sa = g.W;

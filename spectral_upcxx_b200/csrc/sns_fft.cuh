@@ -58,7 +58,8 @@ int run_line_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags, d
                   int prec, cudaStream_t stream, int prologue = PRO_LOAD);
 
 // Geometry of the lines along `axis` (0 = x, 1 = y, 2 = z) of nx*ny*nz fields.
-LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec);
+// wmax > 0 caps the adjacent lines per tile at that width (a tuned value).
+LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec, int wmax = 0);
 
 // Full 3D C2C transform of nf fields in place (the Scalar::transform
 // contract, src/Scalar.cpp:400-646), with optional fused Nyquist zeroing

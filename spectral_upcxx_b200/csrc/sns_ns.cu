@@ -25,6 +25,7 @@
 #include "sns_fft_core.cuh"
 #include "sns_ns.cuh"
 #include "sns_ops.cuh"
+#include "sns_tiles.cuh"
 
 namespace sns {
 
@@ -33,243 +34,21 @@ namespace sns {
 template <typename T, int L>
 __global__ void __launch_bounds__(MaxThreads<T>::value)
     k_xcross(FieldPtrs f, const cx_t<T>* __restrict__ tw, int G, T scale2) {
-  using C = cx_t<T>;
-  using P = LinePlan<L>;
-  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(L);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* sm = reinterpret_cast<C*>(smem_raw);
-  const int64_t row0 = (int64_t)blockIdx.x * G;
-  const int per = G * L;
-
-  // thread t owns line t / TPL (field-major: field = line / G, row = line % G)
-  // at positions j + e*TPL; loads go straight to registers, E per thread
-  const int j = threadIdx.x % TPL, line = threadIdx.x / TPL;
-  const int fld = line / G, gl = line - fld * G;
-  C* row = sm + line * RS;
-  C v[E];
-  {
-    const C* __restrict__ src = reinterpret_cast<const C*>(f.in[fld]);
-    const int64_t i0 = (row0 + gl) * L + j;
-#pragma unroll
-    for (int e = 0; e < E; e++) v[e] = src[i0 + TPL * e];
-  }
-  line_fft<L>(v, row, j, tw, (T)1);
-#pragma unroll
-  for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
-  __syncthreads();
-
-  // c = (u/N) x (omega/N): u in rows of fields 0..2, omega in 3..5
-  for (int q = threadIdx.x; q < per; q += blockDim.x) {
-    const int g = q / L, p = q & (L - 1);
-    C u[3], w[3];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      u[d] = sm[(d * G + g) * RS + pad_pos(p)];
-      w[d] = sm[((3 + d) * G + g) * RS + pad_pos(p)];
-    }
-    const C c0 = csub(cmul(u[1], w[2]), cmul(u[2], w[1]));
-    const C c1 = csub(cmul(u[2], w[0]), cmul(u[0], w[2]));
-    const C c2 = csub(cmul(u[0], w[1]), cmul(u[1], w[0]));
-    sm[(0 * G + g) * RS + pad_pos(p)] = cscale(scale2, c0);
-    sm[(1 * G + g) * RS + pad_pos(p)] = cscale(scale2, c1);
-    sm[(2 * G + g) * RS + pad_pos(p)] = cscale(scale2, c2);
-  }
-  __syncthreads();
-
-  // forward x of the three products.  Lines of up to 32 threads synchronise
-  // within their warp, so warps that hold only omega rows (every warp when G
-  // is a multiple of the lines per warp) skip it; longer lines synchronise the
-  // block and every thread takes part.
-  constexpr int kLinesPerWarp = TPL <= 32 ? 32 / TPL : 1;
-  const bool skip = (TPL <= 32) && (G % kLinesPerWarp == 0) && fld >= 3;
-  if (!skip) {
-#pragma unroll
-    for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
-    line_sync<TPL>();
-    line_fft<L>(v, row, j, tw, (T)-1);
-  }
-
-  if (fld < 3) {
-    C* __restrict__ dst = reinterpret_cast<C*>(f.out[fld]);
-    const int64_t i0 = (row0 + gl) * L + j;
-#pragma unroll
-    for (int e = 0; e < E; e++) dst[i0 + TPL * e] = v[e];
-  }
+  xcross_tile<T, L>(ParamFields{f}, tw, G, scale2, (int64_t)blockIdx.x, (int)blockDim.x,
+                    reinterpret_cast<cx_t<T>*>(smem_raw));
 }
 
 // ---------------------------------------------------------------------------
 // K5: z lines -- forward 3 fields + Nyquist zeroing, then the AB2 /
 // projection / CN update per mode.
-struct UpdateArgs {
-  const void* U[3];  // cross1 after x, y forward passes
-  void* V[3];        // in: V1, out: V (new)
-  void* C0[3];       // in: cross0, out: cross1
-  int nx, ny, nz;
-  int W;
-  double hK;      // K/2
-  double nuhK;    // nu*K/2
-  double* stats;  // per block: sum|div|, sum|V|^2, sum|k x V|^2, max|div|
-};
-
 template <typename T, int L>
 __global__ void __launch_bounds__(MaxThreads<T>::value)
     k_zfwd_update(const UpdateArgs a, const cx_t<T>* __restrict__ tw) {
-  using C = cx_t<T>;
-  using P = LinePlan<L>;
-  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(L);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* sm = reinterpret_cast<C*>(smem_raw);
   __shared__ double red[4][32];
-
-  const int W = a.W;
-  const int tiles_x = a.nx / W;
-  const int x0 = (blockIdx.x % tiles_x) * W;
-  const int y = blockIdx.x / tiles_x;
-  const int64_t nxy = (int64_t)a.nx * a.ny;
-  const int64_t base = x0 + (int64_t)a.nx * y;
-  const int per = W * L;
-
-  // thread t owns z line (field, x0 + w) at positions j + e*TPL with
-  // w = t mod W, j = (t / W) mod TPL, field = t / (W*TPL): consecutive threads
-  // load adjacent x, so the direct loads are coalesced
-  {
-    const int w = threadIdx.x % W, s = threadIdx.x / W;
-    const int j = s % TPL, fld = s / TPL;
-    C* row = sm + (fld * W + w) * RS;
-    const C* __restrict__ src = reinterpret_cast<const C*>(a.U[fld]);
-    const int64_t i0 = base + w + nxy * j;
-    C v[E];
-#pragma unroll
-    for (int e = 0; e < E; e++) v[e] = src[i0 + nxy * (TPL * e)];
-    line_fft<L, true>(v, row, j, tw, (T)-1);
-#pragma unroll
-    for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
-  }
-  __syncthreads();
-
-  const T hK = (T)a.hK, nuhK = (T)a.nuhK;
-  const T ky = (T)freq_i(y, a.ny);
-  const bool ynyq = (y == (a.ny >> 1));
-  double s_div = 0, s_e = 0, s_w = 0, m_div = 0;
-  C* __restrict__ Vp[3] = {reinterpret_cast<C*>(a.V[0]), reinterpret_cast<C*>(a.V[1]),
-                           reinterpret_cast<C*>(a.V[2])};
-  C* __restrict__ Cp[3] = {reinterpret_cast<C*>(a.C0[0]), reinterpret_cast<C*>(a.C0[1]),
-                           reinterpret_cast<C*>(a.C0[2])};
-  auto update_point = [&](int q, const C (&V1)[3], const C (&c0)[3]) {
-    const int w = q % W, z = q / W;
-    const int x = x0 + w;
-    const int64_t idx = base + w + nxy * z;
-    const T kx = (T)freq_i(x, a.nx), kz = (T)freq_i(z, a.nz);
-    const bool nyq = ynyq || x == (a.nx >> 1) || z == (a.nz >> 1);
-    C c1[3];
-#pragma unroll
-    for (int d = 0; d < 3; d++) c1[d] = nyq ? mk((T)0, (T)0) : sm[(d * W + w) * RS + pad_pos(z)];
-    const T kk[3] = {kx, ky, kz};
-    const T k2 = kx * kx + ky * ky + kz * kz;
-    const double k2d = (double)kx * kx + (double)ky * ky + (double)kz * kz;
-    // F = K/2 (3 c1 - c0)                      (ns.cpp:171)
-    // lap1 = nu K/2 (-|k|^2 V1)                (ns.cpp:174)
-    // s = V1 + lap1 + F; G = div s / (-|k|^2)  (ns.cpp:177-178)
-    C F[3], lap[3], s[3];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      F[d] = cscale(hK, csub(cscale((T)3, c1[d]), c0[d]));
-      lap[d] = cscale(nuhK, cscale(-k2, V1[d]));
-      s[d] = cadd(cadd(V1[d], lap[d]), F[d]);
-    }
-    C G = cadd(cadd(ikmul(kx, s[0]), ikmul(ky, s[1])), ikmul(kz, s[2]));
-    // The divisors -|k|^2 (projection) and 1 + nu K/2 |k|^2 (Crank-Nicolson)
-    // are formed in FP64.  complex128 divides as the reference does; complex64
-    // multiplies by the FP64 reciprocals rounded once to FP32.
-    const bool nonzero = k2d != 0.0;
-    const double den_cn = 1.0 + a.nuhK * k2d;
-    T r_p = (T)1, r_cn = (T)1;
-    if constexpr (sizeof(T) == 4) {
-      if (nonzero) {
-        r_p = (T)(-1.0 / k2d);
-        r_cn = (T)(1.0 / den_cn);
-      }
-      G = cscale(r_p, G);
-    } else {
-      if (nonzero) G = mk(G.x / -k2d, G.y / -k2d);
-    }
-    // Vhalf = V1 + F - grad G; V = (Vhalf + lap1) / (1 + nu K/2 |k|^2)  (ns.cpp:181-187)
-    C Vn[3];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      C vh = csub(cadd(V1[d], F[d]), ikmul(kk[d], G));
-      C vv = cadd(vh, lap[d]);
-      if constexpr (sizeof(T) == 4) {
-        vv = cscale(r_cn, vv);
-      } else {
-        if (nonzero) vv = mk(vv.x / den_cn, vv.y / den_cn);
-      }
-      Vn[d] = vv;
-      Vp[d][idx] = vv;
-      Cp[d][idx] = c1[d];
-    }
-    // diagnostics of the new velocity: per-mode terms in T, sums in FP64
-    const C dv = cadd(cadd(ikmul(kx, Vn[0]), ikmul(ky, Vn[1])), ikmul(kz, Vn[2]));
-    const double ad = (double)sqrt(dv.x * dv.x + dv.y * dv.y);
-    s_div += ad;
-    m_div = fmax(m_div, ad);
-    T e2 = 0;
-#pragma unroll
-    for (int d = 0; d < 3; d++) e2 += Vn[d].x * Vn[d].x + Vn[d].y * Vn[d].y;
-    const C om0 = csub(ikmul(ky, Vn[2]), ikmul(kz, Vn[1]));
-    const C om1 = csub(ikmul(kz, Vn[0]), ikmul(kx, Vn[2]));
-    const C om2 = csub(ikmul(kx, Vn[1]), ikmul(ky, Vn[0]));
-    const T w2 = om0.x * om0.x + om0.y * om0.y + om1.x * om1.x + om1.y * om1.y +
-                 om2.x * om2.x + om2.y * om2.y;
-    s_e += (double)e2;
-    s_w += (double)w2;
-  };
-  // two points per iteration: the 12 global loads of both are issued first
-  for (int q0 = threadIdx.x; q0 < per; q0 += 2 * blockDim.x) {
-    const int q1 = q0 + blockDim.x;
-    const bool has1 = q1 < per;
-    C V1a[3], c0a[3], V1b[3], c0b[3];
-    const int64_t ia = base + (q0 % W) + nxy * (q0 / W);
-    const int64_t ib = has1 ? base + (q1 % W) + nxy * (q1 / W) : ia;
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      V1a[d] = Vp[d][ia];
-      c0a[d] = Cp[d][ia];
-      V1b[d] = Vp[d][ib];
-      c0b[d] = Cp[d][ib];
-    }
-    update_point(q0, V1a, c0a);
-    if (has1) update_point(q1, V1b, c0b);
-  }
-  // block reduction of the diagnostics
-  for (int o = 16; o > 0; o >>= 1) {
-    s_div += __shfl_xor_sync(0xffffffffu, s_div, o);
-    s_e += __shfl_xor_sync(0xffffffffu, s_e, o);
-    s_w += __shfl_xor_sync(0xffffffffu, s_w, o);
-    m_div = fmax(m_div, __shfl_xor_sync(0xffffffffu, m_div, o));
-  }
-  const int warp = threadIdx.x >> 5, nwarps = (blockDim.x + 31) >> 5;
-  if ((threadIdx.x & 31) == 0) {
-    red[0][warp] = s_div;
-    red[1][warp] = s_e;
-    red[2][warp] = s_w;
-    red[3][warp] = m_div;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
-    for (int i = 0; i < nwarps; i++) {
-      t0 += red[0][i];
-      t1 += red[1][i];
-      t2 += red[2][i];
-      t3 = fmax(t3, red[3][i]);
-    }
-    double* out = a.stats + 4 * (int64_t)blockIdx.x;
-    out[0] = t0;
-    out[1] = t1;
-    out[2] = t2;
-    out[3] = t3;
-  }
+  zfwd_update_tile<T, L>(a, tw, (int64_t)blockIdx.x, (int)blockDim.x,
+                         reinterpret_cast<cx_t<T>*>(smem_raw), red);
 }
 
 __global__ void k_stats_final(const double* part, int blocks, double* out) {
@@ -383,7 +162,7 @@ int elems(int L) { return L >= 16 ? 16 : L; }
 
 }  // namespace
 
-int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec) {
+int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW) {
   pl = NSPlan{};
   pl.nx = nx;
   pl.ny = ny;
@@ -413,8 +192,9 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec) {
     const int TPL = nz / elems(nz);
     int W = 1;
     int Wmax = prec == PREC_C128 ? 8 : 16;
+    if (zW > 0) Wmax = zW;  // a tuned width
     // tile width override for tuning sweeps (SNS_Z_W, a power of two)
-    if (const char* e = getenv("SNS_Z_W")) {
+    if (const char* e = zW > 0 ? nullptr : getenv("SNS_Z_W")) {
       const int v = atoi(e);
       if (v >= 1 && (v & (v - 1)) == 0) Wmax = v;
     }
@@ -435,6 +215,7 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec) {
   pl.xy_chunk = 0;
   if (const char* e = getenv("SNS_XY_CHUNK")) pl.xy_chunk = atoi(e);
   pl.passes = (pl.use_xy || (pl.xy_chunk > 0 && pl.xy_chunk < nz)) ? 3 : 5;
+  pl.lineW = lineW > 0 ? lineW : 0;
   return OK;
 }
 
@@ -455,7 +236,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     f.n = 6;
     for (int d = 0; d < 3; d++) f.in[d] = V[d];
     for (int i = 0; i < 6; i++) f.out[i] = U[i];
-    LineGeo g = axis_geo(2, nx, ny, nz, prec);
+    LineGeo g = axis_geo(2, nx, ny, nz, prec, pl.lineW);
     if ((rc = run_line_pass(g, f, +1, 0, 1.0, prec, s, PRO_CURL6))) return rc;
     mark();
   }
@@ -475,7 +256,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
       FieldPtrs f{};
       f.n = 6;
       for (int i = 0; i < 6; i++) f.in[i] = f.out[i] = Uc[i];
-      LineGeo g = axis_geo(1, nx, ny, pz, prec);
+      LineGeo g = axis_geo(1, nx, ny, pz, prec, pl.lineW);
       int r = run_line_pass(g, f, +1, 0, 1.0, prec, s);
       if (r) return r;
       if (marks) mark();
@@ -494,7 +275,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
       FieldPtrs f{};
       f.n = 3;
       for (int i = 0; i < 3; i++) f.in[i] = f.out[i] = Uc[i];
-      LineGeo g = axis_geo(1, nx, ny, pz, prec);
+      LineGeo g = axis_geo(1, nx, ny, pz, prec, pl.lineW);
       int r = run_line_pass(g, f, -1, 0, 1.0, prec, s);
       if (r) return r;
     }
@@ -522,6 +303,8 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     a.ny = ny;
     a.nz = nz;
     a.W = pl.zW;
+    a.lx = 0;
+    while ((1 << a.lx) < nx) a.lx++;
     a.hK = dt / 2;
     a.nuhK = nu * dt / 2;
     a.stats = stats;

@@ -15,10 +15,12 @@ struct NSPlan {
   bool use_xy;        // xy phase as one persistent dataflow launch
   XYPlan xy;
   int xy_chunk;       // planes per slab of the separate xy passes (0 = all)
+  int lineW;          // adjacent lines per tile of the y/z line passes (0 = default)
   int passes;         // timed phases per step: z-inverse, xy, z-forward+update
 };
 
-int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec);
+// zW > 0 and lineW > 0 select tuned tile widths (0 = defaults).
+int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW = 0, int lineW = 0);
 // One step in place on V (Fourier velocity) and C0 (previous cross product),
 // with six work fields U; per-block diagnostics go to `stats`
 // (4 doubles x update_blocks).

@@ -1,0 +1,377 @@
+// Tile bodies of the transform and Navier-Stokes passes.
+//
+// A tile body does the work of one CTA given its tile index `blk`, the CTA's
+// thread count and its shared memory.  The single-field kernels (sns_fft.cu,
+// sns_ns.cu) call them with blockIdx.x; the ensemble kernels (sns_ens.cu)
+// call them for a (box, tile) pair taken from the ensemble's work list, so a
+// box advanced inside an ensemble sees the same arithmetic as a box advanced
+// alone.  Field pointers come through an accessor (`in(i)`, `out(i)`) so that
+// neither caller copies its pointer table to local memory.
+#pragma once
+
+#include "sns_fft.cuh"
+#include "sns_fft_core.cuh"
+
+namespace sns {
+
+// ---------------------------------------------------------------------------
+// Line passes (src/Scalar.cpp:419-566 per axis, src/FFT1D.cpp:95-101 per line)
+//
+// Thread layout of a tile of W adjacent lines x G groups: thread t owns line
+// (w, g) with w = t mod W, and within it positions j + e*TPL (e < E), where
+// s = t / W, j = s mod TPL, g = s / TPL.  Consecutive threads hold the same
+// position of adjacent lines (unit stride in memory) for W > 1, or adjacent
+// positions of one line for W = 1, so the direct global loads and stores are
+// coalesced and each thread has E independent loads in flight.  The line FFT
+// then starts from registers; shared memory only carries the exchanges
+// between radix stages.
+struct LineCoord {
+  int64_t idx0, step;  // global index of position j, stride between e
+  int x, y, z;         // coordinates of position j (3D fields)
+};
+
+__device__ __forceinline__ LineCoord line_coord(const LineGeo& geo, int64_t base, int w, int g,
+                                                int j, int tpl) {
+  LineCoord c;
+  c.idx0 = base + w + g * geo.gs + (int64_t)j * geo.ps;
+  c.step = (int64_t)tpl * geo.ps;
+  c.x = c.y = c.z = 0;
+  if (geo.axis >= 0) {
+    const int64_t nxy = (int64_t)geo.nx * geo.ny;
+    const int64_t z = c.idx0 / nxy;
+    const int64_t r = c.idx0 - z * nxy;
+    const int64_t y = r / geo.nx;
+    c.x = (int)(r - y * geo.nx);
+    c.y = (int)y;
+    c.z = (int)z;
+  }
+  return c;
+}
+
+// Element of the thread's line as the prologue forms it.
+template <int PRO, typename C, typename T>
+__device__ __forceinline__ C pro_load(const C* __restrict__ src, const C* __restrict__ v0,
+                                      const C* __restrict__ v1, const C* __restrict__ v2,
+                                      int field, int64_t idx, T kx, T ky, T kz) {
+  if constexpr (PRO == PRO_CURL6) {
+    if (field < 3) return src[idx];
+    if (field == 3) return csub(ikmul(ky, v2[idx]), ikmul(kz, v1[idx]));
+    if (field == 4) return csub(ikmul(kz, v0[idx]), ikmul(kx, v2[idx]));
+    return csub(ikmul(kx, v1[idx]), ikmul(ky, v0[idx]));
+  } else {
+    return src[idx];
+  }
+}
+
+// One tile of a line pass: field `blk mod nf`, tile `blk / nf` of `geo`.
+template <typename T, int L, int PRO, typename Fields>
+__device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields& f, int nf,
+                                               const cx_t<T>* __restrict__ tw, T sg, T scale,
+                                               int flags, int wshift, int64_t blk,
+                                               cx_t<T>* sm) {
+  using C = cx_t<T>;
+  using P = LinePlan<L>;
+  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(L);
+
+  const int field = (int)(blk % nf);
+  const int64_t t = blk / nf;
+  const int64_t base = (t % geo.TA) * geo.sa + (t / geo.TA) * geo.sb;
+  const int W = geo.W;
+  const int w = threadIdx.x & (W - 1);
+  const int s = threadIdx.x >> wshift;
+  const int j = s & (TPL - 1);
+  const int g = s / TPL;
+  C* row = sm + (w + W * g) * RS;
+  const LineCoord lc = line_coord(geo, base, w, g, j, TPL);
+
+  C v[E];
+  {
+    const C* __restrict__ src = reinterpret_cast<const C*>(f.in(field));
+    const C* __restrict__ v0 = nullptr;
+    const C* __restrict__ v1 = nullptr;
+    const C* __restrict__ v2 = nullptr;
+    if constexpr (PRO == PRO_CURL6) {
+      v0 = reinterpret_cast<const C*>(f.in(0));
+      v1 = reinterpret_cast<const C*>(f.in(1));
+      v2 = reinterpret_cast<const C*>(f.in(2));
+    }
+    // wavenumbers of the line: two are fixed, the one along the axis varies
+    const T kx0 = (T)freq_i(lc.x, geo.nx), ky0 = (T)freq_i(lc.y, geo.ny),
+            kz0 = (T)freq_i(lc.z, geo.nz);
+    const int naxis = geo.axis == 0 ? geo.nx : geo.axis == 1 ? geo.ny : geo.nz;
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const T kp = (T)freq_i(j + TPL * e, naxis);
+      v[e] = pro_load<PRO, C>(src, v0, v1, v2, field, lc.idx0 + e * lc.step,
+                              geo.axis == 0 ? kp : kx0, geo.axis == 1 ? kp : ky0,
+                              geo.axis == 2 ? kp : kz0);
+    }
+  }
+  line_fft<L, true>(v, row, j, tw, sg);
+
+  C* __restrict__ dst = reinterpret_cast<C*>(f.out(field));
+  const bool do_scale = flags & PASS_SCALE;
+  const bool do_zero = flags & PASS_ZERO_NYQUIST;
+  const bool line_on_plane = (geo.axis != 0 && lc.x == (geo.nx >> 1)) ||
+                             (geo.axis != 1 && lc.y == (geo.ny >> 1)) ||
+                             (geo.axis != 2 && lc.z == (geo.nz >> 1));
+  const int half_axis = geo.axis == 0 ? (geo.nx >> 1) : geo.axis == 1 ? (geo.ny >> 1)
+                                                                      : (geo.nz >> 1);
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    C val = v[e];
+    if (do_scale) val = cscale(scale, val);
+    if (do_zero && (line_on_plane || j + TPL * e == half_axis)) val = mk((T)0, (T)0);
+    dst[lc.idx0 + e * lc.step] = val;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K3 of the NS step: x lines -- inverse 6 fields, 1/N^2-scaled complex cross
+// product u x omega, forward 3 fields (src/Vector.cpp:79-89).  A tile is G
+// rows of all six fields; f.in(0..5) = (u, omega), f.out(0..2) = the product.
+template <typename T, int L, typename Fields>
+__device__ __forceinline__ void xcross_tile(const Fields& f, const cx_t<T>* __restrict__ tw, int G,
+                                            T scale2, int64_t blk, int nthr, cx_t<T>* sm) {
+  using C = cx_t<T>;
+  using P = LinePlan<L>;
+  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(L);
+  const int64_t row0 = blk * G;
+  const int per = G * L;
+
+  // thread t owns line t / TPL (field-major: field = line / G, row = line % G)
+  // at positions j + e*TPL; loads go straight to registers, E per thread
+  const int j = threadIdx.x % TPL, line = threadIdx.x / TPL;
+  const int fld = line / G, gl = line - fld * G;
+  C* row = sm + line * RS;
+  C v[E];
+  {
+    const C* __restrict__ src = reinterpret_cast<const C*>(f.in(fld));
+    const int64_t i0 = (row0 + gl) * L + j;
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = src[i0 + TPL * e];
+  }
+  line_fft<L>(v, row, j, tw, (T)1);
+#pragma unroll
+  for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
+  __syncthreads();
+
+  // c = (u/N) x (omega/N): u in rows of fields 0..2, omega in 3..5
+  for (int q = threadIdx.x; q < per; q += nthr) {
+    const int g = q / L, p = q & (L - 1);
+    C u[3], w[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      u[d] = sm[(d * G + g) * RS + pad_pos(p)];
+      w[d] = sm[((3 + d) * G + g) * RS + pad_pos(p)];
+    }
+    const C c0 = csub(cmul(u[1], w[2]), cmul(u[2], w[1]));
+    const C c1 = csub(cmul(u[2], w[0]), cmul(u[0], w[2]));
+    const C c2 = csub(cmul(u[0], w[1]), cmul(u[1], w[0]));
+    sm[(0 * G + g) * RS + pad_pos(p)] = cscale(scale2, c0);
+    sm[(1 * G + g) * RS + pad_pos(p)] = cscale(scale2, c1);
+    sm[(2 * G + g) * RS + pad_pos(p)] = cscale(scale2, c2);
+  }
+  __syncthreads();
+
+  // forward x of the three products.  Lines of up to 32 threads synchronise
+  // within their warp, so warps that hold only omega rows (every warp when G
+  // is a multiple of the lines per warp) skip it; longer lines synchronise the
+  // block and every thread takes part.
+  constexpr int kLinesPerWarp = TPL <= 32 ? 32 / TPL : 1;
+  const bool skip = (TPL <= 32) && (G % kLinesPerWarp == 0) && fld >= 3;
+  if (!skip) {
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
+    line_sync<TPL>();
+    line_fft<L>(v, row, j, tw, (T)-1);
+  }
+
+  if (fld < 3) {
+    C* __restrict__ dst = reinterpret_cast<C*>(f.out(fld));
+    const int64_t i0 = (row0 + gl) * L + j;
+#pragma unroll
+    for (int e = 0; e < E; e++) dst[i0 + TPL * e] = v[e];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K5 of the NS step: z lines -- forward 3 fields + Nyquist zeroing, then the
+// AB2 / projection / CN update per mode (ns.cpp:170-187) and the FP64
+// diagnostics of the new velocity (ns.cpp:206-210).
+struct UpdateArgs {
+  const void* U[3];  // cross1 after x, y forward passes
+  void* V[3];        // in: V1, out: V (new)
+  void* C0[3];       // in: cross0, out: cross1
+  int nx, ny, nz;
+  int lx;         // log2(nx)
+  int W;          // adjacent z lines per tile (may exceed nx: rows of the xy plane)
+  double hK;      // K/2
+  double nuhK;    // nu*K/2
+  double* stats;  // per tile: sum|div|, sum|V|^2, sum|k x V|^2, max|div|
+};
+
+// Tile `blk` holds the W z lines whose xy-plane offsets are blk*W .. blk*W+W-1.
+template <typename T, int L>
+__device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
+                                                 const cx_t<T>* __restrict__ tw, int64_t blk,
+                                                 int nthr, cx_t<T>* sm, double (*red)[32]) {
+  using C = cx_t<T>;
+  using P = LinePlan<L>;
+  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(L);
+
+  const int W = a.W;
+  const int64_t nxy = (int64_t)a.nx * a.ny;
+  const int64_t base = blk * W;
+  const int per = W * L;
+
+  // thread t owns z line (field, base + w) at positions j + e*TPL with
+  // w = t mod W, j = (t / W) mod TPL, field = t / (W*TPL): consecutive threads
+  // load adjacent x, so the direct loads are coalesced
+  {
+    const int w = threadIdx.x % W, s = threadIdx.x / W;
+    const int j = s % TPL, fld = s / TPL;
+    C* row = sm + (fld * W + w) * RS;
+    const C* __restrict__ src = reinterpret_cast<const C*>(a.U[fld]);
+    const int64_t i0 = base + w + nxy * j;
+    C v[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = src[i0 + nxy * (TPL * e)];
+    line_fft<L, true>(v, row, j, tw, (T)-1);
+#pragma unroll
+    for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
+  }
+  __syncthreads();
+
+  const T hK = (T)a.hK, nuhK = (T)a.nuhK;
+  double s_div = 0, s_e = 0, s_w = 0, m_div = 0;
+  C* __restrict__ Vp[3] = {reinterpret_cast<C*>(a.V[0]), reinterpret_cast<C*>(a.V[1]),
+                           reinterpret_cast<C*>(a.V[2])};
+  C* __restrict__ Cp[3] = {reinterpret_cast<C*>(a.C0[0]), reinterpret_cast<C*>(a.C0[1]),
+                           reinterpret_cast<C*>(a.C0[2])};
+  auto update_point = [&](int q, const C (&V1)[3], const C (&c0)[3]) {
+    const int w = q % W, z = q / W;
+    const int64_t xy = base + w;
+    const int x = (int)(xy & (a.nx - 1)), y = (int)(xy >> a.lx);
+    const int64_t idx = xy + nxy * z;
+    const T kx = (T)freq_i(x, a.nx), ky = (T)freq_i(y, a.ny), kz = (T)freq_i(z, a.nz);
+    const bool nyq = y == (a.ny >> 1) || x == (a.nx >> 1) || z == (a.nz >> 1);
+    C c1[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) c1[d] = nyq ? mk((T)0, (T)0) : sm[(d * W + w) * RS + pad_pos(z)];
+    const T kk[3] = {kx, ky, kz};
+    const T k2 = kx * kx + ky * ky + kz * kz;
+    const double k2d = (double)kx * kx + (double)ky * ky + (double)kz * kz;
+    // F = K/2 (3 c1 - c0)                      (ns.cpp:171)
+    // lap1 = nu K/2 (-|k|^2 V1)                (ns.cpp:174)
+    // s = V1 + lap1 + F; G = div s / (-|k|^2)  (ns.cpp:177-178)
+    C F[3], lap[3], s[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      F[d] = cscale(hK, csub(cscale((T)3, c1[d]), c0[d]));
+      lap[d] = cscale(nuhK, cscale(-k2, V1[d]));
+      s[d] = cadd(cadd(V1[d], lap[d]), F[d]);
+    }
+    C G = cadd(cadd(ikmul(kx, s[0]), ikmul(ky, s[1])), ikmul(kz, s[2]));
+    // The divisors -|k|^2 (projection) and 1 + nu K/2 |k|^2 (Crank-Nicolson)
+    // are formed in FP64.  complex128 divides as the reference does; complex64
+    // multiplies by the FP64 reciprocals rounded once to FP32.
+    const bool nonzero = k2d != 0.0;
+    const double den_cn = 1.0 + a.nuhK * k2d;
+    T r_p = (T)1, r_cn = (T)1;
+    if constexpr (sizeof(T) == 4) {
+      if (nonzero) {
+        r_p = (T)(-1.0 / k2d);
+        r_cn = (T)(1.0 / den_cn);
+      }
+      G = cscale(r_p, G);
+    } else {
+      if (nonzero) G = mk(G.x / -k2d, G.y / -k2d);
+    }
+    // Vhalf = V1 + F - grad G; V = (Vhalf + lap1) / (1 + nu K/2 |k|^2)  (ns.cpp:181-187)
+    C Vn[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      C vh = csub(cadd(V1[d], F[d]), ikmul(kk[d], G));
+      C vv = cadd(vh, lap[d]);
+      if constexpr (sizeof(T) == 4) {
+        vv = cscale(r_cn, vv);
+      } else {
+        if (nonzero) vv = mk(vv.x / den_cn, vv.y / den_cn);
+      }
+      Vn[d] = vv;
+      Vp[d][idx] = vv;
+      Cp[d][idx] = c1[d];
+    }
+    // diagnostics of the new velocity: per-mode terms in T, sums in FP64
+    const C dv = cadd(cadd(ikmul(kx, Vn[0]), ikmul(ky, Vn[1])), ikmul(kz, Vn[2]));
+    const double ad = (double)sqrt(dv.x * dv.x + dv.y * dv.y);
+    s_div += ad;
+    m_div = fmax(m_div, ad);
+    T e2 = 0;
+#pragma unroll
+    for (int d = 0; d < 3; d++) e2 += Vn[d].x * Vn[d].x + Vn[d].y * Vn[d].y;
+    const C om0 = csub(ikmul(ky, Vn[2]), ikmul(kz, Vn[1]));
+    const C om1 = csub(ikmul(kz, Vn[0]), ikmul(kx, Vn[2]));
+    const C om2 = csub(ikmul(kx, Vn[1]), ikmul(ky, Vn[0]));
+    const T w2 = om0.x * om0.x + om0.y * om0.y + om1.x * om1.x + om1.y * om1.y +
+                 om2.x * om2.x + om2.y * om2.y;
+    s_e += (double)e2;
+    s_w += (double)w2;
+  };
+  // two points per iteration: the 12 global loads of both are issued first
+  for (int q0 = threadIdx.x; q0 < per; q0 += 2 * nthr) {
+    const int q1 = q0 + nthr;
+    const bool has1 = q1 < per;
+    C V1a[3], c0a[3], V1b[3], c0b[3];
+    const int64_t ia = base + (q0 % W) + nxy * (q0 / W);
+    const int64_t ib = has1 ? base + (q1 % W) + nxy * (q1 / W) : ia;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      V1a[d] = Vp[d][ia];
+      c0a[d] = Cp[d][ia];
+      V1b[d] = Vp[d][ib];
+      c0b[d] = Cp[d][ib];
+    }
+    update_point(q0, V1a, c0a);
+    if (has1) update_point(q1, V1b, c0b);
+  }
+  // block reduction of the diagnostics
+  for (int o = 16; o > 0; o >>= 1) {
+    s_div += __shfl_xor_sync(0xffffffffu, s_div, o);
+    s_e += __shfl_xor_sync(0xffffffffu, s_e, o);
+    s_w += __shfl_xor_sync(0xffffffffu, s_w, o);
+    m_div = fmax(m_div, __shfl_xor_sync(0xffffffffu, m_div, o));
+  }
+  const int warp = threadIdx.x >> 5, nwarps = (nthr + 31) >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][warp] = s_div;
+    red[1][warp] = s_e;
+    red[2][warp] = s_w;
+    red[3][warp] = m_div;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+    for (int i = 0; i < nwarps; i++) {
+      t0 += red[0][i];
+      t1 += red[1][i];
+      t2 += red[2][i];
+      t3 = fmax(t3, red[3][i]);
+    }
+    double* out = a.stats + 4 * blk;
+    out[0] = t0;
+    out[1] = t1;
+    out[2] = t2;
+    out[3] = t3;
+  }
+}
+
+// Field accessor over a FieldPtrs held in kernel parameters.
+struct ParamFields {
+  const FieldPtrs& f;
+  __device__ __forceinline__ const void* in(int i) const { return f.in[i]; }
+  __device__ __forceinline__ void* out(int i) const { return f.out[i]; }
+};
+
+}  // namespace sns

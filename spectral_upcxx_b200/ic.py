@@ -87,3 +87,46 @@ def ns_vortex_tubes(n: int) -> np.ndarray:
     w2d = mag * gauss(np.pi - dist, np.pi - dist) + mag * gauss(np.pi + dist, np.pi - dist) + \
         mag * gauss(np.pi, np.pi + dist)
     return np.broadcast_to(w2d, (n, n, n)).astype(np.complex128).copy()
+
+
+def solenoidal_spectrum_hat(n: int, seed: int, device, k0: float = 4.0, u_rms: float = 1.0):
+    """Fourier transform of ``solenoidal_spectrum(n, seed)`` (Nyquist planes
+    zeroed) built on a torch device: the same seeded amplitudes, with the
+    transforms of the construction done by torch.fft so that large ensembles
+    of initial fields are quick to make.  Returns 3 complex128 tensors."""
+    import torch
+    g = rng(seed)
+    k = torch.as_tensor(wavenumbers(n), device=device)
+    KZ, KY, KX = torch.meshgrid(k, k, k, indexing="ij")
+    K2 = KX ** 2 + KY ** 2 + KZ ** 2
+    Kmag = torch.sqrt(K2)
+    E = Kmag ** 4 * torch.exp(-2.0 * (Kmag / k0) ** 2)
+    amp = torch.where(K2 > 0, torch.sqrt(E / (4 * np.pi * torch.clamp(K2, min=1.0))),
+                      torch.zeros_like(K2))
+    uh = []
+    for _ in range(3):
+        re = torch.as_tensor(g.standard_normal((n, n, n)), device=device)
+        im = torch.as_tensor(g.standard_normal((n, n, n)), device=device)
+        uh.append(amp * torch.complex(re, im))
+    K2s = torch.where(K2 > 0, K2, torch.ones_like(K2))
+
+    def project(vh):
+        kdotv = (KX * vh[0] + KY * vh[1] + KZ * vh[2]) / K2s
+        return [vh[0] - KX * kdotv, vh[1] - KY * kdotv, vh[2] - KZ * kdotv]
+
+    uh = project(uh)
+    u = [torch.fft.ifftn(c).real.to(torch.complex128) for c in uh]
+    uh = project([torch.fft.fftn(c) for c in u])
+    h = n // 2
+    for c in uh:
+        c[h, :, :] = 0
+        c[:, h, :] = 0
+        c[:, :, h] = 0
+    u = [torch.fft.ifftn(c).real for c in uh]
+    rms = torch.sqrt(torch.mean(u[0] ** 2 + u[1] ** 2 + u[2] ** 2) / 3.0)
+    out = [torch.fft.fftn((c * (u_rms / rms)).to(torch.complex128)) for c in u]
+    for c in out:
+        c[h, :, :] = 0
+        c[:, h, :] = 0
+        c[:, :, h] = 0
+    return out

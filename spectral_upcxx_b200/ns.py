@@ -84,3 +84,102 @@ class NSStepper:
         if n < 0:
             N.check("sns_ns_pass_times", n)
         return [(tot[i], cnt[i]) for i in range(n)]
+
+
+ENS_GRAPH, ENS_EAGER, ENS_SEQUENTIAL = 0, 1, 2
+
+
+class NSEnsemble:
+    """Independent boxes of uneven size advanced together (sns_ens_*).
+
+    ``shapes`` holds one (nz, ny, nx) per box and ``nus`` one viscosity per
+    box; dt and dtype are shared.  Each box follows ns.cpp exactly as
+    ``NSStepper`` does; one ensemble step is five launches over every box.
+    """
+
+    def __init__(self, shapes, nus, dt: float, dtype=torch.complex64, tune: bool = True,
+                 device="cuda"):
+        shapes = [tuple(int(n) for n in s) for s in shapes]
+        if len(shapes) != len(nus):
+            raise ValueError("one viscosity per box")
+        self.shapes = shapes
+        self.nus = [float(v) for v in nus]
+        self.dt = float(dt)
+        self.dtype = dtype
+        self.device = torch.device(device)
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.prec = N.SNS_C64 if dtype == torch.complex64 else N.SNS_C128
+        self._stream = torch.cuda.current_stream(self.device)
+        dims = (C.c_int64 * (3 * len(shapes)))()
+        for i, (nz, ny, nx) in enumerate(shapes):
+            dims[3 * i], dims[3 * i + 1], dims[3 * i + 2] = nx, ny, nz
+        nu = (C.c_double * len(shapes))(*self.nus)
+        h = C.c_void_p()
+        N.call("sns_ens_create", C.byref(h), len(shapes), dims, nu, self.dt, self.prec,
+               int(bool(tune)), C.c_void_p(self._stream.cuda_stream))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            N.lib().sns_ens_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.shapes)
+
+    def _vec(self, box, v):
+        v = list(v)
+        for f in v:
+            if _check_field(f) != self.prec or tuple(f.shape) != self.shapes[box]:
+                raise ValueError("vector components must match the box's shape and dtype")
+        return N.ptr3([f.data_ptr() for f in v])
+
+    def bootstrap(self, box: int, V0, omega0):
+        N.call("sns_ens_bootstrap", self.h, int(box), self._vec(box, V0), self._vec(box, omega0))
+
+    def set_state(self, box: int, V1, cross0):
+        N.call("sns_ens_set_state", self.h, int(box), self._vec(box, V1), self._vec(box, cross0))
+
+    def step(self, n: int = 1, mode: int = ENS_GRAPH):
+        N.call("sns_ens_step", self.h, int(n), int(mode))
+
+    def state(self, box: int):
+        shape = self.shapes[box]
+        mk = lambda: [torch.empty(shape, dtype=self.dtype, device=self.device) for _ in range(3)]
+        V1, w1, c0 = mk(), mk(), mk()
+        N.call("sns_ens_get_state", self.h, int(box), self._vec(box, V1), self._vec(box, w1),
+               self._vec(box, c0))
+        return {"V1": V1, "omega1": w1, "cross0": c0}
+
+    def stats(self):
+        """Per box: div_avg, energy, enstrophy, max_div (as sns_ns_stats)."""
+        out = (C.c_double * (4 * len(self.shapes)))()
+        N.call("sns_ens_stats", self.h, out)
+        keys = ("div_avg", "energy", "enstrophy", "max_div")
+        return [dict(zip(keys, out[4 * i:4 * i + 4])) for i in range(len(self.shapes))]
+
+    def tuning(self):
+        """Per stage: (threads per CTA, line-run cap, persistent grid)."""
+        out = (C.c_int * 15)()
+        n = N.lib().sns_ens_tuning(self.h, out, 15)
+        if n < 0:
+            N.check("sns_ens_tuning", n)
+        return [tuple(out[3 * s:3 * s + 3]) for s in range(n)]
+
+    def launches_per_step(self, mode: int = ENS_GRAPH) -> int:
+        return N.lib().sns_ens_launches_per_step(self.h, int(mode))
+
+    def stage_times(self, n: int = 5):
+        """Run n steps with events between the stages; mean ms per stage."""
+        ms = (C.c_double * 5)()
+        k = N.lib().sns_ens_stage_times(self.h, int(n), ms)
+        if k < 0:
+            N.check("sns_ens_stage_times", k)
+        return list(ms[:k])

@@ -53,6 +53,32 @@ def test_unsupported_sizes_are_reported(sns):
     assert rc == N.SNS_ERR_UNSUPPORTED and not h.value
 
 
+def test_ensemble_arguments_are_checked_before_any_device_work(sns):
+    from spectral_upcxx_b200 import _native as N
+    L = N.lib()
+    h = C.c_void_p()
+
+    def create(shapes, nus, prec=0):
+        dims = (C.c_int64 * max(1, 3 * len(shapes)))(*[n for s in shapes for n in s])
+        nu = (C.c_double * max(1, len(nus)))(*nus)
+        return L.sns_ens_create(C.byref(h), len(shapes), dims, nu, 2e-3, prec, 0, None)
+
+    assert create([], []) == N.SNS_ERR_ARG
+    assert create([(32, 32, 32)], [0.01], prec=5) == N.SNS_ERR_ARG
+    assert create([(32, 32, 24)], [0.01]) == N.SNS_ERR_UNSUPPORTED
+    assert create([(512, 512, 512)], [0.01]) == N.SNS_ERR_UNSUPPORTED
+    assert create([(8, 16, 16)], [0.01]) == N.SNS_ERR_UNSUPPORTED
+    nine = [(16 << (i % 5), 16 << (i // 5), 16) for i in range(9)]
+    assert create(nine, [0.01] * 9) == N.SNS_ERR_UNSUPPORTED
+    assert "distinct" in N.last_error()
+    assert not h.value
+    assert L.sns_ens_step(None, 1, 0) == N.SNS_ERR_ARG
+    assert L.sns_ens_stats(None, None) == N.SNS_ERR_ARG
+    assert L.sns_ens_bootstrap(None, 0, None, None) == N.SNS_ERR_ARG
+    assert L.sns_ens_boxes(None) == N.SNS_ERR_ARG
+    assert L.sns_ens_destroy(None) == 0
+
+
 def test_call_wrapper_raises(sns):
     from spectral_upcxx_b200 import _native as N
     with pytest.raises(N.SNSError):
