@@ -181,6 +181,63 @@ int sns_ns_launches_per_step(sns_ns* handle);
 int sns_ns_profile(sns_ns* handle, int enable);
 int sns_ns_pass_times(sns_ns* handle, double* total_ms, int* launches, int max);
 
+/* ---- eddy-viscosity closure of the stepper ---------------------------------
+ * No reference counterpart (exec/ns.cpp has no subgrid model).  With a
+ * closure set, every step adds the divergence of tau_ij = 2 nu_t S_ij to the
+ * nonlinear term cross1 (ns.cpp:203-206) before the unchanged AB2 /
+ * projection / Crank-Nicolson update; S_ij and the model inputs come from the
+ * velocity gradient A_ij = d_j u_i (real parts).  Models: SNS_CLOSURE_NONE
+ * (the plain step), SNS_CLOSURE_SMAGORINSKY (nu_t = cs_delta2 sqrt(2 S:S),
+ * cs_delta2 = (Cs Delta)^2), SNS_CLOSURE_MLP (nu_t from the packed MLP at
+ * `mlp`, device memory that must outlive the steps).  Needs nx*ny*nz to be a
+ * multiple of 32; allocates six more work fields on first use. */
+#define SNS_CLOSURE_NONE 0
+#define SNS_CLOSURE_SMAGORINSKY 1
+#define SNS_CLOSURE_MLP 2
+int sns_ns_set_closure(sns_ns* handle, int model, double cs_delta2, const void* mlp);
+
+/* ---- learned closure: MLP 9 -> 64 -> 64 -> 1 on the tensor cores ----------
+ * No reference counterpart.  FP32 master parameters (nparams floats: W1[64][16]
+ * with columns 9..15 zero, b1[64], W2[64][64], b2[64], w3[64], b3) and a packed
+ * inference copy (packed_bytes: bf16 W1, W2, w3; f32 b1, b2, b3, s_in, s_out).
+ * Inputs are 16 bf16 per sample (s_in * A_ij in row-major order, zero padded);
+ * nu_t = s_out * softplus(z), ReLU hidden layers, FP32 accumulation. */
+int sns_mlp_sizes(int64_t* nparams, int64_t* packed_bytes);
+int sns_mlp_pack(const float* master, double s_in, double s_out, void* packed, void* stream);
+/* nut[M] = the model at the M rows of X (device pointers). */
+int sns_mlp_infer(const void* packed, const void* X, int64_t M, float* nut, void* stream);
+/* Gradient of the mean squared error of softplus(z) against target (model
+ * units, i.e. nu_t / s_out) over B samples (rows idx[0..B) of X, or rows
+ * 0..B when idx is NULL).  grad: nparams + 1 floats (gradients, then the mean
+ * loss), device memory.  Synchronises the stream. */
+int sns_mlp_grad(const void* packed, const void* X, const float* target, const int* idx, int64_t B,
+                 float* grad, void* stream);
+/* One Adam step (bias correction for step >= 1) on the masters; refreshes
+ * the packed copy's weights and biases. */
+int sns_mlp_adam(float* master, float* m, float* v, const float* grad, int step, double lr,
+                 double beta1, double beta2, double eps, void* packed, void* stream);
+
+/* ---- filtered-DNS data for the closure -------------------------------------
+ * Cubic grids, powers of two.  Fourier fields follow the reference's
+ * unnormalised convention, so a coarse copy is scaled by nc^3 / nf^3. */
+/* Sharp spherical cutoff |k| <= kc of nfields fine fields onto nc^3 grids. */
+int sns_spectral_truncate(const void* const* in, void* const* out, int nfields, int64_t nf,
+                          int64_t nc, double kc, int prec, void* stream);
+/* Zero-padded copy of coarse fields on nf^3 grids (modes |k_d| < nc/2). */
+int sns_spectral_pad(const void* const* in, void* const* out, int nfields, int64_t nc, int64_t nf,
+                     int prec, void* stream);
+/* Training pairs from one fine Fourier velocity V (nf^3): X (nc^3 rows of 16
+ * bf16: s_in times the filtered gradient) and nut (nc^3 floats: the pointwise
+ * least-squares eddy viscosity -(tau^d : S) / (2 S : S) of the filtered SGS
+ * stress tau_ij = filter(u_i u_j) - filter(ubar_i ubar_j), products formed on
+ * the fine grid), and optionally the filtered coarse velocity Vc. */
+int sns_sgs_sample(const void* const V[3], int64_t nf, int64_t nc, double kc, double s_in,
+                   int prec, void* X, float* nut, void* const Vc[3], void* stream);
+/* E[k] = sum over the shell round(|k|) = k of |V_hat|^2 / (2 N^2), k < nshell
+ * (device doubles), so that sum_k E[k] = <|u|^2> / 2. */
+int sns_energy_spectrum(const void* const V[3], int64_t nx, int64_t ny, int64_t nz, int prec,
+                        double* E, int nshell, void* stream);
+
 /* ---- batched ensemble of NS boxes ----------------------------------------
  * No reference counterpart: the reference runs one box per process
  * (exec/ns.cpp).  An ensemble holds independent boxes of up to 8 distinct

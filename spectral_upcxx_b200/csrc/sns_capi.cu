@@ -13,6 +13,7 @@
 #include "sns_fft.cuh"
 #include "sns_ns.cuh"
 #include "sns_ens.cuh"
+#include "sns_les.cuh"
 #include "sns_ops.cuh"
 
 namespace sns {
@@ -203,6 +204,9 @@ struct sns_ns {
   double* stats_out;
   int* sync_words;  // dataflow xy pass: ticket, per-plane counters, error word
   bool stepped;
+  // eddy-viscosity closure (none by default) and its six extra work fields
+  Closure cl;
+  void* U2[6] = {};
   // per-pass profiling
   bool profiling = false;
   int recorded = 0;
@@ -521,6 +525,7 @@ int sns_ns_destroy(sns_ns* h) {
   pool_free(h->stats_part);
   pool_free(h->stats_out);
   pool_free(h->sync_words);
+  for (int i = 0; i < 6; i++) pool_free(h->U2[i]);
   for (cudaEvent_t e : h->events) cudaEventDestroy(e);
   delete h;
   return OK;
@@ -561,6 +566,19 @@ int sns_ns_step(sns_ns* h, int nsteps) {
   if (nsteps < 0) {
     set_error("sns_ns_step: negative step count");
     return ERR_ARG;
+  }
+  if (h->cl.model != CLOSURE_NONE) {
+    void* U[kLESWork];
+    for (int i = 0; i < 6; i++) {
+      U[i] = h->U[i];
+      U[6 + i] = h->U2[i];
+    }
+    for (int t = 0; t < nsteps; t++) {
+      int rc = les_step_once(h->pl, h->V, h->C0, U, h->stats_part, h->nu, h->dt, h->cl, h->s);
+      if (rc) return rc;
+      h->stepped = true;
+    }
+    return OK;
   }
   for (int t = 0; t < nsteps; t++) {
     cudaEvent_t* ev = nullptr;
@@ -678,8 +696,41 @@ int sns_ns_stats(sns_ns* h, double* div_avg, double* energy, double* enstrophy, 
 }
 
 int sns_ns_launches_per_step(sns_ns* h) {
-  (void)h;
-  return h->pl.passes;
+  if (!nonnull(h, "sns_ns_launches_per_step")) return ERR_ARG;
+  return h->cl.model != CLOSURE_NONE ? kLESLaunches : h->pl.passes;
+}
+
+int sns_ns_set_closure(sns_ns* h, int model, double cs_delta2, const void* mlp) {
+  if (!nonnull(h, "sns_ns_set_closure")) return ERR_ARG;
+  if (model != SNS_CLOSURE_NONE && model != SNS_CLOSURE_SMAGORINSKY && model != SNS_CLOSURE_MLP) {
+    set_error("sns_ns_set_closure: unknown model");
+    return ERR_ARG;
+  }
+  if (model == SNS_CLOSURE_MLP && !mlp) {
+    set_error("sns_ns_set_closure: the MLP model needs packed weights");
+    return ERR_ARG;
+  }
+  if (model == SNS_CLOSURE_SMAGORINSKY && !(cs_delta2 >= 0)) {
+    set_error("sns_ns_set_closure: (Cs Delta)^2 must be >= 0");
+    return ERR_ARG;
+  }
+  if (model != SNS_CLOSURE_NONE && !h->U2[0]) {
+    const size_t bytes = esize(h->pl.prec) * (size_t)h->pl.nx * h->pl.ny * h->pl.nz;
+    for (int i = 0; i < 6; i++) {
+      int rc = pool_malloc(&h->U2[i], bytes);
+      if (rc) {
+        for (int j = 0; j < i; j++) {
+          pool_free(h->U2[j]);
+          h->U2[j] = nullptr;
+        }
+        return rc;
+      }
+    }
+  }
+  h->cl.model = model;
+  h->cl.csd2 = cs_delta2;
+  h->cl.mlp = mlp;
+  return OK;
 }
 
 }  // extern "C"

@@ -12,8 +12,9 @@
 // ensemble itself and keeps the fastest.
 //
 // The tile bodies are the ones the single-box kernels run (sns_tiles.cuh), so
-// a box advanced in the ensemble is bit-identical to the same box advanced by
-// the single-box stepper.
+// a box advanced in the ensemble follows the single-box stepper's arithmetic;
+// the two agree to rounding (the compiler may contract multiply-adds
+// differently once the bodies are inlined into other kernels).
 #include <math.h>
 #include <stdlib.h>
 
@@ -70,11 +71,13 @@ struct BoxCurlFields {  // K1: V in, U out
   const EnsBox* __restrict__ b;
   __device__ __forceinline__ const void* in(int i) const { return i < 3 ? b->V[i] : nullptr; }
   __device__ __forceinline__ void* out(int i) const { return b->U[i]; }
+  __device__ __forceinline__ int first() const { return 0; }
 };
 struct BoxWorkFields {  // K2, K3, K4: in place on U
   const EnsBox* __restrict__ b;
   __device__ __forceinline__ const void* in(int i) const { return b->U[i]; }
   __device__ __forceinline__ void* out(int i) const { return b->U[i]; }
+  __device__ __forceinline__ int first() const { return 0; }
 };
 
 template <typename T, int L, int STAGE>

@@ -42,13 +42,13 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
 // ---------------------------------------------------------------------------
 // K5: z lines -- forward 3 fields + Nyquist zeroing, then the AB2 /
 // projection / CN update per mode.
-template <typename T, int L>
+template <typename T, int L, bool SGS>
 __global__ void __launch_bounds__(MaxThreads<T>::value)
     k_zfwd_update(const UpdateArgs a, const cx_t<T>* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[4][32];
-  zfwd_update_tile<T, L>(a, tw, (int64_t)blockIdx.x, (int)blockDim.x,
-                         reinterpret_cast<cx_t<T>*>(smem_raw), red);
+  zfwd_update_tile<T, L, SGS>(a, tw, (int64_t)blockIdx.x, (int)blockDim.x,
+                              reinterpret_cast<cx_t<T>*>(smem_raw), red);
 }
 
 __global__ void k_stats_final(const double* part, int blocks, double* out) {
@@ -106,7 +106,7 @@ int launch_xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream
   return OK;
 }
 
-template <typename T, int L>
+template <typename T, int L, bool SGS>
 int launch_update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
   using C = cx_t<T>;
   constexpr int TPL = LinePlan<L>::TPL;
@@ -116,12 +116,12 @@ int launch_update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr[dev & 63]) {
-    cudaError_t e = allow_max_dynamic_smem(k_zfwd_update<T, L>);
+    cudaError_t e = allow_max_dynamic_smem(k_zfwd_update<T, L, SGS>);
     if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_zfwd_update)");
     attr[dev & 63] = true;
   }
   const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
-  k_zfwd_update<T, L><<<pl.update_blocks, threads, smem, s>>>(a, tw);
+  k_zfwd_update<T, L, SGS><<<pl.update_blocks, threads, smem, s>>>(a, tw);
   SNS_CHECK_LAUNCH("k_zfwd_update");
   return OK;
 }
@@ -142,18 +142,18 @@ int xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream_t s) {
   }
 }
 
-template <typename T>
+template <typename T, bool SGS>
 int update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
   switch (pl.nz) {
-    case 4: return launch_update<T, 4>(pl, a, s);
-    case 8: return launch_update<T, 8>(pl, a, s);
-    case 16: return launch_update<T, 16>(pl, a, s);
-    case 32: return launch_update<T, 32>(pl, a, s);
-    case 64: return launch_update<T, 64>(pl, a, s);
-    case 128: return launch_update<T, 128>(pl, a, s);
-    case 256: return launch_update<T, 256>(pl, a, s);
-    case 512: return launch_update<T, 512>(pl, a, s);
-    case 1024: return launch_update<T, 1024>(pl, a, s);
+    case 4: return launch_update<T, 4, SGS>(pl, a, s);
+    case 8: return launch_update<T, 8, SGS>(pl, a, s);
+    case 16: return launch_update<T, 16, SGS>(pl, a, s);
+    case 32: return launch_update<T, 32, SGS>(pl, a, s);
+    case 64: return launch_update<T, 64, SGS>(pl, a, s);
+    case 128: return launch_update<T, 128, SGS>(pl, a, s);
+    case 256: return launch_update<T, 256, SGS>(pl, a, s);
+    case 512: return launch_update<T, 512, SGS>(pl, a, s);
+    case 1024: return launch_update<T, 1024, SGS>(pl, a, s);
     default: set_error("fused NS step: nz must be a power of two in [4, 1024]"); return ERR_UNSUPPORTED;
   }
 }
@@ -308,11 +308,16 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     a.hK = dt / 2;
     a.nuhK = nu * dt / 2;
     a.stats = stats;
-    rc = prec == PREC_C128 ? update<double>(pl, a, s) : update<float>(pl, a, s);
+    rc = ns_update(pl, a, false, s);
     if (rc) return rc;
     mark();
   }
   return OK;
+}
+
+int ns_update(const NSPlan& pl, const UpdateArgs& a, bool sgs, cudaStream_t s) {
+  if (pl.prec == PREC_C128) return sgs ? update<double, true>(pl, a, s) : update<double, false>(pl, a, s);
+  return sgs ? update<float, true>(pl, a, s) : update<float, false>(pl, a, s);
 }
 
 int ns_stats_final(const NSPlan& pl, const double* partials, double* out4, cudaStream_t s) {

@@ -30,6 +30,10 @@ constexpr int kNSPasses = 5;
 int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* const U[6],
                  double* stats, int* sync_words, double nu, double dt, cudaStream_t s,
                  cudaEvent_t* ev = nullptr);
+// The update pass (z-forward + AB2 / projection / CN update) on the fields of
+// `a`; sgs adds the divergence of the Fourier eddy stress a.tau.
+struct UpdateArgs;
+int ns_update(const NSPlan& pl, const UpdateArgs& a, bool sgs, cudaStream_t s);
 // Reduce the per-block diagnostics into out4 (device): sum|div|, sum|V|^2,
 // sum|i k x V|^2, max|div|.
 int ns_stats_final(const NSPlan& pl, const double* partials, double* out4, cudaStream_t s);

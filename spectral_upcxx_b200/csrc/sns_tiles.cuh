@@ -48,16 +48,22 @@ __device__ __forceinline__ LineCoord line_coord(const LineGeo& geo, int64_t base
   return c;
 }
 
-// Element of the thread's line as the prologue forms it.
+// Element of the thread's line as the prologue forms it (q: the output index
+// of the field for PRO_GRAD12, block-uniform).
 template <int PRO, typename C, typename T>
 __device__ __forceinline__ C pro_load(const C* __restrict__ src, const C* __restrict__ v0,
                                       const C* __restrict__ v1, const C* __restrict__ v2,
-                                      int field, int64_t idx, T kx, T ky, T kz) {
+                                      int field, int q, int64_t idx, T kx, T ky, T kz) {
   if constexpr (PRO == PRO_CURL6) {
     if (field < 3) return src[idx];
     if (field == 3) return csub(ikmul(ky, v2[idx]), ikmul(kz, v1[idx]));
     if (field == 4) return csub(ikmul(kz, v0[idx]), ikmul(kx, v2[idx]));
     return csub(ikmul(kx, v1[idx]), ikmul(ky, v0[idx]));
+  } else if constexpr (PRO == PRO_GRAD12) {
+    if (q < 3) return (q == 0 ? v0 : q == 1 ? v1 : v2)[idx];
+    const int i = (q - 3) / 3, j = (q - 3) - 3 * ((q - 3) / 3);
+    const C* __restrict__ vi = i == 0 ? v0 : i == 1 ? v1 : v2;
+    return ikmul(j == 0 ? kx : j == 1 ? ky : kz, vi[idx]);
   } else {
     return src[idx];
   }
@@ -86,15 +92,17 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
 
   C v[E];
   {
-    const C* __restrict__ src = reinterpret_cast<const C*>(f.in(field));
+    const C* __restrict__ src =
+        PRO == PRO_GRAD12 ? nullptr : reinterpret_cast<const C*>(f.in(field));
     const C* __restrict__ v0 = nullptr;
     const C* __restrict__ v1 = nullptr;
     const C* __restrict__ v2 = nullptr;
-    if constexpr (PRO == PRO_CURL6) {
+    if constexpr (PRO == PRO_CURL6 || PRO == PRO_GRAD12) {
       v0 = reinterpret_cast<const C*>(f.in(0));
       v1 = reinterpret_cast<const C*>(f.in(1));
       v2 = reinterpret_cast<const C*>(f.in(2));
     }
+    const int q = PRO == PRO_GRAD12 ? f.first() + field : field;
     // wavenumbers of the line: two are fixed, the one along the axis varies
     const T kx0 = (T)freq_i(lc.x, geo.nx), ky0 = (T)freq_i(lc.y, geo.ny),
             kz0 = (T)freq_i(lc.z, geo.nz);
@@ -102,7 +110,7 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
 #pragma unroll
     for (int e = 0; e < E; e++) {
       const T kp = (T)freq_i(j + TPL * e, naxis);
-      v[e] = pro_load<PRO, C>(src, v0, v1, v2, field, lc.idx0 + e * lc.step,
+      v[e] = pro_load<PRO, C>(src, v0, v1, v2, field, q, lc.idx0 + e * lc.step,
                               geo.axis == 0 ? kp : kx0, geo.axis == 1 ? kp : ky0,
                               geo.axis == 2 ? kp : kz0);
     }
@@ -209,10 +217,13 @@ struct UpdateArgs {
   double hK;      // K/2
   double nuhK;    // nu*K/2
   double* stats;  // per tile: sum|div|, sum|V|^2, sum|k x V|^2, max|div|
+  // SGS: Fourier eddy stress tau_xx, tau_yy, tau_zz, tau_xy, tau_xz, tau_yz
+  // whose divergence i k_j tau_ij joins cross1 before the Nyquist zeroing
+  const void* tau[6];
 };
 
 // Tile `blk` holds the W z lines whose xy-plane offsets are blk*W .. blk*W+W-1.
-template <typename T, int L>
+template <typename T, int L, bool SGS = false>
 __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
                                                  const cx_t<T>* __restrict__ tw, int64_t blk,
                                                  int nthr, cx_t<T>* sm, double (*red)[32]) {
@@ -259,6 +270,17 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
     C c1[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) c1[d] = nyq ? mk((T)0, (T)0) : sm[(d * W + w) * RS + pad_pos(z)];
+    if constexpr (SGS) {
+      if (!nyq) {
+        C t6[6];
+#pragma unroll
+        for (int q = 0; q < 6; q++) t6[q] = reinterpret_cast<const C*>(a.tau[q])[idx];
+        // (div tau)_i = i (kx tau_ix + ky tau_iy + kz tau_iz)
+        c1[0] = cadd(c1[0], cadd(cadd(ikmul(kx, t6[0]), ikmul(ky, t6[3])), ikmul(kz, t6[4])));
+        c1[1] = cadd(c1[1], cadd(cadd(ikmul(kx, t6[3]), ikmul(ky, t6[1])), ikmul(kz, t6[5])));
+        c1[2] = cadd(c1[2], cadd(cadd(ikmul(kx, t6[4]), ikmul(ky, t6[5])), ikmul(kz, t6[2])));
+      }
+    }
     const T kk[3] = {kx, ky, kz};
     const T k2 = kx * kx + ky * ky + kz * kz;
     const double k2d = (double)kx * kx + (double)ky * ky + (double)kz * kz;
@@ -372,6 +394,7 @@ struct ParamFields {
   const FieldPtrs& f;
   __device__ __forceinline__ const void* in(int i) const { return f.in[i]; }
   __device__ __forceinline__ void* out(int i) const { return f.out[i]; }
+  __device__ __forceinline__ int first() const { return f.first; }
 };
 
 }  // namespace sns

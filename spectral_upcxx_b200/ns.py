@@ -63,6 +63,21 @@ class NSStepper:
         N.call("sns_ns_get_state", self.h, self._vec(V1), self._vec(w1), self._vec(c0))
         return {"V1": V1, "omega1": w1, "cross0": c0}
 
+    def set_closure(self, model: int, cs_delta2: float = 0.0, mlp=None):
+        """Eddy-viscosity closure of every following step: N.SNS_CLOSURE_NONE,
+        _SMAGORINSKY (nu_t = cs_delta2 sqrt(2 S:S)) or _MLP (`mlp`: the packed
+        model tensor, kept alive by the caller)."""
+        self._mlp = mlp
+        N.call("sns_ns_set_closure", self.h, int(model), float(cs_delta2),
+               C.c_void_p(mlp.data_ptr()) if mlp is not None else None)
+
+    def velocity(self, out=None):
+        """The Fourier velocity V1 (into `out`, three device fields, if given)."""
+        if out is None:
+            out = [torch.empty(self.shape, dtype=self.dtype, device=self.device) for _ in range(3)]
+        N.call("sns_ns_get_state", self.h, self._vec(out), None, None)
+        return out
+
     def stats(self):
         v = [C.c_double() for _ in range(4)]
         N.call("sns_ns_stats", self.h, *[C.byref(x) for x in v])
