@@ -70,7 +70,14 @@ WORKLOADS = {
     "fft256_c128": dict(kind="fft", n=256, prec="c128"),
     "fft512_c128": dict(kind="fft", n=512, prec="c128"),
     "ens_config4": dict(kind="ens", n=128, prec="c64"),
+    "closure_config5": dict(kind="closure", n=256, prec="c64"),
 }
+# learned closure: 256^3 DNS (nu = 1/400, dt = 5e-4 as the plain benchmark)
+# filtered at kc = 21 onto 64^3; training snapshots every 5 steps of 2000 from
+# 5 seeds (2000 snapshots), evaluation on 3 held-out seeds over 2000 steps
+CLOSURE = dict(nf=256, nc=64, kc=21, train_seeds=[101, 102, 103, 104, 105],
+               eval_seeds=[201, 202, 203], steps=2000, every=5, train_steps=3000,
+               batch=65536, lr=2e-3, cs=0.17)
 # batched ensemble: 32 boxes of 32^3, 24 of 64^3 and 8 of 128^3, each with its
 # own spectrum-seeded field and nu log-uniform in [1/800, 1/100].  dt = 1e-3:
 # at the stated 2e-3 the AB2/CN scheme blows up in the 128^3 boxes of smallest
@@ -93,6 +100,15 @@ def peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback"
+
+
+def bf16_peak():
+    """Dense bf16 TFLOP/s: measured burst figure, else the fallback."""
+    try:
+        with open(PEAKS_FILE) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
 
 
 # ---------------------------------------------------------------- clocks
@@ -504,6 +520,16 @@ def run_b200(args, rank, world, local):
                "grid": f"{n}^3", "precision": wl["prec"], "parallelism": f"replicas x{world}",
                "l2": "no flush: 12 resident fields (%.2f GB) exceed the 126 MB L2" % (
                    12 * field_bytes / 1e9)}
+    elif wl["kind"] == "closure":
+        result.update(closure_bench(S, torch, dev, args, world, rank, hbm, peak_src, clocks))
+        cfg = {"workload": "closure_config5: %d^3 DNS (nu=1/400, dt=5e-4) sharp-spectral filtered "
+                           "at kc=%d onto %d^3; MLP 9-64-64-1 trained on %d snapshots of %d "
+                           "seeds; %d^3 runs (modes |k| <= kc) of %d held-out seeds over %d "
+                           "steps" % (CLOSURE["nf"], CLOSURE["kc"], CLOSURE["nc"],
+                                      result["snapshots"], len(CLOSURE["train_seeds"]),
+                                      CLOSURE["nc"], len(CLOSURE["eval_seeds"]), CLOSURE["steps"]),
+               "precision": "c64 fields, bf16 MLP with fp32 accumulation",
+               "parallelism": f"replicas x{world}", "l2": "coarse fields L2-resident by size"}
     elif wl["kind"] == "ens":
         result.update(ens_bench(S, torch, dev, stream, args, world, rank, hbm, peak_src, clocks,
                                 barrier, max_over_ranks))
@@ -716,6 +742,98 @@ def ens_bench(S, torch, dev, stream, args, world, rank, hbm, peak_src, clocks, b
                 "d2h_bytes_per_step": (3 * points * esz + 32 * nb * args.steps) / args.steps,
                 "includes": "upload of V0/omega0 of every box from pinned host, bootstrap, K graph "
                             "steps each with the per-box diagnostics read, download of every V1"},
+    }
+
+
+def closure_bench(S, torch, dev, args, world, rank, hbm, peak_src, clocks):
+    """Config 5: dataset from filtered DNS, GPU training, coarse runs judged by
+    the filtered DNS energy spectrum.  value = steps/s of the 64^3 MLP-closure
+    run (device time, K steps through a CUDA-event window)."""
+    from spectral_upcxx_b200 import closure as CL
+    from spectral_upcxx_b200 import ic
+    c = CLOSURE
+    t0 = time.perf_counter()
+    X, nut, w, s_in, snaps = CL.dns_dataset(S, c["nf"], c["nc"], c["kc"], c["train_seeds"], NU,
+                                            DT, c["steps"], c["every"], device=dev)
+    t_data = time.perf_counter() - t0
+    s_out = float((nut * w).mean() / w.mean())
+    model = CL.MLPModel.init(0, s_in=s_in, s_out=s_out, device=dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = CL.train(model, X, nut, c["train_steps"], c["batch"], c["lr"], weight=w)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    samples = X.shape[0]
+    del X, nut, w
+    torch.cuda.empty_cache()
+    res = CL.evaluate(S, model, c["nf"], c["nc"], c["kc"], c["eval_seeds"], NU, DT, c["steps"],
+                      cs=c["cs"], device=dev)
+    # device-timed steps/s of the coarse MLP run and of the plain coarse run
+    nc = c["nc"]
+    Vc0 = CL.truncate([x.to(torch.complex64) for x in ic.solenoidal_spectrum_hat(
+        c["nf"], c["eval_seeds"][0], dev)], nc, c["kc"])
+    timing, launches = {}, {}
+    for name in ("mlp", "plain"):
+        st = S.NSStepper((nc, nc, nc), NU, DT, torch.complex64, device=dev)
+        if name == "mlp":
+            st.set_closure(S._native.SNS_CLOSURE_MLP, mlp=model.packed, kc=c["kc"])
+        else:
+            st.set_closure(S._native.SNS_CLOSURE_NONE, kc=c["kc"])
+        st.bootstrap(Vc0, S.curl(Vc0))
+        st.step(args.warmup)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        if name == "mlp":
+            clocks.start()
+            time.sleep(0.3)
+        tw0 = time.time()
+        e0.record()
+        st.step(args.steps)
+        e1.record()
+        torch.cuda.synchronize()
+        if name == "mlp":
+            clocks.window(tw0, time.time())
+            time.sleep(0.2)
+            clocks.stop()
+        timing[name] = args.steps / (e0.elapsed_time(e1) / 1e3)
+        launches[name] = st.launches_per_step()
+        st.close()
+    # MLP inference throughput on the tensor cores (64^3 points per call)
+    Xi = torch.randn((nc ** 3, 16), device=dev).to(torch.bfloat16)
+    for _ in range(3):
+        model.infer(Xi)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(50):
+        model.infer(Xi)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_inf = e0.elapsed_time(e1) / 50
+    flops = 9472.0 * nc ** 3
+    tpeak, tsrc = bf16_peak()
+    achieved = flops / (ms_inf / 1e3) / 1e12
+    return {
+        "metric": "closure64 steps/s (MLP eddy-viscosity 64^3 run)",
+        "value": world * timing["mlp"], "unit": "steps/s", "ms_per_step": 1000.0 / timing["mlp"],
+        "dtype": "fp32 fields + bf16/fp32 MLP", "snapshots": snaps,
+        "spectrum_error": {"plain": res["plain"], "smagorinsky": res["smagorinsky"],
+                           "mlp": res["mlp"], "shells": f"1..{c['kc'] - 1}", "target": 0.05,
+                           "spectra_first_seed": res["spectra_first_seed"]},
+        "throughput": {"mlp_coarse_steps_per_s": timing["mlp"],
+                       "plain_coarse_steps_per_s": timing["plain"],
+                       "dns_steps_per_s": res["dns_steps_per_s"],
+                       "ratio_mlp_vs_dns": timing["mlp"] / res["dns_steps_per_s"],
+                       "target_ratio": 20.0},
+        "training": {"samples": samples, "steps": c["train_steps"], "batch": c["batch"],
+                     "seconds": t_train, "dataset_seconds": t_data,
+                     "loss_first": losses[0][1], "loss_last": losses[-1][1],
+                     "s_in": s_in, "s_out": s_out},
+        "roofline": {"bound": "tensor", "kernel": "MLP inference (k_mlp_infer, 64^3 points)",
+                     "achieved": achieved, "unit": "TFLOP/s", "peak": tpeak,
+                     "frac": achieved / tpeak, "traffic": None,
+                     "peak_source": f"{tsrc} bf16_tflops (burst)",
+                     "algorithmic_flops_per_launch": flops},
+        "gpu_launches": args.steps * launches["mlp"],
     }
 
 

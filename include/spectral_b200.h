@@ -73,7 +73,7 @@ int sns_convert(void* dst, int dst_prec, const void* src, int src_prec, int64_t 
  * src/FFT1D.cpp:95-101).  flags: SNS_FFT_NORMALISE | SNS_FFT_ZERO_NYQUIST. */
 int sns_fft3d(void* field, int64_t nx, int64_t ny, int64_t nz, int dir, int flags, int prec,
               void* stream);
-/* The same transform over up to 6 fields of equal shape in one batch. */
+/* The same transform over up to 12 fields of equal shape in one batch. */
 int sns_fft3d_many(void* const* fields, int nfields, int64_t nx, int64_t ny, int64_t nz,
                    int dir, int flags, int prec, void* stream);
 /* Scalar::forward(): transform(-1) + zeroHighModes (src/Scalar.cpp:208-215). */
@@ -156,7 +156,10 @@ int sns_ns_bootstrap(sns_ns* handle, const void* const V0[3], const void* const 
 /* Set the AB2 state directly: Fourier V1 and cross0 (= V0 x omega0). */
 int sns_ns_set_state(sns_ns* handle, const void* const V1[3], const void* const cross0[3]);
 /* Advance nsteps AB2 / projection / Crank-Nicolson steps (ns.cpp:167-217),
- * queued on the stepper's stream without host synchronisation. */
+ * queued on the stepper's stream without host synchronisation.  After the
+ * first step the step's launches are captured once as a CUDA graph (on a
+ * private stream) and replayed; environment SNS_GRAPH=0 at creation keeps
+ * direct launches.  Changing the closure drops the captured graph. */
 int sns_ns_step(sns_ns* handle, int nsteps);
 /* Copy out V1, omega1 = curl V1 and cross0 (any pointer may be NULL). */
 int sns_ns_get_state(sns_ns* handle, void* const V1[3], void* const omega1[3],
@@ -189,12 +192,15 @@ int sns_ns_pass_times(sns_ns* handle, double* total_ms, int* launches, int max);
  * velocity gradient A_ij = d_j u_i (real parts).  Models: SNS_CLOSURE_NONE
  * (the plain step), SNS_CLOSURE_SMAGORINSKY (nu_t = cs_delta2 sqrt(2 S:S),
  * cs_delta2 = (Cs Delta)^2), SNS_CLOSURE_MLP (nu_t from the packed MLP at
- * `mlp`, device memory that must outlive the steps).  Needs nx*ny*nz to be a
- * multiple of 32; allocates six more work fields on first use. */
+ * `mlp`, device memory that must outlive the steps).  kc > 0 restricts the
+ * run to the modes |k| <= kc (the LES cutoff: the nonlinear term, velocity
+ * and history of the modes beyond it are set to zero every step; with
+ * SNS_CLOSURE_NONE it applies to the plain step).  Needs nx*ny*nz to be a
+ * multiple of 32 for a model; allocates six more work fields on first use. */
 #define SNS_CLOSURE_NONE 0
 #define SNS_CLOSURE_SMAGORINSKY 1
 #define SNS_CLOSURE_MLP 2
-int sns_ns_set_closure(sns_ns* handle, int model, double cs_delta2, const void* mlp);
+int sns_ns_set_closure(sns_ns* handle, int model, double cs_delta2, const void* mlp, double kc);
 
 /* ---- learned closure: MLP 9 -> 64 -> 64 -> 1 on the tensor cores ----------
  * No reference counterpart.  FP32 master parameters (nparams floats: W1[64][16]
@@ -206,12 +212,13 @@ int sns_mlp_sizes(int64_t* nparams, int64_t* packed_bytes);
 int sns_mlp_pack(const float* master, double s_in, double s_out, void* packed, void* stream);
 /* nut[M] = the model at the M rows of X (device pointers). */
 int sns_mlp_infer(const void* packed, const void* X, int64_t M, float* nut, void* stream);
-/* Gradient of the mean squared error of softplus(z) against target (model
- * units, i.e. nu_t / s_out) over B samples (rows idx[0..B) of X, or rows
- * 0..B when idx is NULL).  grad: nparams + 1 floats (gradients, then the mean
- * loss), device memory.  Synchronises the stream. */
-int sns_mlp_grad(const void* packed, const void* X, const float* target, const int* idx, int64_t B,
-                 float* grad, void* stream);
+/* Gradient of the mean weighted squared error w (softplus(z) - target)^2
+ * (target in model units, i.e. nu_t / s_out; weight NULL = 1) over B samples
+ * (rows idx[0..B) of X, target and weight, or rows 0..B when idx is NULL).
+ * grad: nparams + 1 floats (gradients, then the mean loss), device memory.
+ * Synchronises the stream. */
+int sns_mlp_grad(const void* packed, const void* X, const float* target, const float* weight,
+                 const int* idx, int64_t B, float* grad, void* stream);
 /* One Adam step (bias correction for step >= 1) on the masters; refreshes
  * the packed copy's weights and biases. */
 int sns_mlp_adam(float* master, float* m, float* v, const float* grad, int step, double lr,
@@ -230,9 +237,11 @@ int sns_spectral_pad(const void* const* in, void* const* out, int nfields, int64
  * bf16: s_in times the filtered gradient) and nut (nc^3 floats: the pointwise
  * least-squares eddy viscosity -(tau^d : S) / (2 S : S) of the filtered SGS
  * stress tau_ij = filter(u_i u_j) - filter(ubar_i ubar_j), products formed on
- * the fine grid), and optionally the filtered coarse velocity Vc. */
+ * the fine grid); optionally the weight S : S of each pair (the stress
+ * residual |tau^d + 2 nu S|^2 is 4 S:S (nu - nut)^2 plus a constant) and the
+ * filtered coarse velocity Vc. */
 int sns_sgs_sample(const void* const V[3], int64_t nf, int64_t nc, double kc, double s_in,
-                   int prec, void* X, float* nut, void* const Vc[3], void* stream);
+                   int prec, void* X, float* nut, float* weight, void* const Vc[3], void* stream);
 /* E[k] = sum over the shell round(|k|) = k of |V_hat|^2 / (2 N^2), k < nshell
  * (device doubles), so that sum_k E[k] = <|u|^2> / 2. */
 int sns_energy_spectrum(const void* const V[3], int64_t nx, int64_t ny, int64_t nz, int prec,

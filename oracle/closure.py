@@ -142,16 +142,17 @@ class MLP:
         z, _ = self.forward(X)
         return self.s_out * softplus(z)
 
-    def loss_and_grads(self, X, t, rounding=True):
-        """Mean squared error of softplus(z) against targets t (model units)
-        and its gradients, with the GPU's BF16 rounding of the backward
-        operands (dPre2, dPre1)."""
+    def loss_and_grads(self, X, t, rounding=True, w=None):
+        """Mean weighted squared error w (softplus(z) - t)^2 (targets in model
+        units, w = 1 when None) and its gradients, with the GPU's BF16 rounding
+        of the backward operands (dPre2, dPre1)."""
         r = bf16 if rounding else (lambda a: np.asarray(a, dtype=np.float64))
         B = X.shape[0]
+        w = np.ones(B) if w is None else np.asarray(w, dtype=np.float64)
         z, (Xb, pre1, h1, pre2, h2) = self.forward(X, rounding)
         y = softplus(z)
-        loss = float(np.mean((y - t) ** 2))
-        dz = (2.0 / B) * (y - t) * sigmoid(z)
+        loss = float(np.mean(w * (y - t) ** 2))
+        dz = (2.0 / B) * w * (y - t) * sigmoid(z)
         w3b = r(self.w3)
         g = {"w3": h2.T @ dz, "b3": np.array([dz.sum()])}
         dpre2 = (dz[:, None] * w3b[None, :]) * (pre2 > 0)
@@ -194,11 +195,14 @@ def nonlinear(V, model="plain", params=None):
     return [zero_nyquist(x) for x in out]
 
 
-def update(V1, c0, c1, nu, dt):
-    """ns.cpp:170-187 on Fourier fields."""
+def update(V1, c0, c1, nu, dt, kc=None):
+    """ns.cpp:170-187 on Fourier fields.  With a cutoff kc the modes |k| > kc
+    are not evolved: their nonlinear term, velocity and history are zero."""
     KX, KY, KZ = kgrid(V1[0].shape)
     K = (KX, KY, KZ)
     k2 = KX ** 2 + KY ** 2 + KZ ** 2
+    if kc is not None:
+        c1 = [np.where(k2 > kc * kc, 0, c) for c in c1]
     hK = dt / 2
     F = [hK * (3 * c1[d] - c0[d]) for d in range(3)]
     lap = [nu * hK * (-k2 * V1[d]) for d in range(3)]
@@ -211,15 +215,18 @@ def update(V1, c0, c1, nu, dt):
     for d in range(3):
         vh = V1[d] + F[d] - 1j * K[d] * G
         vv = vh + lap[d]
-        out.append(np.where(nz, vv / den, vv))
-    return out
+        vv = np.where(nz, vv / den, vv)
+        if kc is not None:
+            vv = np.where(k2 > kc * kc, 0, vv)
+        out.append(vv)
+    return (out, c1) if kc is not None else out
 
 
 class LES:
     """FP64 LES stepper: state (V1, cross0) as in exec/ns.cpp."""
 
-    def __init__(self, nu, dt, model="plain", params=None):
-        self.nu, self.dt, self.model, self.params = nu, dt, model, params
+    def __init__(self, nu, dt, model="plain", params=None, kc=None):
+        self.nu, self.dt, self.model, self.params, self.kc = nu, dt, model, params, kc
         self.V1 = self.c0 = None
 
     def set_state(self, V1, cross0):
@@ -229,7 +236,10 @@ class LES:
     def step(self, n=1):
         for _ in range(n):
             c1 = nonlinear(self.V1, self.model, self.params)
-            self.V1 = update(self.V1, self.c0, c1, self.nu, self.dt)
+            if self.kc is None:
+                self.V1 = update(self.V1, self.c0, c1, self.nu, self.dt)
+            else:
+                self.V1, c1 = update(self.V1, self.c0, c1, self.nu, self.dt, self.kc)
             self.c0 = c1
 
 
@@ -262,8 +272,9 @@ def sgs_sample(Vf, nc, kc, s_in, eps=1e-30):
     gradient (points, 16) and the eddy viscosity nu_t of the least-squares
     projection of the filtered SGS stress onto -2 nu_t S (pointwise):
       tau_ij = filter(u_i u_j) - filter(ubar_i ubar_j) on the fine grid,
-      nu_t = -(tau^d : Sbar) / (2 Sbar : Sbar).
-    Also returns the coarse filtered velocity."""
+      nu_t = -(tau^d : Sbar) / (2 Sbar : Sbar),
+    with the weight Sbar : Sbar of each pair.  Also returns the coarse
+    filtered velocity."""
     nf = Vf[0].shape[0]
     Vc = [truncate(v, nc, kc) for v in Vf]
     u = [inverse(v) for v in Vf]
@@ -285,7 +296,7 @@ def sgs_sample(Vf, nc, kc, s_in, eps=1e-30):
             num = num + td * S
             den = den + S * S
     nut = -num / (2.0 * den + eps)
-    return features(Ar, s_in), np.ravel(nut), Vc
+    return features(Ar, s_in), np.ravel(nut), np.ravel(den), Vc
 
 
 def spectrum(V):

@@ -76,15 +76,15 @@ SIGNATURES = {
     "sns_ns_launches_per_step": ([_vp], _int),
     "sns_ns_profile": ([_vp, _int], _int),
     "sns_ns_pass_times": ([_vp, C.POINTER(_dbl), C.POINTER(_int), _int], _int),
-    "sns_ns_set_closure": ([_vp, _int, _dbl, _vp], _int),
+    "sns_ns_set_closure": ([_vp, _int, _dbl, _vp, _dbl], _int),
     "sns_mlp_sizes": ([C.POINTER(_i64), C.POINTER(_i64)], _int),
     "sns_mlp_pack": ([_vp, _dbl, _dbl, _vp, _vp], _int),
     "sns_mlp_infer": ([_vp, _vp, _i64, _vp, _vp], _int),
-    "sns_mlp_grad": ([_vp, _vp, _vp, _vp, _i64, _vp, _vp], _int),
+    "sns_mlp_grad": ([_vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp], _int),
     "sns_mlp_adam": ([_vp, _vp, _vp, _vp, _int, _dbl, _dbl, _dbl, _dbl, _vp, _vp], _int),
     "sns_spectral_truncate": ([_vp3, _vp3, _int, _i64, _i64, _dbl, _int, _vp], _int),
     "sns_spectral_pad": ([_vp3, _vp3, _int, _i64, _i64, _int, _vp], _int),
-    "sns_sgs_sample": ([_vp3, _i64, _i64, _dbl, _dbl, _int, _vp, _vp, _vp3, _vp], _int),
+    "sns_sgs_sample": ([_vp3, _i64, _i64, _dbl, _dbl, _int, _vp, _vp, _vp, _vp3, _vp], _int),
     "sns_energy_spectrum": ([_vp3, _i64, _i64, _i64, _int, _vp, _int, _vp], _int),
     "sns_ens_create": ([C.POINTER(_vp), _int, C.POINTER(_i64), C.POINTER(_dbl), _dbl, _int, _int,
                         _vp], _int),

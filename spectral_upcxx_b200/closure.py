@@ -98,12 +98,13 @@ class MLPModel:
         N.call("sns_mlp_infer", _p(self.packed), _p(X), X.shape[0], _p(out), _stream(X))
         return out
 
-    def gradient(self, X, target, idx=None, batch=None):
-        """(mean loss, gradient vector) of the MSE of softplus(z) against target
-        (model units) over rows idx of X (or the first `batch` rows)."""
+    def gradient(self, X, target, idx=None, batch=None, weight=None):
+        """Gradient vector (its last entry: the mean loss) of the weighted
+        squared error of softplus(z) against target (model units) over rows
+        idx of X (or the first `batch` rows)."""
         B = int(idx.numel()) if idx is not None else int(batch or X.shape[0])
-        N.call("sns_mlp_grad", _p(self.packed), _p(X), _p(target), _p(idx), B, _p(self.grad),
-               _stream(X))
+        N.call("sns_mlp_grad", _p(self.packed), _p(X), _p(target), _p(weight), _p(idx), B,
+               _p(self.grad), _stream(X))
         return self.grad
 
     def adam(self, lr, beta1=0.9, beta2=0.999, eps=1e-8):
@@ -134,20 +135,22 @@ def pad(fields, nf: int):
     return out
 
 
-def sgs_sample(V, nc: int, kc: float, s_in: float, X=None, nut=None, Vc=None):
+def sgs_sample(V, nc: int, kc: float, s_in: float, Vc=None):
     """Training pairs of one fine Fourier velocity (see sns_sgs_sample).
-    Returns (X (nc^3, 16) bf16, nu_t (nc^3,) float32, Vc or None)."""
+    Returns (X (nc^3, 16) bf16, nu_t (nc^3,) float32, weight S:S (nc^3,)
+    float32, Vc or None)."""
     V = list(V)
     p = _same(V)
     nf = V[0].shape[0]
     dev = V[0].device
     n3 = nc ** 3
-    X = X if X is not None else torch.empty((n3, KPAD), dtype=torch.bfloat16, device=dev)
-    nut = nut if nut is not None else torch.empty(n3, dtype=torch.float32, device=dev)
+    X = torch.empty((n3, KPAD), dtype=torch.bfloat16, device=dev)
+    nut = torch.empty(n3, dtype=torch.float32, device=dev)
+    w = torch.empty(n3, dtype=torch.float32, device=dev)
     vc = N.ptrs([v.data_ptr() for v in Vc]) if Vc is not None else None
     N.call("sns_sgs_sample", N.ptrs([v.data_ptr() for v in V]), nf, nc, float(kc), float(s_in), p,
-           _p(X), _p(nut), vc, _stream(V[0]))
-    return X, nut, Vc
+           _p(X), _p(nut), _p(w), vc, _stream(V[0]))
+    return X, nut, w, Vc
 
 
 def spectrum(V, nshell=None):
@@ -170,9 +173,9 @@ def spectrum_error(E, Eref, kmax):
     return float(np.mean(np.abs(E[k] - Eref[k]) / Eref[k]))
 
 
-def smagorinsky_cs_delta2(cs: float, nc: int) -> float:
-    """(Cs Delta)^2 with Delta the coarse grid spacing 2 pi / nc."""
-    return (cs * 2 * math.pi / nc) ** 2
+def smagorinsky_cs_delta2(cs: float, kc: float) -> float:
+    """(Cs Delta)^2 with Delta = pi / kc, the width of the sharp cutoff."""
+    return (cs * math.pi / kc) ** 2
 
 
 def _initial(n, seed, dtype, device):
@@ -184,9 +187,10 @@ def dns_dataset(S, nf, nc, kc, seeds, nu, dt, steps, every, dtype=torch.complex6
                 s_in=None, log=None):
     """Run fine DNS from each seed for `steps` steps and take a filtered
     training sample every `every` steps.  Returns X (M, 16) bf16, nu_t (M,)
-    float32, s_in (the feature scale: 1 / rms of the first snapshot's
-    gradient when not given) and the number of snapshots."""
-    Xs, ts = [], []
+    float32, the weights S:S / mean(S:S) (M,) float32, s_in (the feature
+    scale: 1 / rms of the first snapshot's gradient when not given) and the
+    number of snapshots."""
+    Xs, ts, ws = [], [], []
     snaps = 0
     for seed in seeds:
         V0 = _initial(nf, seed, dtype, device)
@@ -199,27 +203,31 @@ def dns_dataset(S, nf, nc, kc, seeds, nu, dt, steps, every, dtype=torch.complex6
                 continue
             V1 = st.velocity()
             if s_in is None:
-                X0, _, _ = sgs_sample(V1, nc, kc, 1.0)
+                X0, _, _, _ = sgs_sample(V1, nc, kc, 1.0)
                 s_in = 1.0 / float(X0[:, :NIN].float().pow(2).mean().sqrt())
-            X, t, _ = sgs_sample(V1, nc, kc, s_in)
+            X, t, w, _ = sgs_sample(V1, nc, kc, s_in)
             Xs.append(X)
             ts.append(t)
+            ws.append(w)
             snaps += 1
         st.close()
         if log:
             log(f"seed {seed}: {snaps} snapshots so far")
-    return torch.cat(Xs), torch.cat(ts), s_in, snaps
+    w = torch.cat(ws)
+    w /= w.mean()
+    return torch.cat(Xs), torch.cat(ts), w, s_in, snaps
 
 
-def train(model, X, nut, steps, batch, lr, seed=0, log=None):
-    """Adam on the MSE of nu_t / s_out over random batches (with replacement)."""
+def train(model, X, nut, steps, batch, lr, weight=None, seed=0, log=None):
+    """Adam on the (weighted) mean squared error of nu_t / s_out over random
+    batches (with replacement)."""
     g = torch.Generator(device=X.device).manual_seed(seed)
     target = (nut / model.s_out).contiguous()
     M = X.shape[0]
     losses = []
     for it in range(steps):
         idx = torch.randint(0, M, (batch,), device=X.device, generator=g, dtype=torch.int32)
-        grad = model.gradient(X, target, idx=idx)
+        grad = model.gradient(X, target, idx=idx, weight=weight)
         model.adam(lr if it < steps * 3 // 4 else lr / 10)
         if it % max(1, steps // 20) == 0 or it == steps - 1:
             losses.append((it, float(grad[-1])))
@@ -228,15 +236,18 @@ def train(model, X, nut, steps, batch, lr, seed=0, log=None):
     return losses
 
 
-def coarse_run(S, Vc0, nu, dt, steps, model=None, csd2=0.0, dtype=torch.complex64):
-    """Coarse run from the filtered field Vc0 with no closure, Smagorinsky
-    (csd2 > 0, model None) or the MLP (model).  Returns the final velocity."""
+def coarse_run(S, Vc0, nu, dt, steps, model=None, csd2=0.0, kc=0.0, dtype=torch.complex64):
+    """Coarse run from the filtered field Vc0 over the modes |k| <= kc (all
+    modes when kc = 0) with no closure, Smagorinsky (csd2 > 0, model None) or
+    the MLP (model).  Returns the final velocity."""
     n = Vc0[0].shape[0]
     st = S.NSStepper((n, n, n), nu, dt, dtype, device=Vc0[0].device)
     if model is not None:
-        st.set_closure(N.SNS_CLOSURE_MLP, mlp=model.packed)
+        st.set_closure(N.SNS_CLOSURE_MLP, mlp=model.packed, kc=kc)
     elif csd2 > 0:
-        st.set_closure(N.SNS_CLOSURE_SMAGORINSKY, cs_delta2=csd2)
+        st.set_closure(N.SNS_CLOSURE_SMAGORINSKY, cs_delta2=csd2, kc=kc)
+    else:
+        st.set_closure(N.SNS_CLOSURE_NONE, kc=kc)
     st.bootstrap(Vc0, S.curl(Vc0))
     st.step(steps)
     V = st.velocity()
@@ -250,7 +261,8 @@ def evaluate(S, model, nf, nc, kc, seeds, nu, dt, steps, cs=0.17, dtype=torch.co
     filtered fine DNS, for the plain, Smagorinsky and MLP coarse runs, plus
     the steps/s of the coarse MLP run and of the fine DNS."""
     res = {"plain": [], "smagorinsky": [], "mlp": []}
-    csd2 = smagorinsky_cs_delta2(cs, nc)
+    spectra = {}
+    csd2 = smagorinsky_cs_delta2(cs, kc)
     t_dns = t_les = 0.0
     for seed in seeds:
         V0 = _initial(nf, seed, dtype, device)
@@ -267,12 +279,18 @@ def evaluate(S, model, nf, nc, kc, seeds, nu, dt, steps, cs=0.17, dtype=torch.co
         for name, kw in (("plain", {}), ("smagorinsky", {"csd2": csd2}), ("mlp", {"model": model})):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            V = coarse_run(S, Vc0, nu, dt, steps, dtype=dtype, **kw)
+            V = coarse_run(S, Vc0, nu, dt, steps, kc=kc, dtype=dtype, **kw)
             torch.cuda.synchronize()
             if name == "mlp":
                 t_les += time.perf_counter() - t0
-            res[name].append(spectrum_error(spectrum(V), Eref, int(kc)))
+            E = spectrum(V)
+            res[name].append(spectrum_error(E, Eref, int(kc)))
+            if seed == seeds[0]:
+                spectra[name] = E[:int(kc) + 1].tolist()
+        if seed == seeds[0]:
+            spectra["filtered_dns"] = Eref[:int(kc) + 1].tolist()
     out = {k: float(np.mean(v)) for k, v in res.items()}
+    out["spectra_first_seed"] = spectra
     out["dns_steps_per_s"] = steps * len(seeds) / t_dns
     out["mlp_run_steps_per_s"] = steps * len(seeds) / t_les
     return out

@@ -1,6 +1,7 @@
 // extern "C" entry points of include/spectral_b200.h: argument checking,
 // the caching device pool, and the fused NS stepper object.
 #include <cuda_runtime.h>
+#include <stdlib.h>
 
 #include <algorithm>
 #include <map>
@@ -211,7 +212,64 @@ struct sns_ns {
   bool profiling = false;
   int recorded = 0;
   std::vector<cudaEvent_t> events;  // (kNSPasses + 1) per recorded step
+  // one step captured as a CUDA graph (on a private stream, after one eager
+  // step has set up twiddles and kernel attributes), replayed on s
+  bool use_graph = true;
+  bool eager_done = false;
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
 };
+
+namespace {
+
+void drop_graph(sns_ns* h) {
+  if (h->exec) cudaGraphExecDestroy(h->exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  h->exec = nullptr;
+  h->graph = nullptr;
+}
+
+// One step (plain or closure) queued on `s`.
+int step_on(sns_ns* h, cudaStream_t s, cudaEvent_t* ev) {
+  if (h->cl.model != CLOSURE_NONE) {
+    void* U[kLESWork];
+    for (int i = 0; i < 6; i++) {
+      U[i] = h->U[i];
+      U[6 + i] = h->U2[i];
+    }
+    return les_step_once(h->pl, h->V, h->C0, U, h->stats_part, h->nu, h->dt, h->cl, s);
+  }
+  return ns_step_once(h->pl, h->V, h->C0, h->U, h->stats_part, h->sync_words, h->nu, h->dt, s,
+                      ev);
+}
+
+int capture_step(sns_ns* h) {
+  int rc = OK;
+  if (!h->cap)
+    rc = cuda_status(cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking),
+                     "sns_ns_step(capture stream)");
+  if (rc) return rc;
+  if ((rc = cuda_status(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal),
+                        "sns_ns_step(capture)")))
+    return rc;
+  const int src = step_on(h, h->cap, nullptr);
+  cudaGraph_t g = nullptr;
+  rc = cuda_status(cudaStreamEndCapture(h->cap, &g), "sns_ns_step(capture)");
+  if (src || rc) {
+    if (g) cudaGraphDestroy(g);
+    return src ? src : rc;
+  }
+  if ((rc = cuda_status(cudaGraphInstantiate(&h->exec, g, 0), "sns_ns_step(instantiate)"))) {
+    cudaGraphDestroy(g);
+    h->exec = nullptr;
+    return rc;
+  }
+  h->graph = g;
+  return OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -276,7 +334,7 @@ int sns_fft3d_many(void* const* fields, int nfields, int64_t nx, int64_t ny, int
     return ERR_ARG;
   }
   if (!fields || nfields < 1 || nfields > kMaxFields) {
-    set_error("sns_fft3d_many: 1..6 fields");
+    set_error("sns_fft3d_many: 1..12 fields");
     return ERR_ARG;
   }
   for (int i = 0; i < nfields; i++)
@@ -508,6 +566,8 @@ int sns::ns_create_tuned(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, do
     return rc;
   }
   h->stepped = false;
+  // SNS_GRAPH=0 launches every step's kernels directly
+  if (const char* e = getenv("SNS_GRAPH")) h->use_graph = e[0] != '0';
   *handle = h;
   return OK;
 }
@@ -527,6 +587,8 @@ int sns_ns_destroy(sns_ns* h) {
   pool_free(h->sync_words);
   for (int i = 0; i < 6; i++) pool_free(h->U2[i]);
   for (cudaEvent_t e : h->events) cudaEventDestroy(e);
+  drop_graph(h);
+  if (h->cap) cudaStreamDestroy(h->cap);
   delete h;
   return OK;
 }
@@ -567,18 +629,25 @@ int sns_ns_step(sns_ns* h, int nsteps) {
     set_error("sns_ns_step: negative step count");
     return ERR_ARG;
   }
-  if (h->cl.model != CLOSURE_NONE) {
-    void* U[kLESWork];
-    for (int i = 0; i < 6; i++) {
-      U[i] = h->U[i];
-      U[6 + i] = h->U2[i];
-    }
+  if (!h->profiling) {
     for (int t = 0; t < nsteps; t++) {
-      int rc = les_step_once(h->pl, h->V, h->C0, U, h->stats_part, h->nu, h->dt, h->cl, h->s);
+      int rc = OK;
+      if (h->use_graph && h->eager_done && !h->exec) rc = capture_step(h);
+      if (rc) return rc;
+      if (h->exec) {
+        rc = cuda_status(cudaGraphLaunch(h->exec, h->s), "sns_ns_step(graph)");
+      } else {
+        rc = step_on(h, h->s, nullptr);
+        h->eager_done = true;
+      }
       if (rc) return rc;
       h->stepped = true;
     }
     return OK;
+  }
+  if (h->cl.model != CLOSURE_NONE) {
+    set_error("sns_ns_step: per-pass profiling covers the plain step only");
+    return ERR_UNSUPPORTED;
   }
   for (int t = 0; t < nsteps; t++) {
     cudaEvent_t* ev = nullptr;
@@ -700,8 +769,12 @@ int sns_ns_launches_per_step(sns_ns* h) {
   return h->cl.model != CLOSURE_NONE ? kLESLaunches : h->pl.passes;
 }
 
-int sns_ns_set_closure(sns_ns* h, int model, double cs_delta2, const void* mlp) {
+int sns_ns_set_closure(sns_ns* h, int model, double cs_delta2, const void* mlp, double kc) {
   if (!nonnull(h, "sns_ns_set_closure")) return ERR_ARG;
+  if (!(kc >= 0)) {
+    set_error("sns_ns_set_closure: the cutoff must be >= 0 (0: none)");
+    return ERR_ARG;
+  }
   if (model != SNS_CLOSURE_NONE && model != SNS_CLOSURE_SMAGORINSKY && model != SNS_CLOSURE_MLP) {
     set_error("sns_ns_set_closure: unknown model");
     return ERR_ARG;
@@ -730,6 +803,9 @@ int sns_ns_set_closure(sns_ns* h, int model, double cs_delta2, const void* mlp) 
   h->cl.model = model;
   h->cl.csd2 = cs_delta2;
   h->cl.mlp = mlp;
+  h->pl.kc2 = kc > 0 ? kc * kc : 1e300;
+  drop_graph(h);
+  h->eager_done = false;
   return OK;
 }
 

@@ -118,6 +118,7 @@ __device__ __forceinline__ void ens_item(const EnsClass* __restrict__ k,
       a.hK = box->hK;
       a.nuhK = box->nuhK;
       a.stats = box->stats;
+      a.kc2 = 1e300;
     }
     __syncthreads();
     zfwd_update_tile<T, L>(a, tw, blk, (int)blockDim.x, sm, red);

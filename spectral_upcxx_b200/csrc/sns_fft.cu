@@ -1,7 +1,7 @@
 // Batched line-FFT passes: the replacement for FFT1D's per-line FFTW calls
 // (src/FFT1D.cpp:95-101) and for the three 1D phases of Scalar::transform
 // (src/Scalar.cpp:419-566).  One kernel launch transforms every line along
-// one axis of up to six fields.  A CTA owns a tile of W adjacent lines x G
+// one axis of up to twelve fields.  A CTA owns a tile of W adjacent lines x G
 // groups: its threads load the tile straight into registers with coalesced
 // reads, run the register/shared-memory Stockham line FFT, and store the
 // tile back with the epilogue (1/N scaling, Nyquist zeroing) applied.  Tiles
@@ -178,7 +178,7 @@ static int dispatch_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int f
 int run_line_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags, double scale,
                   int prec, cudaStream_t stream, int prologue) {
   if (f.n < 1 || f.n > kMaxFields) {
-    set_error("line pass: 1..6 fields");
+    set_error("line pass: 1..12 fields");
     return ERR_ARG;
   }
   if (geo.TA * geo.TB == 0) return OK;

@@ -10,7 +10,7 @@
 
 namespace sns {
 
-constexpr int kMaxFields = 6;
+constexpr int kMaxFields = 12;
 constexpr int kMaxLine = 4096;
 
 // Epilogue flags of a pass.

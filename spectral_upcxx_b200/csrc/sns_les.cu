@@ -5,13 +5,13 @@
 // step adds the divergence of the eddy stress tau_ij = 2 nu_t S_ij to the
 // nonlinear term cross1 (ns.cpp:203-206) and is otherwise the ns.cpp step:
 //
-//   z-inverse of V and grad V (i k_j V_i)   2 launches x 6 fields
-//   y-inverse                               2 x 6
-//   x-inverse                               2 x 6
+//   z-inverse of V and grad V (i k_j V_i)   1 launch x 12 fields
+//   y-inverse                               1 x 12
+//   x-inverse                               1 x 12
 //   closure: nu_t (Smagorinsky or the MLP on the tensor cores), u x omega
 //            and tau_ij pointwise           1
-//   x-forward, y-forward of u x omega, tau  2 x (6 + 3)
-//   z-forward of tau                        1
+//   x-forward, y-forward of u x omega, tau  2 x 9
+//   z-forward of tau                        1 x 6
 //   z-forward of u x omega + i k_j tau_ij + the AB2 / projection / CN
 //   update                                  1
 #include <cuda_bf16.h>
@@ -123,8 +123,10 @@ __global__ void __launch_bounds__(kClWarps * 32) k_les_closure(const ClosureArgs
 
 template <typename T>
 int launch_closure(const ClosureArgs& a, int model, cudaStream_t s) {
+  // MLP: a resident grid (two CTAs per SM), so each CTA loads the weights once
   const int64_t groups = a.n / 32;
-  const int blocks = (int)std::min<int64_t>((groups + kClWarps - 1) / kClWarps, 8 * 148);
+  const int cap = model == CLOSURE_MLP ? 2 * sm_count() : 8 * sm_count();
+  const int blocks = (int)std::min<int64_t>((groups + kClWarps - 1) / kClWarps, cap);
   if (model == CLOSURE_MLP)
     k_les_closure<T, CLOSURE_MLP><<<blocks, kClWarps * 32, 0, s>>>(a);
   else
@@ -158,12 +160,9 @@ int les_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* c
     return run_line_pass(g, f, sign, 0, 1.0, prec, s, pro);
   };
   // inverse of V (3) and grad V (9): z with the gradient prologue, then y, x
-  if ((rc = pass(2, 0, 6, +1, PRO_GRAD12, true))) return rc;
-  if ((rc = pass(2, 6, 6, +1, PRO_GRAD12, true))) return rc;
-  for (int axis : {1, 0}) {
-    if ((rc = pass(axis, 0, 6, +1, PRO_LOAD, false))) return rc;
-    if ((rc = pass(axis, 6, 6, +1, PRO_LOAD, false))) return rc;
-  }
+  if ((rc = pass(2, 0, kLESWork, +1, PRO_GRAD12, true))) return rc;
+  for (int axis : {1, 0})
+    if ((rc = pass(axis, 0, kLESWork, +1, PRO_LOAD, false))) return rc;
   // pointwise closure
   {
     ClosureArgs a{};
@@ -177,10 +176,8 @@ int les_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* c
     if (rc) return rc;
   }
   // forward x, y of u x omega (U[0..2]) and tau (U[3..8]); z of tau
-  for (int axis : {0, 1}) {
-    if ((rc = pass(axis, 3, 6, -1, PRO_LOAD, false))) return rc;
-    if ((rc = pass(axis, 0, 3, -1, PRO_LOAD, false))) return rc;
-  }
+  for (int axis : {0, 1})
+    if ((rc = pass(axis, 0, 9, -1, PRO_LOAD, false))) return rc;
   if ((rc = pass(2, 3, 6, -1, PRO_LOAD, false))) return rc;
   // z-forward of u x omega + div tau + update
   UpdateArgs a{};
@@ -199,6 +196,7 @@ int les_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* c
   a.hK = dt / 2;
   a.nuhK = nu * dt / 2;
   a.stats = stats;
+  a.kc2 = pl.kc2;
   return ns_update(pl, a, true, s);
 }
 
@@ -281,6 +279,7 @@ struct TargetArgs {
   double s_in;
   __nv_bfloat16* X;  // [n][16]
   float* nut;        // [n]
+  float* weight;     // [n] S:S (may be null)
 };
 
 // Features s_in * Re A (padded to 16) and the pointwise least-squares eddy
@@ -302,6 +301,7 @@ __global__ void k_sgs_target(const TargetArgs a) {
                        2.0 * (t6[3] * Sxy + t6[4] * Sxz + t6[5] * Syz);
     const double den = Sxx * Sxx + Syy * Syy + Szz * Szz + 2.0 * (Sxy * Sxy + Sxz * Sxz + Syz * Syz);
     a.nut[p] = (float)(-num / (2.0 * den + 1e-30));
+    if (a.weight) a.weight[p] = (float)den;
     __nv_bfloat16* row = a.X + p * kMlpK1;
 #pragma unroll
     for (int q = 0; q < kMlpK1; q++)
@@ -409,7 +409,7 @@ int sns_spectral_truncate(const void* const* in, void* const* out, int nfields, 
   if (nfields < 1 || nfields > kMaxFields || !fields_ok(in, nfields, "sns_spectral_truncate") ||
       !fields_ok((const void* const*)out, nfields, "sns_spectral_truncate") ||
       (prec != PREC_C64 && prec != PREC_C128)) {
-    if (nfields < 1 || nfields > kMaxFields) set_error("sns_spectral_truncate: 1..6 fields");
+    if (nfields < 1 || nfields > kMaxFields) set_error("sns_spectral_truncate: 1..12 fields");
     if (prec != PREC_C64 && prec != PREC_C128) set_error("sns_spectral_truncate: bad precision");
     return ERR_ARG;
   }
@@ -423,7 +423,7 @@ int sns_spectral_pad(const void* const* in, void* const* out, int nfields, int64
   if (nfields < 1 || nfields > kMaxFields || !fields_ok(in, nfields, "sns_spectral_pad") ||
       !fields_ok((const void* const*)out, nfields, "sns_spectral_pad") ||
       (prec != PREC_C64 && prec != PREC_C128)) {
-    if (nfields < 1 || nfields > kMaxFields) set_error("sns_spectral_pad: 1..6 fields");
+    if (nfields < 1 || nfields > kMaxFields) set_error("sns_spectral_pad: 1..12 fields");
     if (prec != PREC_C64 && prec != PREC_C128) set_error("sns_spectral_pad: bad precision");
     return ERR_ARG;
   }
@@ -433,7 +433,8 @@ int sns_spectral_pad(const void* const* in, void* const* out, int nfields, int64
 }
 
 int sns_sgs_sample(const void* const V[3], int64_t nf, int64_t nc, double kc, double s_in,
-                   int prec, void* X, float* nut, void* const Vc_out[3], void* stream) {
+                   int prec, void* X, float* nut, float* weight, void* const Vc_out[3],
+                   void* stream) {
   if (!fields_ok(V, 3, "sns_sgs_sample") || !X || !nut ||
       (prec != PREC_C64 && prec != PREC_C128)) {
     if (!X || !nut) set_error("sns_sgs_sample: null output");
@@ -504,6 +505,7 @@ int sns_sgs_sample(const void* const V[3], int64_t nf, int64_t nc, double kc, do
     ta.s_in = s_in;
     ta.X = reinterpret_cast<__nv_bfloat16*>(X);
     ta.nut = nut;
+    ta.weight = weight;
     if (prec == PREC_C128)
       k_sgs_target<double><<<grid_for(nc3), 256, 0, s>>>(ta);
     else

@@ -43,8 +43,9 @@ struct TrainSmem {
 
 __global__ void __launch_bounds__(kTrainRows)
     k_mlp_grad(const MlpPacked* __restrict__ P, const __nv_bfloat16* __restrict__ X,
-               const float* __restrict__ target, const int* __restrict__ idx, int64_t B,
-               float inv_batch, float* __restrict__ part) {
+               const float* __restrict__ target, const float* __restrict__ weight,
+               const int* __restrict__ idx, int64_t B, float inv_batch,
+               float* __restrict__ part) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
@@ -99,8 +100,9 @@ __global__ void __launch_bounds__(kTrainRows)
       const float z = T.z[h];
       const float y = softplus_f(z);
       const float d = v ? y - target[r] : 0.f;
-      if (t == 0) loss += d * d;
-      dz[h] = 2.f * inv_batch * d / (1.f + expf(-z));
+      const float wt = (v && weight) ? weight[r] : 1.f;
+      if (t == 0) loss += wt * d * d;
+      dz[h] = 2.f * inv_batch * wt * d / (1.f + expf(-z));
       if (t == 0) db3 += dz[h];
     }
     // layer 3 and layer-2 activation gradients; dPre2 as bf16 A fragments
@@ -361,8 +363,8 @@ __global__ void __launch_bounds__(256)
 
 namespace {
 
-int grad_launch(const void* packed, const void* X, const float* t, const int* idx, int64_t B,
-                float* grad, cudaStream_t s) {
+int grad_launch(const void* packed, const void* X, const float* t, const float* w,
+                const int* idx, int64_t B, float* grad, cudaStream_t s) {
   const int64_t nb = (B + kTrainRows - 1) / kTrainRows;
   if (nb > (1 << 24)) {
     set_error("sns_mlp_grad: batch too large");
@@ -386,7 +388,7 @@ int grad_launch(const void* packed, const void* X, const float* t, const int* id
   }
   const float inv = (float)(1.0 / (double)B);
   k_mlp_grad<<<(unsigned)nb, kTrainRows, sizeof(TrainSmem), s>>>(
-      reinterpret_cast<const MlpPacked*>(packed), reinterpret_cast<const __nv_bfloat16*>(X), t,
+      reinterpret_cast<const MlpPacked*>(packed), reinterpret_cast<const __nv_bfloat16*>(X), t, w,
       idx, B, inv, reinterpret_cast<float*>(part));
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) {
@@ -439,13 +441,14 @@ int sns_mlp_infer(const void* packed, const void* X, int64_t M, float* nut, void
   return OK;
 }
 
-int sns_mlp_grad(const void* packed, const void* X, const float* target, const int* idx,
-                 int64_t B, float* grad, void* stream) {
+int sns_mlp_grad(const void* packed, const void* X, const float* target, const float* weight,
+                 const int* idx, int64_t B, float* grad, void* stream) {
   if (!packed || !X || !target || !grad || B < 1) {
     set_error("sns_mlp_grad: bad arguments");
     return ERR_ARG;
   }
-  return grad_launch(packed, X, target, idx, B, grad, reinterpret_cast<cudaStream_t>(stream));
+  return grad_launch(packed, X, target, weight, idx, B, grad,
+                     reinterpret_cast<cudaStream_t>(stream));
 }
 
 int sns_mlp_adam(float* master, float* m, float* v, const float* grad, int step, double lr,

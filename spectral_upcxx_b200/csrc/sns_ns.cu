@@ -216,6 +216,7 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW) {
   if (const char* e = getenv("SNS_XY_CHUNK")) pl.xy_chunk = atoi(e);
   pl.passes = (pl.use_xy || (pl.xy_chunk > 0 && pl.xy_chunk < nz)) ? 3 : 5;
   pl.lineW = lineW > 0 ? lineW : 0;
+  pl.kc2 = 1e300;
   return OK;
 }
 
@@ -308,6 +309,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     a.hK = dt / 2;
     a.nuhK = nu * dt / 2;
     a.stats = stats;
+    a.kc2 = pl.kc2;
     rc = ns_update(pl, a, false, s);
     if (rc) return rc;
     mark();

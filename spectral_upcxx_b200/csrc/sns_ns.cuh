@@ -17,6 +17,7 @@ struct NSPlan {
   int xy_chunk;       // planes per slab of the separate xy passes (0 = all)
   int lineW;          // adjacent lines per tile of the y/z line passes (0 = default)
   int passes;         // timed phases per step: z-inverse, xy, z-forward+update
+  double kc2;         // spectral cutoff |k|^2 <= kc2 of the evolved modes (1e300: none)
 };
 
 // zW > 0 and lineW > 0 select tuned tile widths (0 = defaults).

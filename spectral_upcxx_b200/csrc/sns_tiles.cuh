@@ -220,6 +220,7 @@ struct UpdateArgs {
   // SGS: Fourier eddy stress tau_xx, tau_yy, tau_zz, tau_xy, tau_xz, tau_yz
   // whose divergence i k_j tau_ij joins cross1 before the Nyquist zeroing
   const void* tau[6];
+  double kc2;  // spectral cutoff |k|^2 <= kc2 of an LES run (1e300: none)
 };
 
 // Tile `blk` holds the W z lines whose xy-plane offsets are blk*W .. blk*W+W-1.
@@ -266,7 +267,10 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
     const int x = (int)(xy & (a.nx - 1)), y = (int)(xy >> a.lx);
     const int64_t idx = xy + nxy * z;
     const T kx = (T)freq_i(x, a.nx), ky = (T)freq_i(y, a.ny), kz = (T)freq_i(z, a.nz);
-    const bool nyq = y == (a.ny >> 1) || x == (a.nx >> 1) || z == (a.nz >> 1);
+    const double k2d = (double)kx * kx + (double)ky * ky + (double)kz * kz;
+    // modes beyond the cutoff are not evolved (zero velocity and history)
+    const bool cut = k2d > a.kc2;
+    const bool nyq = cut || y == (a.ny >> 1) || x == (a.nx >> 1) || z == (a.nz >> 1);
     C c1[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) c1[d] = nyq ? mk((T)0, (T)0) : sm[(d * W + w) * RS + pad_pos(z)];
@@ -283,7 +287,6 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
     }
     const T kk[3] = {kx, ky, kz};
     const T k2 = kx * kx + ky * ky + kz * kz;
-    const double k2d = (double)kx * kx + (double)ky * ky + (double)kz * kz;
     // F = K/2 (3 c1 - c0)                      (ns.cpp:171)
     // lap1 = nu K/2 (-|k|^2 V1)                (ns.cpp:174)
     // s = V1 + lap1 + F; G = div s / (-|k|^2)  (ns.cpp:177-178)
@@ -321,6 +324,7 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
       } else {
         if (nonzero) vv = mk(vv.x / den_cn, vv.y / den_cn);
       }
+      if (cut) vv = mk((T)0, (T)0);
       Vn[d] = vv;
       Vp[d][idx] = vv;
       Cp[d][idx] = c1[d];
@@ -389,11 +393,22 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
   }
 }
 
+// Entry i of a pointer table in kernel parameters, selected with constant
+// indices so that the table is read in place rather than copied to local
+// memory for a dynamic index.
+__device__ __forceinline__ void* select_ptr(void* const (&a)[kMaxFields], int i) {
+  void* r = a[0];
+#pragma unroll
+  for (int k = 1; k < kMaxFields; k++)
+    if (i == k) r = a[k];
+  return r;
+}
+
 // Field accessor over a FieldPtrs held in kernel parameters.
 struct ParamFields {
   const FieldPtrs& f;
-  __device__ __forceinline__ const void* in(int i) const { return f.in[i]; }
-  __device__ __forceinline__ void* out(int i) const { return f.out[i]; }
+  __device__ __forceinline__ const void* in(int i) const { return select_ptr(f.in, i); }
+  __device__ __forceinline__ void* out(int i) const { return select_ptr(f.out, i); }
   __device__ __forceinline__ int first() const { return f.first; }
 };
 

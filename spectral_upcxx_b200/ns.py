@@ -63,13 +63,14 @@ class NSStepper:
         N.call("sns_ns_get_state", self.h, self._vec(V1), self._vec(w1), self._vec(c0))
         return {"V1": V1, "omega1": w1, "cross0": c0}
 
-    def set_closure(self, model: int, cs_delta2: float = 0.0, mlp=None):
+    def set_closure(self, model: int, cs_delta2: float = 0.0, mlp=None, kc: float = 0.0):
         """Eddy-viscosity closure of every following step: N.SNS_CLOSURE_NONE,
         _SMAGORINSKY (nu_t = cs_delta2 sqrt(2 S:S)) or _MLP (`mlp`: the packed
-        model tensor, kept alive by the caller)."""
+        model tensor, kept alive by the caller); kc > 0 evolves only the modes
+        |k| <= kc."""
         self._mlp = mlp
         N.call("sns_ns_set_closure", self.h, int(model), float(cs_delta2),
-               C.c_void_p(mlp.data_ptr()) if mlp is not None else None)
+               C.c_void_p(mlp.data_ptr()) if mlp is not None else None, float(kc))
 
     def velocity(self, out=None):
         """The Fourier velocity V1 (into `out`, three device fields, if given)."""

@@ -106,6 +106,6 @@ def test_sgs_target_of_a_resolved_field_vanishes(C):
     """A field already inside the cutoff has no subgrid stress."""
     n, nc, kc = 32, 16, 5
     V = [C.pad(C.truncate(v, nc, kc), n) for v in _field(n, 6)]
-    X, nut, Vc = C.sgs_sample(V, nc, kc, s_in=1.0)
+    X, nut, w, Vc = C.sgs_sample(V, nc, kc, s_in=1.0)
     assert X.shape == (nc ** 3, C.KPAD)
     assert np.max(np.abs(nut)) < 1e-10

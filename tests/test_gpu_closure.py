@@ -78,9 +78,11 @@ def test_mlp_gradient_matches_oracle(CO, CL, cuda):
     r = np.random.default_rng(5)
     t = np.abs(r.standard_normal(4096)).astype(np.float32)
     idx = r.integers(0, 4096, B).astype(np.int32)
+    wt = (0.5 + r.random(4096)).astype(np.float32)
     g = model.gradient(dev(X, torch.bfloat16, cuda), dev(t, torch.float32, cuda),
-                       idx=dev(idx, torch.int32, cuda)).cpu().double().numpy()
-    loss, ref = net.loss_and_grads(X[idx], t[idx].astype(np.float64))
+                       idx=dev(idx, torch.int32, cuda),
+                       weight=dev(wt, torch.float32, cuda)).cpu().double().numpy()
+    loss, ref = net.loss_and_grads(X[idx], t[idx].astype(np.float64), w=wt[idx])
     assert abs(g[-1] / loss - 1) < 1e-4
     o = {"W1": (0, 1024), "b1": (1024, 1088), "W2": (1088, 5184), "b2": (5184, 5248),
          "w3": (5248, 5312), "b3": (5312, 5313)}
@@ -129,10 +131,11 @@ def test_truncate_pad_spectrum_match_oracle(CO, CL, cuda):
 def test_sgs_sample_matches_oracle(CO, CL, cuda):
     n, nc, kc = 32, 16, 5
     V = _field(n, 9)
-    X, nut, Vc = CL.sgs_sample([dev(v, torch.complex128, cuda) for v in V], nc, kc, 0.7,
-                               Vc=[torch.empty((nc,) * 3, dtype=torch.complex128, device=cuda)
-                                   for _ in range(3)])
-    Xo, nuto, Vco = CO.sgs_sample(V, nc, kc, 0.7)
+    X, nut, w, Vc = CL.sgs_sample([dev(v, torch.complex128, cuda) for v in V], nc, kc, 0.7,
+                                  Vc=[torch.empty((nc,) * 3, dtype=torch.complex128, device=cuda)
+                                      for _ in range(3)])
+    Xo, nuto, wo, Vco = CO.sgs_sample(V, nc, kc, 0.7)
+    assert rel_l2(w.cpu().double().numpy(), wo) < 1e-6
     for a, b in zip(Vc, Vco):
         assert rel_l2(host(a), b) < 1e-14
     # nu_t divides by S:S, which amplifies the FFTs' FP64 rounding where the
@@ -158,13 +161,16 @@ def _les_pair(CO, S, cuda, n, nu, dt, seed):
     return st, [host(x) for x in s0["V1"]], [host(x) for x in s0["cross0"]]
 
 
-def test_smagorinsky_step_matches_oracle(CO, CL, sns, cuda):
+@pytest.mark.parametrize("kc", [0.0, 10.0])
+def test_smagorinsky_step_matches_oracle(CO, CL, sns, cuda, kc):
+    """complex128 closure step (with and without the spectral cutoff)."""
     n, nu, dt = 32, 1 / 400, 1e-3
-    csd2 = CL.smagorinsky_cs_delta2(0.17, n)
+    csd2 = CL.smagorinsky_cs_delta2(0.17, 10.0)
     st, V1, c0 = _les_pair(CO, sns, cuda, n, nu, dt, 10)
-    st.set_closure(sns._native.SNS_CLOSURE_SMAGORINSKY, cs_delta2=csd2)
-    assert st.launches_per_step() == 13
-    les = CO.LES(nu, dt, "smagorinsky", {"cs": 0.17, "delta": 2 * np.pi / n})
+    st.set_closure(sns._native.SNS_CLOSURE_SMAGORINSKY, cs_delta2=csd2, kc=kc)
+    assert st.launches_per_step() == 8
+    les = CO.LES(nu, dt, "smagorinsky", {"cs": 0.17, "delta": np.pi / 10.0},
+                 kc=kc if kc > 0 else None)
     les.set_state(V1, c0)
     st.step(3)
     les.step(3)
@@ -219,9 +225,26 @@ def test_closure_fp32_runs_and_dissipates(CL, sns, cuda):
         st = sns.NSStepper((n, n, n), nu, dt, torch.complex64)
         if name == "smag":
             st.set_closure(sns._native.SNS_CLOSURE_SMAGORINSKY,
-                           cs_delta2=CL.smagorinsky_cs_delta2(0.17, n))
+                           cs_delta2=CL.smagorinsky_cs_delta2(0.17, n / 3))
         st.bootstrap(V0, sns.curl(V0))
         st.step(50)
         e[name] = st.stats()["energy"]
         st.close()
     assert np.isfinite(e["smag"]) and e["smag"] < e["plain"]
+
+
+def test_trained_mlp_beats_the_unclosed_coarse_run(CL, sns, cuda):
+    """Scaled-down closure experiment: 128^3 DNS filtered at kc = 10 onto
+    32^3, a short training run, then 32^3 runs (modes |k| <= kc) from a
+    held-out seed judged by their energy spectrum against the filtered DNS
+    (shells 1..9)."""
+    nf, nc, kc, nu, dt = 128, 32, 10, 1 / 400, 1e-3
+    X, nut, w, s_in, snaps = CL.dns_dataset(sns, nf, nc, kc, seeds=[1, 2], nu=nu, dt=dt,
+                                            steps=400, every=10, device=cuda)
+    assert snaps == 80 and X.shape[0] == 80 * nc ** 3
+    s_out = float((nut * w).mean() / w.mean())
+    model = CL.MLPModel.init(0, s_in=s_in, s_out=s_out, device=cuda)
+    losses = CL.train(model, X, nut, steps=600, batch=16384, lr=2e-3, weight=w)
+    assert losses[-1][1] < losses[0][1]
+    res = CL.evaluate(sns, model, nf, nc, kc, seeds=[7], nu=nu, dt=dt, steps=400, device=cuda)
+    assert res["mlp"] < res["plain"], res
