@@ -753,8 +753,9 @@ def closure_bench(S, torch, dev, args, world, rank, hbm, peak_src, clocks):
     from spectral_upcxx_b200 import ic
     c = CLOSURE
     t0 = time.perf_counter()
+    calib = {}
     X, nut, w, s_in, snaps = CL.dns_dataset(S, c["nf"], c["nc"], c["kc"], c["train_seeds"], NU,
-                                            DT, c["steps"], c["every"], device=dev)
+                                            DT, c["steps"], c["every"], device=dev, calib=calib)
     t_data = time.perf_counter() - t0
     s_out = float((nut * w).mean() / w.mean())
     model = CL.MLPModel.init(0, s_in=s_in, s_out=s_out, device=dev)
@@ -766,6 +767,8 @@ def closure_bench(S, torch, dev, args, world, rank, hbm, peak_src, clocks):
     samples = X.shape[0]
     del X, nut, w
     torch.cuda.empty_cache()
+    # output scale fitted a posteriori on the first training seed (not held out)
+    calib_errs = CL.calibrate(S, model, calib, NU, DT, c["steps"], c["kc"])
     res = CL.evaluate(S, model, c["nf"], c["nc"], c["kc"], c["eval_seeds"], NU, DT, c["steps"],
                       cs=c["cs"], device=dev)
     # device-timed steps/s of the coarse MLP run and of the plain coarse run
@@ -827,7 +830,9 @@ def closure_bench(S, torch, dev, args, world, rank, hbm, peak_src, clocks):
         "training": {"samples": samples, "steps": c["train_steps"], "batch": c["batch"],
                      "seconds": t_train, "dataset_seconds": t_data,
                      "loss_first": losses[0][1], "loss_last": losses[-1][1],
-                     "s_in": s_in, "s_out": s_out},
+                     "s_in": s_in, "s_out": s_out,
+                     "output_scale_calibration": {str(k): v for k, v in calib_errs.items()},
+                     "output_scale": model.s_out / s_out},
         "roofline": {"bound": "tensor", "kernel": "MLP inference (k_mlp_infer, 64^3 points)",
                      "achieved": achieved, "unit": "TFLOP/s", "peak": tpeak,
                      "frac": achieved / tpeak, "traffic": None,

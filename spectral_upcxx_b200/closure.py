@@ -173,6 +173,23 @@ def spectrum_error(E, Eref, kmax):
     return float(np.mean(np.abs(E[k] - Eref[k]) / Eref[k]))
 
 
+def calibrate(S, model, calib, nu, dt, steps, kc, scales=(0.5, 1.0, 1.5, 2.0, 3.0, 4.0),
+              dtype=torch.complex64):
+    """Scale the model's output by the factor of `scales` whose coarse run from
+    a training seed's filtered field (calib from dns_dataset) ends with the
+    smallest spectrum error against that seed's filtered DNS.  Returns
+    {scale: error} and leaves the best scale applied."""
+    s_out0 = model.s_out
+    errs = {}
+    for c in scales:
+        model.set_scales(model.s_in, s_out0 * c)
+        V = coarse_run(S, calib["Vc0"], nu, dt, steps, model=model, kc=kc, dtype=dtype)
+        errs[c] = spectrum_error(spectrum(V), calib["Eref"], int(kc))
+    best = min(errs, key=errs.get)
+    model.set_scales(model.s_in, s_out0 * best)
+    return errs
+
+
 def smagorinsky_cs_delta2(cs: float, kc: float) -> float:
     """(Cs Delta)^2 with Delta = pi / kc, the width of the sharp cutoff."""
     return (cs * math.pi / kc) ** 2
@@ -184,16 +201,20 @@ def _initial(n, seed, dtype, device):
 
 
 def dns_dataset(S, nf, nc, kc, seeds, nu, dt, steps, every, dtype=torch.complex64, device="cuda",
-                s_in=None, log=None):
+                s_in=None, log=None, calib=None):
     """Run fine DNS from each seed for `steps` steps and take a filtered
     training sample every `every` steps.  Returns X (M, 16) bf16, nu_t (M,)
     float32, the weights S:S / mean(S:S) (M,) float32, s_in (the feature
     scale: 1 / rms of the first snapshot's gradient when not given) and the
-    number of snapshots."""
+    number of snapshots.  With `calib` (a dict), the first seed's filtered
+    initial field ('Vc0') and filtered final spectrum ('Eref') are stored in
+    it for calibrate()."""
     Xs, ts, ws = [], [], []
     snaps = 0
     for seed in seeds:
         V0 = _initial(nf, seed, dtype, device)
+        if calib is not None and seed == seeds[0]:
+            calib["Vc0"] = truncate(V0, nc, kc)
         st = S.NSStepper((nf, nf, nf), nu, dt, dtype, device=device)
         st.bootstrap(V0, S.curl(V0))
         del V0
@@ -210,6 +231,8 @@ def dns_dataset(S, nf, nc, kc, seeds, nu, dt, steps, every, dtype=torch.complex6
             ts.append(t)
             ws.append(w)
             snaps += 1
+        if calib is not None and seed == seeds[0]:
+            calib["Eref"] = spectrum(truncate(st.velocity(), nc, kc))
         st.close()
         if log:
             log(f"seed {seed}: {snaps} snapshots so far")

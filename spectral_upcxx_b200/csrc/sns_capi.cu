@@ -551,7 +551,9 @@ int sns::ns_create_tuned(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, do
   }
   for (int i = 0; i < 6; i++) all[6 + i] = &h->U[i];
   for (int i = 0; i < 12 && rc == OK; i++) rc = pool_malloc(all[i], bytes);
-  if (rc == OK) rc = pool_malloc((void**)&h->stats_part, sizeof(double) * 4 * h->pl.update_blocks);
+  if (rc == OK)
+    rc = pool_malloc((void**)&h->stats_part,
+                     sizeof(double) * 4 * std::max(h->pl.update_blocks, h->pl.sgs_blocks));
   if (rc == OK) rc = pool_malloc((void**)&h->stats_out, sizeof(double) * 4);
   if (rc == OK) rc = pool_malloc((void**)&h->sync_words, sizeof(int) * xy_sync_words((int)nz));
   if (rc == OK)
@@ -749,7 +751,9 @@ int sns_ns_stats(sns_ns* h, double* div_avg, double* energy, double* enstrophy, 
   }
   int rc = sns_ns_check(h);
   if (rc) return rc;
-  rc = ns_stats_final(h->pl, h->stats_part, h->stats_out, h->s);
+  rc = ns_stats_final(h->stats_part,
+                      h->cl.model != CLOSURE_NONE ? h->pl.sgs_blocks : h->pl.update_blocks,
+                      h->stats_out, h->s);
   if (rc) return rc;
   double v[4];
   if ((rc = cuda_status(cudaMemcpyAsync(v, h->stats_out, sizeof(v), cudaMemcpyDeviceToHost, h->s),

@@ -7,13 +7,12 @@
 //
 //   z-inverse of V and grad V (i k_j V_i)   1 launch x 12 fields
 //   y-inverse                               1 x 12
-//   x-inverse                               1 x 12
-//   closure: nu_t (Smagorinsky or the MLP on the tensor cores), u x omega
-//            and tau_ij pointwise           1
-//   x-forward, y-forward of u x omega, tau  2 x 9
-//   z-forward of tau                        1 x 6
-//   z-forward of u x omega + i k_j tau_ij + the AB2 / projection / CN
-//   update                                  1
+//   x-inverse, closure (nu_t by Smagorinsky or the MLP on the tensor cores,
+//   u x omega and tau_ij per point), x-forward of the 9 results: one fused
+//   pass through shared memory             1
+//   y-forward of u x omega, tau             1 x 9
+//   z-forward of u x omega and tau, + i k_j tau_ij, then the AB2 /
+//   projection / CN update                  1 x 9 in, 6 out
 #include <cuda_bf16.h>
 #include <math.h>
 
@@ -30,109 +29,185 @@
 
 namespace sns {
 
-constexpr int kClWarps = 8;
-constexpr int kXsStride = 24;  // bf16 per feature row (bank-spread A loads)
+// Rows of x lines per CTA of the fused x pass: 12 fields x G rows x TPL
+// threads = 384 whatever the line length (TPL = L / 16).
+constexpr int kXlesThreads = 384;
 
-struct ClosureArgs {
-  void* U[kLESWork];  // in: u (3), A_ij = d_j u_i (9), unnormalised; out: u x omega, tau
-  int64_t n;
+struct XlesArgs {
+  FieldPtrs f;  // in: u (3), A_ij = d_j u_i (9) after the z and y inverses; out: u x omega, tau
   double invN;
   double csd2;
   const MlpPacked* mlp;
 };
 
-// Per point: nu_t, omega and u x omega from the velocity gradient, tau_ij =
-// 2 nu_t S_ij.  Warps take 32 points; with the MLP, a warp evaluates its
-// points as two 16-row tiles on the tensor cores.
-template <typename T, int MODEL>
-__global__ void __launch_bounds__(kClWarps * 32) k_les_closure(const ClosureArgs a) {
+// nu_t -> u x omega (from omega = (A_zy - A_yz, A_xz - A_zx, A_yx - A_xy)) and
+// tau = 2 nu_t S (xx, yy, zz, xy, xz, yz) of one point; A_ij at index 3 i + j.
+template <typename T>
+__device__ __forceinline__ void closure_point(const cx_t<T> (&u)[3], const cx_t<T> (&A)[9], T nu,
+                                              cx_t<T> (&o)[9]) {
+  const cx_t<T> w0 = csub(A[7], A[5]), w1 = csub(A[2], A[6]), w2 = csub(A[3], A[1]);
+  o[0] = csub(cmul(u[1], w2), cmul(u[2], w1));
+  o[1] = csub(cmul(u[2], w0), cmul(u[0], w2));
+  o[2] = csub(cmul(u[0], w1), cmul(u[1], w0));
+  o[3] = cscale((T)2 * nu, A[0]);
+  o[4] = cscale((T)2 * nu, A[4]);
+  o[5] = cscale((T)2 * nu, A[8]);
+  o[6] = cscale(nu, cadd(A[1], A[3]));
+  o[7] = cscale(nu, cadd(A[2], A[6]));
+  o[8] = cscale(nu, cadd(A[5], A[7]));
+}
+
+// The closure's x pass: x-inverse of the 12 fields of G rows into shared
+// memory, nu_t per point (the MLP as 16-point tiles on the tensor cores, or
+// Smagorinsky (Cs Delta)^2 sqrt(2 S:S) from the real gradient), u x omega and
+// tau written over the rows, x-forward of the 9 results.  Rows are
+// field-major (line = field * G + row), so the warps that hold only the
+// three discarded gradient fields skip the forward transform.
+template <typename T, int L, int MODEL>
+__global__ void __launch_bounds__(kXlesThreads)
+    k_xles(const XlesArgs a, const cx_t<T>* __restrict__ tw) {
   using C = cx_t<T>;
+  using P = LinePlan<L>;
+  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(L);
+  constexpr int G = 32 / TPL;
+  constexpr int PTS = G * L;
+  static_assert(TPL <= 32 && 12 * G * TPL == kXlesThreads, "tile shape");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sm = reinterpret_cast<C*>(smem_raw);
   __shared__ MlpSmem S;
-  __shared__ __align__(16) __nv_bfloat16 xs[kClWarps][32 * kXsStride];
-  __shared__ float nus[kClWarps][32];
+  __shared__ float nus[PTS];
+  const int64_t row0 = (int64_t)blockIdx.x * G;
+  const int j = threadIdx.x % TPL, line = threadIdx.x / TPL;
+  const int fld = line / G, gl = line - fld * G;
+  C* row = sm + line * RS;
+  if constexpr (MODEL == CLOSURE_MLP) mlp_load_smem(a.mlp, S, threadIdx.x, blockDim.x);
+  C v[E];
+  {
+    const C* __restrict__ src = reinterpret_cast<const C*>(select_ptr(a.f.in, fld));
+    const int64_t i0 = (row0 + gl) * L + j;
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = src[i0 + TPL * e];
+  }
+  line_fft<L>(v, row, j, tw, (T)1);
+#pragma unroll
+  for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
+  __syncthreads();
+
+  const T invN = (T)a.invN;
+  auto at = [&](int field, int p) -> C& {
+    return sm[(field * G + p / L) * RS + pad_pos(p % L)];
+  };
   if constexpr (MODEL == CLOSURE_MLP) {
-    mlp_load_smem(a.mlp, S, threadIdx.x, blockDim.x);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const float s_in = S.s_in;
+    auto feat = [&](int p, int q) -> float {
+      return (float)(at(3 + q, p).x * invN) * s_in;
+    };
+    for (int mt = warp; mt < PTS / 16; mt += kXlesThreads / 32) {
+      const int pa = 16 * mt + g, pb = pa + 8;
+      // A operand: rows = points, columns = the 9 features (zero padded to 16)
+      uint32_t xa[4];
+      xa[0] = pack_bf16(feat(pa, 2 * t), feat(pa, 2 * t + 1));
+      xa[1] = pack_bf16(feat(pb, 2 * t), feat(pb, 2 * t + 1));
+      xa[2] = t == 0 ? pack_bf16(feat(pa, 8), 0.f) : 0u;
+      xa[3] = t == 0 ? pack_bf16(feat(pb, 8), 0.f) : 0u;
+      MlpTile tile;
+      mlp_tile_forward<false>(S, xa, tile);
+      if (t == 0) {
+        nus[pa] = S.s_out * softplus_f(tile.z[0]);
+        nus[pb] = S.s_out * softplus_f(tile.z[1]);
+      }
+    }
     __syncthreads();
   }
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const T invN = (T)a.invN;
-  const C* __restrict__ in[kLESWork];
+  for (int p = threadIdx.x; p < PTS; p += kXlesThreads) {
+    C u[3], A[9], o[9];
 #pragma unroll
-  for (int q = 0; q < kLESWork; q++) in[q] = reinterpret_cast<const C*>(a.U[q]);
-  for (int64_t p0 = ((int64_t)blockIdx.x * kClWarps + warp) * 32; p0 < a.n;
-       p0 += (int64_t)gridDim.x * kClWarps * 32) {
-    const int64_t p = p0 + lane;
-    T nu = 0;
+    for (int d = 0; d < 3; d++) u[d] = cscale(invN, at(d, p));
+#pragma unroll
+    for (int q = 0; q < 9; q++) A[q] = cscale(invN, at(3 + q, p));
+    T nu;
     if constexpr (MODEL == CLOSURE_MLP) {
-      __nv_bfloat16* row = &xs[warp][lane * kXsStride];
-#pragma unroll
-      for (int q = 0; q < kMlpIn; q++)
-        row[q] = __float2bfloat16_rn((float)(in[3 + q][p].x * invN) * S.s_in);
-#pragma unroll
-      for (int q = kMlpIn; q < kMlpK1; q++) row[q] = __float2bfloat16_rn(0.f);
-      __syncwarp();
-#pragma unroll
-      for (int m = 0; m < 2; m++) {
-        uint32_t xa[4];
-        load_a_tile(&xs[warp][16 * m * kXsStride], kXsStride, xa);
-        MlpTile tile;
-        mlp_tile_forward<false>(S, xa, tile);
-        if ((lane & 3) == 0) {
-          const int g = lane >> 2;
-          nus[warp][16 * m + g] = S.s_out * softplus_f(tile.z[0]);
-          nus[warp][16 * m + g + 8] = S.s_out * softplus_f(tile.z[1]);
-        }
-      }
-      __syncwarp();
-      nu = (T)nus[warp][lane];
-    }
-    C A[9], u[3];
-#pragma unroll
-    for (int q = 0; q < 9; q++) A[q] = cscale(invN, in[3 + q][p]);
-#pragma unroll
-    for (int d = 0; d < 3; d++) u[d] = cscale(invN, in[d][p]);
-    if constexpr (MODEL == CLOSURE_SMAGORINSKY) {
-      // (Cs Delta)^2 sqrt(2 S:S), S from the real gradient
+      nu = (T)nus[p];
+    } else {
       T s2 = 0;
 #pragma unroll
       for (int i = 0; i < 3; i++)
 #pragma unroll
-        for (int j = 0; j < 3; j++) {
-          const T sij = (T)0.5 * (A[3 * i + j].x + A[3 * j + i].x);
+        for (int jj = 0; jj < 3; jj++) {
+          const T sij = (T)0.5 * (A[3 * i + jj].x + A[3 * jj + i].x);
           s2 += sij * sij;
         }
       nu = (T)a.csd2 * sqrt((T)2 * s2);
     }
-    // omega = (A_zy - A_yz, A_xz - A_zx, A_yx - A_xy), A_ij at 3 i + j
-    const C w0 = csub(A[7], A[5]), w1 = csub(A[2], A[6]), w2 = csub(A[3], A[1]);
-    C* __restrict__ out[9];
+    closure_point<T>(u, A, nu, o);
 #pragma unroll
-    for (int q = 0; q < 9; q++) out[q] = reinterpret_cast<C*>(a.U[q]);
-    out[0][p] = csub(cmul(u[1], w2), cmul(u[2], w1));
-    out[1][p] = csub(cmul(u[2], w0), cmul(u[0], w2));
-    out[2][p] = csub(cmul(u[0], w1), cmul(u[1], w0));
-    // tau = 2 nu S: xx, yy, zz, xy, xz, yz
-    out[3][p] = cscale((T)2 * nu, A[0]);
-    out[4][p] = cscale((T)2 * nu, A[4]);
-    out[5][p] = cscale((T)2 * nu, A[8]);
-    out[6][p] = cscale(nu, cadd(A[1], A[3]));
-    out[7][p] = cscale(nu, cadd(A[2], A[6]));
-    out[8][p] = cscale(nu, cadd(A[5], A[7]));
+    for (int q = 0; q < 9; q++) at(q, p) = o[q];
+  }
+  __syncthreads();
+
+  constexpr int kLinesPerWarp = 32 / TPL;
+  const bool skip = ((9 * G) % kLinesPerWarp == 0) && fld >= 9;
+  if (!skip) {
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
+    line_sync<TPL>();
+    line_fft<L>(v, row, j, tw, (T)-1);
+  }
+  if (fld < 9) {
+    C* __restrict__ dst = reinterpret_cast<C*>(select_ptr(a.f.out, fld));
+    const int64_t i0 = (row0 + gl) * L + j;
+#pragma unroll
+    for (int e = 0; e < E; e++) dst[i0 + TPL * e] = v[e];
+  }
+}
+
+template <typename T, int L, int MODEL>
+int launch_xles_l(const XlesArgs& a, int64_t rows, cudaStream_t s) {
+  using C = cx_t<T>;
+  constexpr int TPL = LinePlan<L>::TPL;
+  constexpr int G = 32 / TPL;
+  if (rows % G) {
+    set_error("closure step: ny * nz must be a multiple of the x-pass rows per CTA");
+    return ERR_UNSUPPORTED;
+  }
+  const size_t smem = (size_t)12 * G * row_stride(L) * sizeof(C);
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr[dev & 63]) {
+    cudaError_t e = allow_max_dynamic_smem(k_xles<T, L, MODEL>);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_xles)");
+    attr[dev & 63] = true;
+  }
+  const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
+  if (!tw) {
+    set_error("twiddle table allocation failed");
+    return ERR_ALLOC;
+  }
+  k_xles<T, L, MODEL><<<(unsigned)(rows / G), kXlesThreads, smem, s>>>(a, tw);
+  SNS_CHECK_LAUNCH("k_xles");
+  return OK;
+}
+
+template <typename T, int MODEL>
+int launch_xles_m(const XlesArgs& a, int nx, int64_t rows, cudaStream_t s) {
+  switch (nx) {
+    case 16: return launch_xles_l<T, 16, MODEL>(a, rows, s);
+    case 32: return launch_xles_l<T, 32, MODEL>(a, rows, s);
+    case 64: return launch_xles_l<T, 64, MODEL>(a, rows, s);
+    case 128: return launch_xles_l<T, 128, MODEL>(a, rows, s);
+    case 256: return launch_xles_l<T, 256, MODEL>(a, rows, s);
+    default:
+      set_error("closure step: nx must be a power of two in [16, 256]");
+      return ERR_UNSUPPORTED;
   }
 }
 
 template <typename T>
-int launch_closure(const ClosureArgs& a, int model, cudaStream_t s) {
-  // MLP: a resident grid (two CTAs per SM), so each CTA loads the weights once
-  const int64_t groups = a.n / 32;
-  const int cap = model == CLOSURE_MLP ? 2 * sm_count() : 8 * sm_count();
-  const int blocks = (int)std::min<int64_t>((groups + kClWarps - 1) / kClWarps, cap);
-  if (model == CLOSURE_MLP)
-    k_les_closure<T, CLOSURE_MLP><<<blocks, kClWarps * 32, 0, s>>>(a);
-  else
-    k_les_closure<T, CLOSURE_SMAGORINSKY><<<blocks, kClWarps * 32, 0, s>>>(a);
-  SNS_CHECK_LAUNCH("k_les_closure");
-  return OK;
+int launch_xles(const XlesArgs& a, int model, int nx, int64_t rows, cudaStream_t s) {
+  return model == CLOSURE_MLP ? launch_xles_m<T, CLOSURE_MLP>(a, nx, rows, s)
+                              : launch_xles_m<T, CLOSURE_SMAGORINSKY>(a, nx, rows, s);
 }
 
 int les_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* const U[kLESWork],
@@ -159,26 +234,27 @@ int les_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* c
     LineGeo g = axis_geo(axis, nx, ny, nz, prec, pl.lineW);
     return run_line_pass(g, f, sign, 0, 1.0, prec, s, pro);
   };
-  // inverse of V (3) and grad V (9): z with the gradient prologue, then y, x
+  // inverse of V (3) and grad V (9): z with the gradient prologue, then y
   if ((rc = pass(2, 0, kLESWork, +1, PRO_GRAD12, true))) return rc;
-  for (int axis : {1, 0})
-    if ((rc = pass(axis, 0, kLESWork, +1, PRO_LOAD, false))) return rc;
-  // pointwise closure
+  if ((rc = pass(1, 0, kLESWork, +1, PRO_LOAD, false))) return rc;
+  // x-inverse, closure, x-forward of u x omega (U[0..2]) and tau (U[3..8])
   {
-    ClosureArgs a{};
-    for (int q = 0; q < kLESWork; q++) a.U[q] = U[q];
-    a.n = n;
+    XlesArgs a{};
+    a.f.n = kLESWork;
+    for (int q = 0; q < kLESWork; q++) {
+      a.f.in[q] = U[q];
+      a.f.out[q] = U[q];
+    }
     a.invN = 1.0 / (double)n;
     a.csd2 = cl.csd2;
     a.mlp = reinterpret_cast<const MlpPacked*>(cl.mlp);
-    rc = prec == PREC_C128 ? launch_closure<double>(a, cl.model, s)
-                           : launch_closure<float>(a, cl.model, s);
+    const int64_t rows = (int64_t)ny * nz;
+    rc = prec == PREC_C128 ? launch_xles<double>(a, cl.model, nx, rows, s)
+                           : launch_xles<float>(a, cl.model, nx, rows, s);
     if (rc) return rc;
   }
-  // forward x, y of u x omega (U[0..2]) and tau (U[3..8]); z of tau
-  for (int axis : {0, 1})
-    if ((rc = pass(axis, 0, 9, -1, PRO_LOAD, false))) return rc;
-  if ((rc = pass(2, 3, 6, -1, PRO_LOAD, false))) return rc;
+  // y-forward of the 9 results
+  if ((rc = pass(1, 0, 9, -1, PRO_LOAD, false))) return rc;
   // z-forward of u x omega + div tau + update
   UpdateArgs a{};
   for (int d = 0; d < 3; d++) {
@@ -192,7 +268,7 @@ int les_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* c
   a.nz = nz;
   a.lx = 0;
   while ((1 << a.lx) < nx) a.lx++;
-  a.W = pl.zW;
+  a.W = pl.sgs_W;
   a.hK = dt / 2;
   a.nuhK = nu * dt / 2;
   a.stats = stats;

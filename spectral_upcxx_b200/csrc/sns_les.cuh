@@ -16,7 +16,7 @@ struct Closure {
 };
 
 constexpr int kLESWork = 12;  // work fields of the closure step
-constexpr int kLESLaunches = 8;
+constexpr int kLESLaunches = 5;
 
 // One step with the eddy-viscosity term of `cl` (the plain step when
 // cl.model == CLOSURE_NONE is ns_step_once): V, C0 as in ns_step_once, U

@@ -32,7 +32,6 @@ constexpr int kPart = kMlpParams + 1;         // gradients + loss sum
 
 struct TrainSmem {
   MlpSmem m;
-  __nv_bfloat16 W2T[kMlpHidden * kW2Stride];  // W2 transposed: W2T[n1][n2]
   __nv_bfloat16 XT[kMlpK1 * kTS];             // inputs, [feature][sample]
   __nv_bfloat16 H1T[kMlpHidden * kTS];        // layer-1 activations, [unit][sample]
   __nv_bfloat16 P2T[kMlpHidden * kTS];        // dPre2, [unit][sample]
@@ -50,11 +49,8 @@ __global__ void __launch_bounds__(kTrainRows)
   TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
   mlp_load_smem(P, S.m, tid, blockDim.x);
-  for (int i = tid; i < kMlpHidden * kMlpHidden; i += blockDim.x) {
-    const int n2 = i / kMlpHidden, n1 = i % kMlpHidden;
-    S.W2T[n1 * kW2Stride + n2] = P->W2[i];
-  }
   __syncthreads();
+  const int lm = lane >> 3, lr = lane & 7;
 
   float db1[8][2], db2[8][2], dw3[8][2];
 #pragma unroll
@@ -142,10 +138,14 @@ __global__ void __launch_bounds__(kTrainRows)
     for (int nt = 0; nt < 8; nt++) {
       float c[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-      for (int kt = 0; kt < 4; kt++) {
-        const __nv_bfloat16* w = &S.W2T[(nt * 8 + g) * kW2Stride + kt * 16 + 2 * t];
-        mma_bf16_16816(c, p2a[kt], *reinterpret_cast<const uint32_t*>(w),
-                       *reinterpret_cast<const uint32_t*>(w + 8));
+      for (int kp = 0; kp < 2; kp++) {
+        // B[k = n2][n = n1] = W2[n2][n1]: transposed 8x8 matrices of W2's rows
+        // 16 kt + 0..15, columns 8 nt..8 nt+7, for k-tiles 2kp and 2kp+1
+        uint32_t b[4];
+        ldsm_x4_trans(b, &S.m.W2[((2 * kp + (lm >> 1)) * 16 + (lm & 1) * 8 + lr) * kW2Stride +
+                                 nt * 8]);
+        mma_bf16_16816(c, p2a[2 * kp], b[0], b[1]);
+        mma_bf16_16816(c, p2a[2 * kp + 1], b[2], b[3]);
       }
       const int col = nt * 8 + 2 * t;
       float dp[4];
@@ -207,10 +207,11 @@ __global__ void __launch_bounds__(kTrainRows)
       uint32_t a[4];
       load_a_tile(&S.P2T[(16 * warp) * kTS + 16 * ks], kTS, a);
 #pragma unroll
-      for (int nt = 0; nt < 8; nt++) {
-        const __nv_bfloat16* b = &S.H1T[(nt * 8 + g) * kTS + 16 * ks + 2 * t];
-        mma_bf16_16816(acc[nt], a, *reinterpret_cast<const uint32_t*>(b),
-                       *reinterpret_cast<const uint32_t*>(b + 8));
+      for (int nt = 0; nt < 8; nt += 2) {
+        uint32_t b[4];
+        load_b_pair(&S.H1T[(nt * 8) * kTS + 16 * ks], kTS, b);
+        mma_bf16_16816(acc[nt], a, b[0], b[1]);
+        mma_bf16_16816(acc[nt + 1], a, b[2], b[3]);
       }
     }
 #pragma unroll
@@ -233,11 +234,11 @@ __global__ void __launch_bounds__(kTrainRows)
     for (int ks = 0; ks < kTrainRows / 16; ks++) {
       uint32_t a[4];
       load_a_tile(&S.P1T[(16 * warp) * kTS + 16 * ks], kTS, a);
-#pragma unroll
-      for (int nt = 0; nt < 2; nt++) {
-        const __nv_bfloat16* b = &S.XT[(nt * 8 + g) * kTS + 16 * ks + 2 * t];
-        mma_bf16_16816(acc[nt], a, *reinterpret_cast<const uint32_t*>(b),
-                       *reinterpret_cast<const uint32_t*>(b + 8));
+      {
+        uint32_t b[4];
+        load_b_pair(&S.XT[16 * ks], kTS, b);
+        mma_bf16_16816(acc[0], a, b[0], b[1]);
+        mma_bf16_16816(acc[1], a, b[2], b[3]);
       }
     }
 #pragma unroll

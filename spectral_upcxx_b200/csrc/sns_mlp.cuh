@@ -43,9 +43,10 @@ static_assert(sizeof(MlpPacked) % 16 == 0, "packed model is copied in 16-byte wo
 
 // Shared-memory copy of the model with padded rows: a row stride of 12 / 36
 // 32-bit words puts the eight g-rows of a B fragment on distinct banks.
-constexpr int kW1Stride = kMlpK1 + 8;      // bf16 per W1 row
-constexpr int kW2Stride = kMlpHidden + 8;  // bf16 per W2 row
-struct MlpSmem {
+constexpr int kW1Stride = kMlpK1 + 8;      // bf16 per W1 row (48 bytes)
+constexpr int kW2Stride = kMlpHidden + 8;  // bf16 per W2 row (144 bytes)
+// 16-byte aligned: ldmatrix reads its rows
+struct __align__(16) MlpSmem {
   __nv_bfloat16 W1[kMlpHidden * kW1Stride];
   __nv_bfloat16 W2[kMlpHidden * kW2Stride];
   float w3[kMlpHidden];
@@ -89,6 +90,22 @@ __device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+// ldmatrix: lanes 8m..8m+7 give the row addresses of 8x8 bf16 matrix m; lane
+// l receives row l/4, columns 2(l%4), 2(l%4)+1 of each matrix (transposed
+// matrices with .trans).  Rows must start on 16-byte boundaries.
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const void* p) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a));
+}
+__device__ __forceinline__ void ldsm_x4_trans(uint32_t (&r)[4], const void* p) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a));
+}
+
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);  // .x = lo (low half), .y = hi
   return *reinterpret_cast<uint32_t*>(&v);
@@ -111,14 +128,16 @@ struct MlpTile {
 template <bool KEEP>
 __device__ __forceinline__ void mlp_tile_forward(const MlpSmem& s, const uint32_t (&xa)[4],
                                                  MlpTile& T) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  // layer 1: [16 x 16] x [16 x 64]
+  const int lane = threadIdx.x & 31, t = lane & 3;
+  const int lm = lane >> 3, lr = lane & 7;  // ldmatrix: matrix and row of this lane's address
+  // layer 1: [16 x 16] x [16 x 64]; B[k][n] = W1[n][k], two n-tiles per ldmatrix
+  uint32_t b1f[4];
 #pragma unroll
   for (int nt = 0; nt < 8; nt++) {
     float c[4] = {0.f, 0.f, 0.f, 0.f};
-    const __nv_bfloat16* w = &s.W1[(nt * 8 + g) * kW1Stride + 2 * t];
-    mma_bf16_16816(c, xa, *reinterpret_cast<const uint32_t*>(w),
-                   *reinterpret_cast<const uint32_t*>(w + 8));
+    if ((nt & 1) == 0)
+      ldsm_x4(b1f, &s.W1[((nt + (lm >> 1)) * 8 + lr) * kW1Stride + (lm & 1) * 8]);
+    mma_bf16_16816(c, xa, b1f[(nt & 1) * 2], b1f[(nt & 1) * 2 + 1]);
     const float bl = s.b1[nt * 8 + 2 * t], bh = s.b1[nt * 8 + 2 * t + 1];
     c[0] += bl;
     c[1] += bh;
@@ -140,10 +159,12 @@ __device__ __forceinline__ void mlp_tile_forward(const MlpSmem& s, const uint32_
   for (int nt = 0; nt < 8; nt++) {
     float c[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-    for (int kt = 0; kt < 4; kt++) {
-      const __nv_bfloat16* w = &s.W2[(nt * 8 + g) * kW2Stride + kt * 16 + 2 * t];
-      mma_bf16_16816(c, T.h1[kt], *reinterpret_cast<const uint32_t*>(w),
-                     *reinterpret_cast<const uint32_t*>(w + 8));
+    for (int kp = 0; kp < 2; kp++) {
+      // B[k][n] = W2[n][k]: k-tiles 2kp and 2kp+1 of n-tile nt in one ldmatrix
+      uint32_t b[4];
+      ldsm_x4(b, &s.W2[(nt * 8 + lr) * kW2Stride + (2 * kp + (lm >> 1)) * 16 + (lm & 1) * 8]);
+      mma_bf16_16816(c, T.h1[2 * kp], b[0], b[1]);
+      mma_bf16_16816(c, T.h1[2 * kp + 1], b[2], b[3]);
     }
     const int col = nt * 8 + 2 * t;
     const float bl = s.b2[col], bh = s.b2[col + 1];
@@ -166,14 +187,20 @@ __device__ __forceinline__ void mlp_tile_forward(const MlpSmem& s, const uint32_
   T.z[1] = zh + s.b3;
 }
 
-// A operand of a 16x16 bf16 tile stored row-major with `stride` bf16 per row.
+// A operand of a 16x16 bf16 tile stored row-major with `stride` bf16 per row
+// (rows 16-byte aligned): matrices (rows 0-7 | 8-15) x (columns 0-7 | 8-15).
 __device__ __forceinline__ void load_a_tile(const __nv_bfloat16* base, int stride,
                                             uint32_t (&a)[4]) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  a[0] = *reinterpret_cast<const uint32_t*>(base + g * stride + 2 * t);
-  a[1] = *reinterpret_cast<const uint32_t*>(base + (g + 8) * stride + 2 * t);
-  a[2] = *reinterpret_cast<const uint32_t*>(base + g * stride + 2 * t + 8);
-  a[3] = *reinterpret_cast<const uint32_t*>(base + (g + 8) * stride + 2 * t + 8);
+  const int lane = threadIdx.x & 31, lm = lane >> 3, lr = lane & 7;
+  ldsm_x4(a, base + ((lm & 1) * 8 + lr) * stride + (lm >> 1) * 8);
+}
+
+// B operands of n-tiles nt, nt+1 (k-tile of 16) from a [n][k] row-major bf16
+// tile: b[0], b[1] for nt and b[2], b[3] for nt + 1.
+__device__ __forceinline__ void load_b_pair(const __nv_bfloat16* base, int stride,
+                                            uint32_t (&b)[4]) {
+  const int lane = threadIdx.x & 31, lm = lane >> 3, lr = lane & 7;
+  ldsm_x4(b, base + ((lm >> 1) * 8 + lr) * stride + (lm & 1) * 8);
 }
 
 }  // namespace sns

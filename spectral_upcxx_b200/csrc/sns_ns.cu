@@ -19,6 +19,7 @@
 #include <math.h>
 #include <stdlib.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "sns_fft.cuh"
@@ -110,8 +111,10 @@ template <typename T, int L, bool SGS>
 int launch_update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
   using C = cx_t<T>;
   constexpr int TPL = LinePlan<L>::TPL;
-  const int threads = 3 * a.W * TPL;
-  const size_t smem = (size_t)3 * a.W * row_stride(L) * sizeof(C);
+  constexpr int NF = SGS ? 9 : 3;
+  const int threads = NF * a.W * TPL;
+  const size_t smem = (size_t)NF * a.W * row_stride(L) * sizeof(C);
+  const int blocks = (int)(((int64_t)pl.nx * pl.ny) / a.W);
   static bool attr[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -121,7 +124,7 @@ int launch_update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
     attr[dev & 63] = true;
   }
   const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
-  k_zfwd_update<T, L, SGS><<<pl.update_blocks, threads, smem, s>>>(a, tw);
+  k_zfwd_update<T, L, SGS><<<blocks, threads, smem, s>>>(a, tw);
   SNS_CHECK_LAUNCH("k_zfwd_update");
   return OK;
 }
@@ -203,6 +206,14 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW) {
       W *= 2;
     pl.zW = W;
     pl.update_blocks = (nx / W) * ny;
+    // closure update: nine fields in the tile
+    const int cap = std::min(576, max_threads(prec));
+    int Ws = 1;
+    while (Ws * 2 <= Wmax && ((int64_t)nx * ny) % (Ws * 2) == 0 && 9 * (Ws * 2) * TPL <= cap &&
+           (size_t)9 * Ws * 2 * row_stride(nz) * esz <= 110 * 1024)
+      Ws *= 2;
+    pl.sgs_W = Ws;
+    pl.sgs_blocks = (int)(((int64_t)nx * ny) / Ws);
   }
   // xy phase: three separate full-domain passes by default.  SNS_XY_PASSES=1
   // selects the persistent dataflow launch (sns_xy.cu), which moves a third of
@@ -322,8 +333,8 @@ int ns_update(const NSPlan& pl, const UpdateArgs& a, bool sgs, cudaStream_t s) {
   return sgs ? update<float, true>(pl, a, s) : update<float, false>(pl, a, s);
 }
 
-int ns_stats_final(const NSPlan& pl, const double* partials, double* out4, cudaStream_t s) {
-  k_stats_final<<<1, 256, 0, s>>>(partials, pl.update_blocks, out4);
+int ns_stats_final(const double* partials, int blocks, double* out4, cudaStream_t s) {
+  k_stats_final<<<1, 256, 0, s>>>(partials, blocks, out4);
   SNS_CHECK_LAUNCH("k_stats_final");
   return OK;
 }

@@ -12,6 +12,8 @@ struct NSPlan {
   int xG;             // rows per CTA of the x cross pass
   int zW;             // adjacent z lines per CTA of the update pass
   int update_blocks;  // CTAs of the update pass (= diagnostics partials)
+  int sgs_W;          // adjacent z lines per CTA of the closure update (9 fields)
+  int sgs_blocks;     // its CTAs (= diagnostics partials of a closure step)
   bool use_xy;        // xy phase as one persistent dataflow launch
   XYPlan xy;
   int xy_chunk;       // planes per slab of the separate xy passes (0 = all)
@@ -37,6 +39,6 @@ struct UpdateArgs;
 int ns_update(const NSPlan& pl, const UpdateArgs& a, bool sgs, cudaStream_t s);
 // Reduce the per-block diagnostics into out4 (device): sum|div|, sum|V|^2,
 // sum|i k x V|^2, max|div|.
-int ns_stats_final(const NSPlan& pl, const double* partials, double* out4, cudaStream_t s);
+int ns_stats_final(const double* partials, int blocks, double* out4, cudaStream_t s);
 
 }  // namespace sns

@@ -217,13 +217,28 @@ struct UpdateArgs {
   double hK;      // K/2
   double nuhK;    // nu*K/2
   double* stats;  // per tile: sum|div|, sum|V|^2, sum|k x V|^2, max|div|
-  // SGS: Fourier eddy stress tau_xx, tau_yy, tau_zz, tau_xy, tau_xz, tau_yz
-  // whose divergence i k_j tau_ij joins cross1 before the Nyquist zeroing
+  // SGS: eddy stress tau_xx, tau_yy, tau_zz, tau_xy, tau_xz, tau_yz after the
+  // x and y forward passes; z-transformed in the tile, its divergence
+  // i k_j tau_ij joins cross1 before the Nyquist zeroing
   const void* tau[6];
   double kc2;  // spectral cutoff |k|^2 <= kc2 of an LES run (1e300: none)
 };
 
+// Field f of the update's z-forward: the cross product (f < 3) or, with the
+// eddy stress, tau_{f-3}; selected with constant indices.
+__device__ __forceinline__ const void* update_field(const UpdateArgs& a, int f) {
+  const void* r = a.U[0];
+  if (f == 1) r = a.U[1];
+  if (f == 2) r = a.U[2];
+#pragma unroll
+  for (int q = 0; q < 6; q++)
+    if (f == 3 + q) r = a.tau[q];
+  return r;
+}
+
 // Tile `blk` holds the W z lines whose xy-plane offsets are blk*W .. blk*W+W-1.
+// With SGS the six stress fields are z-transformed in the same tile (9 fields
+// in shared memory, 9 W TPL threads).
 template <typename T, int L, bool SGS = false>
 __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
                                                  const cx_t<T>* __restrict__ tw, int64_t blk,
@@ -244,7 +259,8 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
     const int w = threadIdx.x % W, s = threadIdx.x / W;
     const int j = s % TPL, fld = s / TPL;
     C* row = sm + (fld * W + w) * RS;
-    const C* __restrict__ src = reinterpret_cast<const C*>(a.U[fld]);
+    const C* __restrict__ src = reinterpret_cast<const C*>(
+        SGS ? update_field(a, fld) : (fld == 0 ? a.U[0] : fld == 1 ? a.U[1] : a.U[2]));
     const int64_t i0 = base + w + nxy * j;
     C v[E];
 #pragma unroll
@@ -278,7 +294,7 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
       if (!nyq) {
         C t6[6];
 #pragma unroll
-        for (int q = 0; q < 6; q++) t6[q] = reinterpret_cast<const C*>(a.tau[q])[idx];
+        for (int q = 0; q < 6; q++) t6[q] = sm[((3 + q) * W + w) * RS + pad_pos(z)];
         // (div tau)_i = i (kx tau_ix + ky tau_iy + kz tau_iz)
         c1[0] = cadd(c1[0], cadd(cadd(ikmul(kx, t6[0]), ikmul(ky, t6[3])), ikmul(kz, t6[4])));
         c1[1] = cadd(c1[1], cadd(cadd(ikmul(kx, t6[3]), ikmul(ky, t6[1])), ikmul(kz, t6[5])));

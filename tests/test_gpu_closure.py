@@ -168,7 +168,7 @@ def test_smagorinsky_step_matches_oracle(CO, CL, sns, cuda, kc):
     csd2 = CL.smagorinsky_cs_delta2(0.17, 10.0)
     st, V1, c0 = _les_pair(CO, sns, cuda, n, nu, dt, 10)
     st.set_closure(sns._native.SNS_CLOSURE_SMAGORINSKY, cs_delta2=csd2, kc=kc)
-    assert st.launches_per_step() == 8
+    assert st.launches_per_step() == 5
     les = CO.LES(nu, dt, "smagorinsky", {"cs": 0.17, "delta": np.pi / 10.0},
                  kc=kc if kc > 0 else None)
     les.set_state(V1, c0)
