@@ -41,6 +41,16 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
 }
 
 // ---------------------------------------------------------------------------
+// K1: z lines -- inverse of V and of omega = i k x V from one load of V.
+template <typename T, int L>
+__global__ void __launch_bounds__(MaxThreads<T>::value)
+    k_zcurl(const LineGeo geo, const FieldPtrs f, const cx_t<T>* __restrict__ tw, int wshift) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  curl_zpass_tile<T, L>(geo, ParamFields{f}, tw, wshift, (int64_t)blockIdx.x,
+                        reinterpret_cast<cx_t<T>*>(smem_raw));
+}
+
+// ---------------------------------------------------------------------------
 // K5: z lines -- forward 3 fields + Nyquist zeroing, then the AB2 /
 // projection / CN update per mode.
 template <typename T, int L, bool SGS>
@@ -105,6 +115,62 @@ int launch_xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream
   k_xcross<T, L><<<blocks, threads, smem, s>>>(f, tw, G, (T)(1.0 / (N * N)));
   SNS_CHECK_LAUNCH("k_xcross");
   return OK;
+}
+
+template <typename T, int L>
+int launch_zcurl(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
+  using C = cx_t<T>;
+  constexpr int TPL = LinePlan<L>::TPL;
+  LineGeo g{};
+  g.L = L;
+  g.W = pl.k1W;
+  g.G = pl.k1G;
+  g.axis = 2;
+  g.nx = pl.nx;
+  g.ny = pl.ny;
+  g.nz = pl.nz;
+  g.ps = (int64_t)pl.nx * pl.ny;
+  g.gs = pl.nx;
+  g.TA = pl.nx / g.W;
+  g.TB = pl.ny / g.G;
+  g.sa = g.W;
+  g.sb = (int64_t)g.G * pl.nx;
+  const int threads = 3 * g.W * g.G * TPL;
+  const size_t smem = (size_t)6 * g.W * g.G * row_stride(L) * sizeof(C);
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr[dev & 63]) {
+    cudaError_t e = allow_max_dynamic_smem(k_zcurl<T, L>);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_zcurl)");
+    attr[dev & 63] = true;
+  }
+  const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
+  if (!tw) {
+    set_error("twiddle table allocation failed");
+    return ERR_ALLOC;
+  }
+  int wshift = 0;
+  while ((1 << wshift) < g.W) wshift++;
+  k_zcurl<T, L><<<(unsigned)(g.TA * g.TB), threads, smem, s>>>(g, f, tw, wshift);
+  SNS_CHECK_LAUNCH("k_zcurl");
+  return OK;
+}
+
+template <typename T>
+int zcurl(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
+  switch (pl.nz) {
+    case 4: return launch_zcurl<T, 4>(pl, f, s);
+    case 8: return launch_zcurl<T, 8>(pl, f, s);
+    case 16: return launch_zcurl<T, 16>(pl, f, s);
+    case 32: return launch_zcurl<T, 32>(pl, f, s);
+    case 64: return launch_zcurl<T, 64>(pl, f, s);
+    case 128: return launch_zcurl<T, 128>(pl, f, s);
+    case 256: return launch_zcurl<T, 256>(pl, f, s);
+    case 512: return launch_zcurl<T, 512>(pl, f, s);
+    case 1024: return launch_zcurl<T, 1024>(pl, f, s);
+    default: set_error("fused NS step: nz must be a power of two in [4, 1024]"); return ERR_UNSUPPORTED;
+  }
 }
 
 template <typename T, int L, bool SGS>
@@ -190,6 +256,29 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW) {
     }
     pl.xG = G;
   }
+  // K1 tile: W adjacent z lines x G groups of the three components, one
+  // CTA for all six outputs (SNS_K1_SPLIT=1: one output field per CTA)
+  {
+    // 16 adjacent lines keep the half-warps of the exchanges on distinct banks;
+    // the two row sets of a 16-line tile take 210 KB at 256 (opt-in limit 227 KB)
+    const int TPL = nz / elems(nz);
+    const int cap = max_threads(prec);
+    const size_t smem_cap = 220 * 1024;
+    int W = 1;
+    const int Wmax = prec == PREC_C128 ? 8 : 16;
+    while (W * 2 <= Wmax && nx % (W * 2) == 0 && 3 * (W * 2) * TPL <= cap &&
+           (size_t)6 * (W * 2) * row_stride(nz) * esz <= smem_cap)
+      W *= 2;
+    int G = 1;
+    while (ny % (G * 2) == 0 && 3 * W * (G * 2) * TPL <= 384 &&
+           (size_t)6 * W * (G * 2) * row_stride(nz) * esz <= smem_cap)
+      G *= 2;
+    pl.k1W = W;
+    pl.k1G = G;
+    const char* e = getenv("SNS_K1_SPLIT");
+    pl.k1_fused = !(e && e[0] == '1') && 3 * W * G * TPL <= cap &&
+                  (size_t)6 * W * G * row_stride(nz) * esz <= smem_cap;
+  }
   // K5 tile: W adjacent z lines of three fields
   {
     const int TPL = nz / elems(nz);
@@ -248,8 +337,13 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     f.n = 6;
     for (int d = 0; d < 3; d++) f.in[d] = V[d];
     for (int i = 0; i < 6; i++) f.out[i] = U[i];
-    LineGeo g = axis_geo(2, nx, ny, nz, prec, pl.lineW);
-    if ((rc = run_line_pass(g, f, +1, 0, 1.0, prec, s, PRO_CURL6))) return rc;
+    if (pl.k1_fused) {
+      rc = prec == PREC_C128 ? zcurl<double>(pl, f, s) : zcurl<float>(pl, f, s);
+    } else {
+      LineGeo g = axis_geo(2, nx, ny, nz, prec, pl.lineW);
+      rc = run_line_pass(g, f, +1, 0, 1.0, prec, s, PRO_CURL6);
+    }
+    if (rc) return rc;
     mark();
   }
   if (pl.use_xy) {

@@ -10,6 +10,8 @@ namespace sns {
 struct NSPlan {
   int nx, ny, nz, prec;
   int xG;             // rows per CTA of the x cross pass
+  int k1W, k1G;       // K1 tile: adjacent z lines x groups (all six outputs per CTA)
+  bool k1_fused;      // K1 loads V once per tile (else one output field per CTA)
   int zW;             // adjacent z lines per CTA of the update pass
   int update_blocks;  // CTAs of the update pass (= diagnostics partials)
   int sgs_W;          // adjacent z lines per CTA of the closure update (9 fields)

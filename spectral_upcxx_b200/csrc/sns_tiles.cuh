@@ -135,6 +135,80 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
 }
 
 // ---------------------------------------------------------------------------
+// K1 of the NS step with one tile for all six outputs: z lines of a W x G tile
+// of the three components of V are loaded once (thread layout of
+// line_pass_tile, component outermost), the curl omega = i k x V is formed in
+// shared memory from the loaded components, and both vectors are
+// z-inverse-transformed: out(0..2) = V, out(3..5) = omega.  Shared memory:
+// two sets of 3 W G padded rows (V, then omega).
+template <typename T, int L, typename Fields>
+__device__ __forceinline__ void curl_zpass_tile(const LineGeo& geo, const Fields& f,
+                                                const cx_t<T>* __restrict__ tw, int wshift,
+                                                int64_t blk, cx_t<T>* sm) {
+  using C = cx_t<T>;
+  using P = LinePlan<L>;
+  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(L);
+  const int W = geo.W, G = geo.G, lines = W * G;
+  const int64_t base = (blk % geo.TA) * geo.sa + (blk / geo.TA) * geo.sb;
+  const int w = threadIdx.x & (W - 1);
+  const int s = threadIdx.x >> wshift;
+  const int j = s & (TPL - 1);
+  const int s2 = s / TPL;
+  const int g = s2 % G, d = s2 / G;  // line (w, g) of component d
+  const int li = w + W * g;
+  C* rowV = sm + (d * lines + li) * RS;
+  C* rowW = sm + ((3 + d) * lines + li) * RS;
+  const LineCoord lc = line_coord(geo, base, w, g, j, TPL);
+
+  C v[E];
+  {
+    const C* __restrict__ src = reinterpret_cast<const C*>(
+        d == 0 ? f.in(0) : d == 1 ? f.in(1) : f.in(2));
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = src[lc.idx0 + e * lc.step];
+  }
+#pragma unroll
+  for (int e = 0; e < E; e++) rowV[pad_pos(j + TPL * e)] = v[e];
+  __syncthreads();
+  {
+    // omega_d at this thread's positions from the other two components
+    const T kx = (T)freq_i(lc.x, geo.nx), ky = (T)freq_i(lc.y, geo.ny);
+    const C* r0 = sm + (0 * lines + li) * RS;
+    const C* r1 = sm + (1 * lines + li) * RS;
+    const C* r2 = sm + (2 * lines + li) * RS;
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int pp = pad_pos(j + TPL * e);
+      const T kz = (T)freq_i(j + TPL * e, geo.nz);
+      C o;
+      if (d == 0)
+        o = csub(ikmul(ky, r2[pp]), ikmul(kz, r1[pp]));
+      else if (d == 1)
+        o = csub(ikmul(kz, r0[pp]), ikmul(kx, r2[pp]));
+      else
+        o = csub(ikmul(kx, r1[pp]), ikmul(ky, r0[pp]));
+      rowW[pp] = o;
+    }
+  }
+  __syncthreads();
+  line_fft<L, true>(v, rowV, j, tw, (T)1);
+  {
+    C* __restrict__ dst = reinterpret_cast<C*>(d == 0 ? f.out(0) : d == 1 ? f.out(1) : f.out(2));
+#pragma unroll
+    for (int e = 0; e < E; e++) dst[lc.idx0 + e * lc.step] = v[e];
+  }
+#pragma unroll
+  for (int e = 0; e < E; e++) v[e] = rowW[pad_pos(j + TPL * e)];
+  __syncthreads();
+  line_fft<L, true>(v, rowW, j, tw, (T)1);
+  {
+    C* __restrict__ dst = reinterpret_cast<C*>(d == 0 ? f.out(3) : d == 1 ? f.out(4) : f.out(5));
+#pragma unroll
+    for (int e = 0; e < E; e++) dst[lc.idx0 + e * lc.step] = v[e];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // K3 of the NS step: x lines -- inverse 6 fields, 1/N^2-scaled complex cross
 // product u x omega, forward 3 fields (src/Vector.cpp:79-89).  A tile is G
 // rows of all six fields; f.in(0..5) = (u, omega), f.out(0..2) = the product.
