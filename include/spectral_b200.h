@@ -148,6 +148,16 @@ typedef struct sns_ns sns_ns;
  * (ns.cpp:43-46).  Allocates its state and work fields (12 fields). */
 int sns_ns_create(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double nu, double dt,
                   int prec, void* stream);
+/* The same stepper for a real velocity field (no reference counterpart; the
+ * reference transforms real data as complex, src/Scalar.cpp:400-646): it keeps
+ * the half spectrum kx = 0 .. nx/2-1 (the kx = nx/2 plane is zero after
+ * zeroHighModes, and kx < 0 is the complex conjugate), so every pass moves
+ * half the bytes; the x transforms become real-to-complex / complex-to-real.
+ * Its functions take and return full Fourier fields exactly as for
+ * sns_ns_create; inputs must be Hermitian (Fourier transforms of real fields).
+ * nx must be a power of two >= 32.  Closures are not available on it. */
+int sns_ns_create_real(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double nu, double dt,
+                       int prec, void* stream);
 int sns_ns_destroy(sns_ns* handle);
 /* Start from Fourier V0 and omega0 = curl V0: the Pi0 projection and the
  * Forward-Euler first step (ns.cpp:132-153).  Device pointers in the

@@ -65,6 +65,7 @@ SIGNATURES = {
     "sns_axpby": ([_dbl, _vp, _dbl, _vp, _vp, _i64, _int, _vp], _int),
     "sns_mul": ([_vp, _vp, _vp, _i64, _int, _vp], _int),
     "sns_ns_create": ([C.POINTER(_vp), _i64, _i64, _i64, _dbl, _dbl, _int, _vp], _int),
+    "sns_ns_create_real": ([C.POINTER(_vp), _i64, _i64, _i64, _dbl, _dbl, _int, _vp], _int),
     "sns_ns_destroy": ([_vp], _int),
     "sns_ns_bootstrap": ([_vp, _vp3, _vp3], _int),
     "sns_ns_set_state": ([_vp, _vp3, _vp3], _int),

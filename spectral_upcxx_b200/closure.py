@@ -279,10 +279,13 @@ def coarse_run(S, Vc0, nu, dt, steps, model=None, csd2=0.0, kc=0.0, dtype=torch.
 
 
 def evaluate(S, model, nf, nc, kc, seeds, nu, dt, steps, cs=0.17, dtype=torch.complex64,
-             device="cuda"):
+             device="cuda", coarse_dt=None):
     """Spectrum errors (shells 1..kc-1) at the end of `steps` steps against the
     filtered fine DNS, for the plain, Smagorinsky and MLP coarse runs, plus
-    the steps/s of the coarse MLP run and of the fine DNS."""
+    the steps/s of the coarse MLP run and of the fine DNS.  The coarse runs
+    take time step coarse_dt (default dt) and end at the same time."""
+    coarse_dt = dt if coarse_dt is None else coarse_dt
+    coarse_steps = int(round(steps * dt / coarse_dt))
     res = {"plain": [], "smagorinsky": [], "mlp": []}
     spectra = {}
     csd2 = smagorinsky_cs_delta2(cs, kc)
@@ -302,7 +305,7 @@ def evaluate(S, model, nf, nc, kc, seeds, nu, dt, steps, cs=0.17, dtype=torch.co
         for name, kw in (("plain", {}), ("smagorinsky", {"csd2": csd2}), ("mlp", {"model": model})):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            V = coarse_run(S, Vc0, nu, dt, steps, kc=kc, dtype=dtype, **kw)
+            V = coarse_run(S, Vc0, nu, coarse_dt, coarse_steps, kc=kc, dtype=dtype, **kw)
             torch.cuda.synchronize()
             if name == "mlp":
                 t_les += time.perf_counter() - t0
@@ -315,5 +318,7 @@ def evaluate(S, model, nf, nc, kc, seeds, nu, dt, steps, cs=0.17, dtype=torch.co
     out = {k: float(np.mean(v)) for k, v in res.items()}
     out["spectra_first_seed"] = spectra
     out["dns_steps_per_s"] = steps * len(seeds) / t_dns
-    out["mlp_run_steps_per_s"] = steps * len(seeds) / t_les
+    out["mlp_run_steps_per_s"] = coarse_steps * len(seeds) / t_les
+    out["coarse_dt"] = coarse_dt
+    out["all_finite"] = bool(np.all(np.isfinite([v for k in res for v in res[k]])))
     return out

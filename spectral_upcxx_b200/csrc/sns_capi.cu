@@ -161,6 +161,71 @@ int vector_cross(const void* const a[3], const void* const b[3], void* const out
   return fft3d(out, 3, d.nx, d.ny, d.nz, -1, PASS_ZERO_NYQUIST, prec, s, tw_axes);
 }
 
+// Half spectrum (kx = 0 .. nx/2-1) of full Fourier fields of a real field, and
+// the full spectrum back by Hermitian symmetry V(-k) = conj V(k) (the kx = nx/2
+// plane is zero).  Three fields (blockIdx.y).
+template <typename T>
+__global__ void k_half_from_full(FieldPtrs f, int nxp, int ny, int nz) {
+  using C = cx_t<T>;
+  const int M = nxp / 2;
+  const int64_t n = (int64_t)M * ny * nz;
+  const C* __restrict__ in = reinterpret_cast<const C*>(f.in[blockIdx.y]);
+  C* __restrict__ out = reinterpret_cast<C*>(f.out[blockIdx.y]);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t x = i % M, r = i / M;
+    out[i] = in[r * nxp + x];
+  }
+}
+
+template <typename T>
+__global__ void k_full_from_half(FieldPtrs f, int nxp, int ny, int nz) {
+  using C = cx_t<T>;
+  const int M = nxp / 2;
+  const int64_t n = (int64_t)nxp * ny * nz;
+  const C* __restrict__ in = reinterpret_cast<const C*>(f.in[blockIdx.y]);
+  C* __restrict__ out = reinterpret_cast<C*>(f.out[blockIdx.y]);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nxp);
+    const int64_t r = i / nxp;
+    const int y = (int)(r % ny), z = (int)(r / ny);
+    C v = mk((T)0, (T)0);
+    if (x < M) {
+      v = in[r * M + x];
+    } else if (x > M) {
+      const int yy = y == 0 ? 0 : ny - y, zz = z == 0 ? 0 : nz - z;
+      const C c = in[((int64_t)zz * ny + yy) * M + (nxp - x)];
+      v = mk(c.x, -c.y);
+    }
+    out[i] = v;
+  }
+}
+
+// dir = +1: full -> half; -1: half -> full.  Three fields.
+int convert_half(void* const* out, const void* const* in, int nxp, int ny, int nz, int prec,
+                 int dir, cudaStream_t s) {
+  FieldPtrs f{};
+  for (int d = 0; d < 3; d++) {
+    f.in[d] = const_cast<void*>(in[d]);
+    f.out[d] = out[d];
+  }
+  const int64_t n = dir > 0 ? (int64_t)(nxp / 2) * ny * nz : (int64_t)nxp * ny * nz;
+  const dim3 grid((unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 3);
+  if (dir > 0) {
+    if (prec == PREC_C128)
+      k_half_from_full<double><<<grid, 256, 0, s>>>(f, nxp, ny, nz);
+    else
+      k_half_from_full<float><<<grid, 256, 0, s>>>(f, nxp, ny, nz);
+  } else {
+    if (prec == PREC_C128)
+      k_full_from_half<double><<<grid, 256, 0, s>>>(f, nxp, ny, nz);
+    else
+      k_full_from_half<float><<<grid, 256, 0, s>>>(f, nxp, ny, nz);
+  }
+  return cuda_status(cudaGetLastError(), "half-spectrum conversion");
+}
+
 // The bootstrap of ns.cpp:132-153 into V (-> V1) and C0 (-> cross0), with six
 // work fields U.
 int ns_bootstrap_fields(Dims d, int prec, double nu, double dt, const void* const V0[3],
@@ -523,19 +588,24 @@ int sns_mul(const void* a, const void* b, void* out, int64_t n, int prec, void* 
 // ---- fused stepper -------------------------------------------------------------
 int sns_ns_create(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double nu, double dt,
                   int prec, void* stream) {
-  return sns::ns_create_tuned(handle, nx, ny, nz, nu, dt, prec, stream, 0, 0);
+  return sns::ns_create(handle, nx, ny, nz, nu, dt, prec, stream, false);
+}
+
+int sns_ns_create_real(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double nu, double dt,
+                       int prec, void* stream) {
+  return sns::ns_create(handle, nx, ny, nz, nu, dt, prec, stream, true);
 }
 
 }  // extern "C"
 
-// sns_ns_create with tile widths chosen by the ensemble's autotuner (0 = defaults).
-int sns::ns_create_tuned(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double nu,
-                         double dt, int prec, void* stream, int zW, int lineW) {
+// A stepper of complex fields, or (real) of the half spectrum of real fields.
+int sns::ns_create(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double nu, double dt,
+                   int prec, void* stream, bool real) {
   if (!nonnull(handle, "sns_ns_create")) return ERR_ARG;
   *handle = nullptr;
   if (!check_prec(prec) || !check_dims(nx, ny, nz)) return ERR_ARG;
   sns_ns* h = new sns_ns();
-  int rc = ns_plan(h->pl, (int)nx, (int)ny, (int)nz, prec, zW, lineW);
+  int rc = ns_plan(h->pl, (int)nx, (int)ny, (int)nz, prec, 0, 0, real);
   if (rc) {
     delete h;
     return rc;
@@ -543,7 +613,7 @@ int sns::ns_create_tuned(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, do
   h->nu = nu;
   h->dt = dt;
   h->s = S(stream);
-  const size_t bytes = esize(prec) * (size_t)nx * ny * nz;
+  const size_t bytes = esize(prec) * (size_t)h->pl.nx * ny * nz;  // stored (half) rows
   void** all[12];
   for (int d = 0; d < 3; d++) {
     all[d] = &h->V[d];
@@ -599,6 +669,14 @@ int sns_ns_set_state(sns_ns* h, const void* const V1[3], const void* const cross
   if (!nonnull(h, "sns_ns_set_state") || !vec_ok(V1, "sns_ns_set_state") ||
       !vec_ok(cross0, "sns_ns_set_state"))
     return ERR_ARG;
+  if (h->pl.real) {
+    int rc = convert_half(h->V, V1, h->pl.nx_phys, h->pl.ny, h->pl.nz, h->pl.prec, +1, h->s);
+    if (!rc) rc = convert_half(h->C0, cross0, h->pl.nx_phys, h->pl.ny, h->pl.nz, h->pl.prec, +1,
+                               h->s);
+    if (rc) return rc;
+    h->stepped = false;
+    return OK;
+  }
   const size_t bytes = esize(h->pl.prec) * (size_t)h->pl.nx * h->pl.ny * h->pl.nz;
   int rc;
   for (int d = 0; d < 3; d++) {
@@ -618,8 +696,26 @@ int sns_ns_bootstrap(sns_ns* h, const void* const V0[3], const void* const omega
   if (!nonnull(h, "sns_ns_bootstrap") || !vec_ok(V0, "sns_ns_bootstrap") ||
       !vec_ok(omega0, "sns_ns_bootstrap"))
     return ERR_ARG;
+  int rc;
+  if (h->pl.real) {
+    // bootstrap on full fields (pooled temporaries), then keep the half spectrum
+    const Dims d{h->pl.nx_phys, h->pl.ny, h->pl.nz};
+    const size_t bytes = esize(h->pl.prec) * (size_t)d.n();
+    void* t[12] = {};
+    rc = OK;
+    for (int i = 0; i < 12 && !rc; i++) rc = pool_malloc(&t[i], bytes);
+    if (!rc) rc = ns_bootstrap_fields(d, h->pl.prec, h->nu, h->dt, V0, omega0, t, t + 3, t + 6,
+                                      h->s);
+    if (!rc) rc = convert_half(h->V, t, d.nx, d.ny, d.nz, h->pl.prec, +1, h->s);
+    if (!rc) rc = convert_half(h->C0, t + 3, d.nx, d.ny, d.nz, h->pl.prec, +1, h->s);
+    cudaStreamSynchronize(h->s);
+    for (void* p : t) pool_free(p);
+    if (rc) return rc;
+    h->stepped = false;
+    return OK;
+  }
   const Dims d{h->pl.nx, h->pl.ny, h->pl.nz};
-  int rc = ns_bootstrap_fields(d, h->pl.prec, h->nu, h->dt, V0, omega0, h->V, h->C0, h->U, h->s);
+  rc = ns_bootstrap_fields(d, h->pl.prec, h->nu, h->dt, V0, omega0, h->V, h->C0, h->U, h->s);
   if (rc) return rc;
   h->stepped = false;
   return OK;
@@ -704,6 +800,36 @@ int sns_ns_pass_times(sns_ns* h, double* total_ms, int* launches, int max) {
 
 int sns_ns_get_state(sns_ns* h, void* const V1[3], void* const omega1[3], void* const cross0[3]) {
   if (!nonnull(h, "sns_ns_get_state")) return ERR_ARG;
+  if (h->pl.real) {
+    // full spectra rebuilt by Hermitian symmetry
+    const Dims d{h->pl.nx_phys, h->pl.ny, h->pl.nz};
+    const size_t bytes = esize(h->pl.prec) * (size_t)d.n();
+    int rc = OK;
+    if (cross0 && cross0[0] && cross0[1] && cross0[2])
+      rc = convert_half(cross0, h->C0, d.nx, d.ny, d.nz, h->pl.prec, -1, h->s);
+    if (rc || (!omega1 && !(V1 && V1[0] && V1[1] && V1[2]))) return rc;
+    void* t[3] = {};
+    const bool own = !(V1 && V1[0] && V1[1] && V1[2]);
+    void* const* vf = V1;
+    if (own) {
+      for (int i = 0; i < 3 && !rc; i++) rc = pool_malloc(&t[i], bytes);
+      vf = t;
+    }
+    if (!rc) rc = convert_half(vf, h->V, d.nx, d.ny, d.nz, h->pl.prec, -1, h->s);
+    if (!rc && omega1) {
+      if (!vec_ok((const void* const*)omega1, "sns_ns_get_state")) {
+        rc = ERR_ARG;
+      } else {
+        const void* v[3] = {vf[0], vf[1], vf[2]};
+        rc = op_curl(v, omega1, d, h->pl.prec, h->s);
+      }
+    }
+    if (own) {
+      cudaStreamSynchronize(h->s);
+      for (void* p : t) pool_free(p);
+    }
+    return rc;
+  }
   const Dims d{h->pl.nx, h->pl.ny, h->pl.nz};
   const size_t bytes = esize(h->pl.prec) * (size_t)d.n();
   int rc;
@@ -760,7 +886,7 @@ int sns_ns_stats(sns_ns* h, double* div_avg, double* energy, double* enstrophy, 
                         "sns_ns_stats")))
     return rc;
   if ((rc = cuda_status(cudaStreamSynchronize(h->s), "sns_ns_stats"))) return rc;
-  const double N = (double)h->pl.nx * h->pl.ny * h->pl.nz;
+  const double N = (double)h->pl.nx_phys * h->pl.ny * h->pl.nz;  // full grid
   if (div_avg) *div_avg = v[0] / N;
   if (energy) *energy = 0.5 * v[1] / (N * N);
   if (enstrophy) *enstrophy = 0.5 * v[2] / (N * N);
@@ -775,6 +901,10 @@ int sns_ns_launches_per_step(sns_ns* h) {
 
 int sns_ns_set_closure(sns_ns* h, int model, double cs_delta2, const void* mlp, double kc) {
   if (!nonnull(h, "sns_ns_set_closure")) return ERR_ARG;
+  if (h->pl.real && model != SNS_CLOSURE_NONE) {
+    set_error("sns_ns_set_closure: closures run on complex-field steppers only");
+    return ERR_UNSUPPORTED;
+  }
   if (!(kc >= 0)) {
     set_error("sns_ns_set_closure: the cutoff must be >= 0 (0: none)");
     return ERR_ARG;

@@ -119,6 +119,7 @@ __device__ __forceinline__ void ens_item(const EnsClass* __restrict__ k,
       a.nuhK = box->nuhK;
       a.stats = box->stats;
       a.kc2 = 1e300;
+      a.kx_half = 0;
     }
     __syncthreads();
     zfwd_update_tile<T, L>(a, tw, blk, (int)blockDim.x, sm, red);
@@ -339,7 +340,7 @@ bool make_class(const sns_ens* e, int s, int c, const StageCfg& cfg, EnsClass& k
     k.L = nx;
     k.G = G;
     k.tiles = rows / G;
-    smem = (size_t)6 * G * row_stride(nx) * esz;
+    smem = (size_t)6 * G * xrow_stride(nx) * esz;
   } else {
     const int tpl = tpl_of(nz);
     if (T % (3 * tpl)) return false;

@@ -13,10 +13,10 @@ namespace sns {
 int pool_malloc(void** ptr, size_t bytes);
 int pool_free(void* ptr);
 
-// sns_ns_create with tuned tile widths (0 = the defaults): zW is the number of
-// adjacent z lines per CTA of the update pass, lineW that of the y/z passes.
-int ns_create_tuned(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double nu, double dt,
-                    int prec, void* stream, int zW, int lineW);
+// A stepper of complex fields (sns_ns_create) or of the half spectrum of real
+// fields (sns_ns_create_real).
+int ns_create(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double nu, double dt,
+              int prec, void* stream, bool real);
 
 // The bootstrap of ns.cpp:132-153 on caller-owned fields: V <- V1, C0 <- cross0,
 // with six work fields U.

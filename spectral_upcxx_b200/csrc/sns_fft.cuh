@@ -42,6 +42,9 @@ struct LineGeo {
   int axis;
   // twiddle table to use instead of the cached one (null: cached table)
   const void* tw;
+  // half-spectrum fields of a real-field run: x index i holds kx = i
+  // (0 <= i < nx), the kx < 0 half being the complex conjugate; no x-Nyquist
+  int kx_half;
 };
 
 struct FieldPtrs {

@@ -26,6 +26,13 @@ __host__ __device__ constexpr int pad_pos(int p) { return p + (p >> 4); }
 __host__ __device__ constexpr int row_stride(int L) {
   return (pad_pos(L) & 1) ? pad_pos(L) : pad_pos(L) + 1;
 }
+// Row stride of a tile of x lines, whose TPL threads access TPL consecutive
+// positions while 32 / TPL lines share a warp: pad_pos(L) = L + TPL is TPL
+// modulo 16 (8-byte slots), so the lines of a warp tile the banks exactly;
+// lines shorter than 16 (one thread each) keep the odd stride.
+__host__ __device__ constexpr int xrow_stride(int L) {
+  return L >= 16 ? pad_pos(L) : row_stride(L);
+}
 
 template <int L>
 struct LinePlan {

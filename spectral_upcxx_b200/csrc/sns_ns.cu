@@ -41,6 +41,117 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
 }
 
 // ---------------------------------------------------------------------------
+// K3 of a real-field run: rows of the half spectrum, M = nx/2 values
+// (kx = 0 .. M-1; kx = M is a Nyquist mode, zero).  Inverse: the real line u of
+// length 2M comes from one M-point complex FFT of
+//   Z[k] = (V[k] + conj V[M-k]) + i w^k (V[k] - conj V[M-k]),  w = e^{+2 pi i/2M},
+// V[M] = 0, as z[m] = u[2m] + i u[2m+1].  The cross product acts on the two real
+// samples of every complex slot.  Forward: Z = FFT_M(c[2m] + i c[2m+1]) and
+//   C[k] = (Z[k] + conj Z[M-k]) / 2 - i W^k (Z[k] - conj Z[M-k]) / 2,  W = e^{-2 pi i/2M}.
+// twN: the 2M-point table exp(-2 pi i m / 2M); twM: the M-point table.
+// The pre- and post-processing run on pairs (k, M-k) in shared memory, so no
+// line values stay in registers across them; FP32 fits two CTAs per SM.
+template <typename T, int M>
+__global__ void __launch_bounds__(384, sizeof(T) == 4 ? 2 : 1)
+    k_xcross_r2c(FieldPtrs f, const cx_t<T>* __restrict__ twN, const cx_t<T>* __restrict__ twM,
+                 int G, T scale2) {
+  using C = cx_t<T>;
+  using P = LinePlan<M>;
+  constexpr int E = P::E, TPL = P::TPL, RS = xrow_stride(M);
+  static_assert(TPL <= 32, "a line's threads share a warp");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sm = reinterpret_cast<C*>(smem_raw);
+  const int64_t row0 = (int64_t)blockIdx.x * G;
+  const int per = G * M;
+  const int j = threadIdx.x % TPL, line = threadIdx.x / TPL;
+  const int fld = line / G, gl = line - fld * G;
+  C* row = sm + line * RS;
+  C v[E];
+  {
+    const C* __restrict__ src = reinterpret_cast<const C*>(select_ptr(f.in, fld));
+    const int64_t i0 = (row0 + gl) * M + j;
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = src[i0 + TPL * e];
+  }
+#pragma unroll
+  for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
+  line_sync<TPL>();
+  // Z in place, one thread per pair (k, M-k):  with A = V[k] + conj V[M-k] and
+  // B = V[k] - conj V[M-k],  Z[k] = A + i w^k B  and  Z[M-k] = conj(A - i w^k B)
+#pragma unroll 1
+  for (int e = 0; e <= M / (2 * TPL); e++) {
+    const int k = j + TPL * e;
+    if (k <= M / 2) {
+      const C vk = row[pad_pos(k)];
+      const C vm = k == 0 ? mk((T)0, (T)0) : row[pad_pos(M - k)];
+      const C vmc = mk(vm.x, -vm.y);
+      const C a = cadd(vk, vmc), b = csub(vk, vmc);
+      const C wb = cmul(mk(twN[k].x, -twN[k].y), b);  // w^k b, w = e^{+2 pi i / 2M}
+      row[pad_pos(k)] = mk(a.x - wb.y, a.y + wb.x);
+      if (k > 0 && k < M / 2) row[pad_pos(M - k)] = mk(a.x + wb.y, wb.x - a.y);
+    }
+  }
+  line_sync<TPL>();
+#pragma unroll
+  for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
+  line_sync<TPL>();
+  line_fft<M>(v, row, j, twM, (T)1);
+#pragma unroll
+  for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
+  __syncthreads();
+
+  // c = (u/N) x (omega/N) on the real samples (.x and .y of each slot)
+  for (int q = threadIdx.x; q < per; q += blockDim.x) {
+    const int g = q / M, p = q & (M - 1);
+    C u[3], w[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      u[d] = sm[(d * G + g) * RS + pad_pos(p)];
+      w[d] = sm[((3 + d) * G + g) * RS + pad_pos(p)];
+    }
+    const C c0 = mk(u[1].x * w[2].x - u[2].x * w[1].x, u[1].y * w[2].y - u[2].y * w[1].y);
+    const C c1 = mk(u[2].x * w[0].x - u[0].x * w[2].x, u[2].y * w[0].y - u[0].y * w[2].y);
+    const C c2 = mk(u[0].x * w[1].x - u[1].x * w[0].x, u[0].y * w[1].y - u[1].y * w[0].y);
+    sm[(0 * G + g) * RS + pad_pos(p)] = cscale(scale2, c0);
+    sm[(1 * G + g) * RS + pad_pos(p)] = cscale(scale2, c1);
+    sm[(2 * G + g) * RS + pad_pos(p)] = cscale(scale2, c2);
+  }
+  __syncthreads();
+
+  // forward: warps holding only omega rows skip it (as in k_xcross)
+  constexpr int kLinesPerWarp = 32 / TPL;
+  const bool skip = (G % kLinesPerWarp == 0) && fld >= 3;
+  if (!skip) {
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
+    line_sync<TPL>();
+    line_fft<M>(v, row, j, twM, (T)-1);
+#pragma unroll
+    for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
+    line_sync<TPL>();
+  }
+  if (fld < 3) {
+    // one thread per pair (k, M-k):  with Ev = (Z[k] + conj Z[M-k]) / 2 and
+    // Od = (Z[k] - conj Z[M-k]) / 2,  C[k] = Ev - i W^k Od  and
+    // C[M-k] = conj(Ev + i W^k Od)
+    C* __restrict__ dst = reinterpret_cast<C*>(select_ptr(f.out, fld)) + (row0 + gl) * M;
+#pragma unroll 1
+    for (int e = 0; e <= M / (2 * TPL); e++) {
+      const int k = j + TPL * e;
+      if (k <= M / 2) {
+        const C z = row[pad_pos(k)];
+        const C zm = row[pad_pos(k == 0 ? 0 : M - k)];
+        const C ev = mk((T)0.5 * (z.x + zm.x), (T)0.5 * (z.y - zm.y));
+        const C od = mk((T)0.5 * (z.x - zm.x), (T)0.5 * (z.y + zm.y));
+        const C wo = cmul(twN[k], od);  // W^k od
+        dst[k] = mk(ev.x + wo.y, ev.y - wo.x);
+        if (k > 0 && k < M / 2) dst[M - k] = mk(ev.x - wo.y, -(ev.y + wo.x));
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // K1: z lines -- inverse of V and of omega = i k x V from one load of V.
 template <typename T, int L>
 __global__ void __launch_bounds__(MaxThreads<T>::value)
@@ -100,7 +211,7 @@ int launch_xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream
   constexpr int TPL = LinePlan<L>::TPL;
   const int G = pl.xG;
   const int threads = 6 * G * TPL;
-  const size_t smem = (size_t)6 * G * row_stride(L) * sizeof(C);
+  const size_t smem = (size_t)6 * G * xrow_stride(L) * sizeof(C);
   static bool attr[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -129,6 +240,7 @@ int launch_zcurl(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
   g.nx = pl.nx;
   g.ny = pl.ny;
   g.nz = pl.nz;
+  g.kx_half = pl.real;
   g.ps = (int64_t)pl.nx * pl.ny;
   g.gs = pl.nx;
   g.TA = pl.nx / g.W;
@@ -155,6 +267,48 @@ int launch_zcurl(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
   k_zcurl<T, L><<<(unsigned)(g.TA * g.TB), threads, smem, s>>>(g, f, tw, wshift);
   SNS_CHECK_LAUNCH("k_zcurl");
   return OK;
+}
+
+template <typename T, int M>
+int launch_xcross_r2c(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream_t s) {
+  using C = cx_t<T>;
+  constexpr int TPL = LinePlan<M>::TPL;
+  const int G = pl.xG;
+  const int threads = 6 * G * TPL;
+  const size_t smem = (size_t)6 * G * xrow_stride(M) * sizeof(C);
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr[dev & 63]) {
+    cudaError_t e = allow_max_dynamic_smem(k_xcross_r2c<T, M>);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_xcross_r2c)");
+    attr[dev & 63] = true;
+  }
+  const int prec = sizeof(T) == 8 ? PREC_C128 : PREC_C64;
+  const C* twN = reinterpret_cast<const C*>(twiddles(2 * M, prec));
+  const C* twM = reinterpret_cast<const C*>(twiddles(M, prec));
+  if (!twN || !twM) {
+    set_error("twiddle table allocation failed");
+    return ERR_ALLOC;
+  }
+  const double N = (double)pl.nx_phys * pl.ny * pl.nz;
+  k_xcross_r2c<T, M><<<(unsigned)(rows / G), threads, smem, s>>>(f, twN, twM, G,
+                                                                   (T)(1.0 / (N * N)));
+  SNS_CHECK_LAUNCH("k_xcross_r2c");
+  return OK;
+}
+
+template <typename T>
+int xcross_r2c(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream_t s) {
+  switch (pl.nx) {
+    case 16: return launch_xcross_r2c<T, 16>(pl, f, rows, s);
+    case 32: return launch_xcross_r2c<T, 32>(pl, f, rows, s);
+    case 64: return launch_xcross_r2c<T, 64>(pl, f, rows, s);
+    case 128: return launch_xcross_r2c<T, 128>(pl, f, rows, s);
+    case 256: return launch_xcross_r2c<T, 256>(pl, f, rows, s);
+    case 512: return launch_xcross_r2c<T, 512>(pl, f, rows, s);
+    default: set_error("real-field NS step: nx must be a power of two in [32, 1024]"); return ERR_UNSUPPORTED;
+  }
 }
 
 template <typename T>
@@ -227,12 +381,30 @@ int update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
   }
 }
 
+// K3 of the plan: complex rows, or half-spectrum rows of a real-field run
+int xpass(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream_t s) {
+  if (pl.real)
+    return pl.prec == PREC_C128 ? xcross_r2c<double>(pl, f, rows, s)
+                                : xcross_r2c<float>(pl, f, rows, s);
+  return pl.prec == PREC_C128 ? xcross<double>(pl, f, rows, s) : xcross<float>(pl, f, rows, s);
+}
+
 int elems(int L) { return L >= 16 ? 16 : L; }
 
 }  // namespace
 
-int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW) {
+int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, bool real) {
   pl = NSPlan{};
+  pl.real = real;
+  pl.nx_phys = nx;
+  if (real) {
+    // half spectrum: kx = 0 .. nx/2-1 stored (the kx = nx/2 plane is zero)
+    if (!is_pow2(nx) || nx < 32 || nx > 1024) {
+      set_error("real-field NS step: nx must be a power of two in [32, 1024]");
+      return ERR_UNSUPPORTED;
+    }
+    nx /= 2;
+  }
   pl.nx = nx;
   pl.ny = ny;
   pl.nz = nz;
@@ -248,7 +420,7 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW) {
     const int TPL = nx / elems(nx);
     int G = 1;
     while (6 * (G * 2) * TPL <= 384 && ((int64_t)ny * nz) % (G * 2) == 0 &&
-           (size_t)6 * G * 2 * row_stride(nx) * esz <= 110 * 1024)
+           (size_t)6 * G * 2 * xrow_stride(nx) * esz <= 110 * 1024)
       G *= 2;
     if (6 * G * TPL > max_threads(prec)) {
       set_error("fused NS step: nx too large for the x-pass tile");
@@ -310,7 +482,8 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW) {
   // (1.09 vs 0.79 ms): these passes are bound by issue and latency, not HBM.
   const char* env = getenv("SNS_XY_PASSES");
   const bool dataflow = env && env[0] == '1';
-  pl.use_xy = dataflow && xy_supported(nx, ny, prec) && xy_plan(pl.xy, nx, ny, nz, prec) == OK;
+  pl.use_xy = !real && dataflow && xy_supported(nx, ny, prec) &&
+              xy_plan(pl.xy, nx, ny, nz, prec) == OK;
   // separate passes run in slabs of xy_chunk planes (SNS_XY_CHUNK; 0 = one slab)
   pl.xy_chunk = 0;
   if (const char* e = getenv("SNS_XY_CHUNK")) pl.xy_chunk = atoi(e);
@@ -341,6 +514,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
       rc = prec == PREC_C128 ? zcurl<double>(pl, f, s) : zcurl<float>(pl, f, s);
     } else {
       LineGeo g = axis_geo(2, nx, ny, nz, prec, pl.lineW);
+      g.kx_half = pl.real;
       rc = run_line_pass(g, f, +1, 0, 1.0, prec, s, PRO_CURL6);
     }
     if (rc) return rc;
@@ -373,7 +547,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
       for (int i = 0; i < 6; i++) f.in[i] = Uc[i];
       for (int i = 0; i < 3; i++) f.out[i] = Uc[i];
       const int64_t rows = (int64_t)ny * pz;
-      int r = prec == PREC_C128 ? xcross<double>(pl, f, rows, s) : xcross<float>(pl, f, rows, s);
+      int r = xpass(pl, f, rows, s);
       if (r) return r;
       if (marks) mark();
     }
@@ -415,6 +589,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     a.nuhK = nu * dt / 2;
     a.stats = stats;
     a.kc2 = pl.kc2;
+    a.kx_half = pl.real;
     rc = ns_update(pl, a, false, s);
     if (rc) return rc;
     mark();

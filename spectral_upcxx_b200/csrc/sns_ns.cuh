@@ -21,11 +21,16 @@ struct NSPlan {
   int xy_chunk;       // planes per slab of the separate xy passes (0 = all)
   int lineW;          // adjacent lines per tile of the y/z line passes (0 = default)
   int passes;         // timed phases per step: z-inverse, xy, z-forward+update
+  bool real;          // half-spectrum fields of a real velocity (R2C / C2R along x)
+  int nx_phys;        // physical nx (= nx, or 2 nx for a real-field run)
   double kc2;         // spectral cutoff |k|^2 <= kc2 of the evolved modes (1e300: none)
 };
 
 // zW > 0 and lineW > 0 select tuned tile widths (0 = defaults).
-int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW = 0, int lineW = 0);
+// real = true: a real-field run on the half spectrum kx = 0 .. nx/2-1 (pl.nx
+// is then nx/2, the stored row length; pl.nx_phys = nx).
+int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW = 0, int lineW = 0,
+            bool real = false);
 // One step in place on V (Fourier velocity) and C0 (previous cross product),
 // with six work fields U; per-block diagnostics go to `stats`
 // (4 doubles x update_blocks).

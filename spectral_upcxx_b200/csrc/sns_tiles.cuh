@@ -77,7 +77,7 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
                                                cx_t<T>* sm) {
   using C = cx_t<T>;
   using P = LinePlan<L>;
-  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(L);
+  constexpr int E = P::E, TPL = P::TPL;
 
   const int field = (int)(blk % nf);
   const int64_t t = blk / nf;
@@ -87,6 +87,8 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
   const int s = threadIdx.x >> wshift;
   const int j = s & (TPL - 1);
   const int g = s / TPL;
+  // single lines (x) share warps line by line; runs of W > 1 read columns
+  const int RS = W == 1 ? xrow_stride(L) : row_stride(L);
   C* row = sm + (w + W * g) * RS;
   const LineCoord lc = line_coord(geo, base, w, g, j, TPL);
 
@@ -104,7 +106,8 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
     }
     const int q = PRO == PRO_GRAD12 ? f.first() + field : field;
     // wavenumbers of the line: two are fixed, the one along the axis varies
-    const T kx0 = (T)freq_i(lc.x, geo.nx), ky0 = (T)freq_i(lc.y, geo.ny),
+    const T kx0 = geo.kx_half ? (T)lc.x : (T)freq_i(lc.x, geo.nx),
+            ky0 = (T)freq_i(lc.y, geo.ny),
             kz0 = (T)freq_i(lc.z, geo.nz);
     const int naxis = geo.axis == 0 ? geo.nx : geo.axis == 1 ? geo.ny : geo.nz;
 #pragma unroll
@@ -120,7 +123,7 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
   C* __restrict__ dst = reinterpret_cast<C*>(f.out(field));
   const bool do_scale = flags & PASS_SCALE;
   const bool do_zero = flags & PASS_ZERO_NYQUIST;
-  const bool line_on_plane = (geo.axis != 0 && lc.x == (geo.nx >> 1)) ||
+  const bool line_on_plane = (geo.axis != 0 && !geo.kx_half && lc.x == (geo.nx >> 1)) ||
                              (geo.axis != 1 && lc.y == (geo.ny >> 1)) ||
                              (geo.axis != 2 && lc.z == (geo.nz >> 1));
   const int half_axis = geo.axis == 0 ? (geo.nx >> 1) : geo.axis == 1 ? (geo.ny >> 1)
@@ -172,7 +175,8 @@ __device__ __forceinline__ void curl_zpass_tile(const LineGeo& geo, const Fields
   __syncthreads();
   {
     // omega_d at this thread's positions from the other two components
-    const T kx = (T)freq_i(lc.x, geo.nx), ky = (T)freq_i(lc.y, geo.ny);
+    const T kx = geo.kx_half ? (T)lc.x : (T)freq_i(lc.x, geo.nx);
+    const T ky = (T)freq_i(lc.y, geo.ny);
     const C* r0 = sm + (0 * lines + li) * RS;
     const C* r1 = sm + (1 * lines + li) * RS;
     const C* r2 = sm + (2 * lines + li) * RS;
@@ -217,7 +221,7 @@ __device__ __forceinline__ void xcross_tile(const Fields& f, const cx_t<T>* __re
                                             T scale2, int64_t blk, int nthr, cx_t<T>* sm) {
   using C = cx_t<T>;
   using P = LinePlan<L>;
-  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(L);
+  constexpr int E = P::E, TPL = P::TPL, RS = xrow_stride(L);
   const int64_t row0 = blk * G;
   const int per = G * L;
 
@@ -296,6 +300,7 @@ struct UpdateArgs {
   // i k_j tau_ij joins cross1 before the Nyquist zeroing
   const void* tau[6];
   double kc2;  // spectral cutoff |k|^2 <= kc2 of an LES run (1e300: none)
+  int kx_half;  // half-spectrum fields (see LineGeo::kx_half)
 };
 
 // Field f of the update's z-forward: the cross product (f < 3) or, with the
@@ -356,11 +361,15 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
     const int64_t xy = base + w;
     const int x = (int)(xy & (a.nx - 1)), y = (int)(xy >> a.lx);
     const int64_t idx = xy + nxy * z;
-    const T kx = (T)freq_i(x, a.nx), ky = (T)freq_i(y, a.ny), kz = (T)freq_i(z, a.nz);
+    const T kx = a.kx_half ? (T)x : (T)freq_i(x, a.nx);
+    const T ky = (T)freq_i(y, a.ny), kz = (T)freq_i(z, a.nz);
     const double k2d = (double)kx * kx + (double)ky * ky + (double)kz * kz;
     // modes beyond the cutoff are not evolved (zero velocity and history)
     const bool cut = k2d > a.kc2;
-    const bool nyq = cut || y == (a.ny >> 1) || x == (a.nx >> 1) || z == (a.nz >> 1);
+    const bool nyq = cut || y == (a.ny >> 1) || (!a.kx_half && x == (a.nx >> 1)) ||
+                     z == (a.nz >> 1);
+    // half spectrum: each stored kx > 0 mode stands for itself and its conjugate
+    const double wgt = (a.kx_half && x > 0) ? 2.0 : 1.0;
     C c1[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) c1[d] = nyq ? mk((T)0, (T)0) : sm[(d * W + w) * RS + pad_pos(z)];
@@ -422,7 +431,7 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
     // diagnostics of the new velocity: per-mode terms in T, sums in FP64
     const C dv = cadd(cadd(ikmul(kx, Vn[0]), ikmul(ky, Vn[1])), ikmul(kz, Vn[2]));
     const double ad = (double)sqrt(dv.x * dv.x + dv.y * dv.y);
-    s_div += ad;
+    s_div += wgt * ad;
     m_div = fmax(m_div, ad);
     T e2 = 0;
 #pragma unroll
@@ -432,8 +441,8 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
     const C om2 = csub(ikmul(kx, Vn[1]), ikmul(ky, Vn[0]));
     const T w2 = om0.x * om0.x + om0.y * om0.y + om1.x * om1.x + om1.y * om1.y +
                  om2.x * om2.x + om2.y * om2.y;
-    s_e += (double)e2;
-    s_w += (double)w2;
+    s_e += wgt * (double)e2;
+    s_w += wgt * (double)w2;
   };
   // two points per iteration: the 12 global loads of both are issued first
   for (int q0 = threadIdx.x; q0 < per; q0 += 2 * nthr) {

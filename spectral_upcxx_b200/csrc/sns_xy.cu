@@ -125,7 +125,7 @@ __device__ __forceinline__ void item_xcross(const XYArgs& a, cx_t<T>* sm, int z,
                                             const cx_t<T>* tw) {
   using C = cx_t<T>;
   using P = LinePlan<LX>;
-  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(LX);
+  constexpr int E = P::E, TPL = P::TPL, RS = xrow_stride(LX);
   const int G = a.G;
   const int t = threadIdx.x;
   const int line = t / TPL, j = t % TPL;
@@ -311,8 +311,8 @@ int xy_plan(XYPlan& p, int nx, int ny, int nz, int prec) {
   p.G = G;
   p.threads = 3 * W * tply;
   p.smem_bytes = (size_t)(3 * W) * row_stride(ny) * esz;
-  if ((size_t)(6 * G) * row_stride(nx) * esz > p.smem_bytes)
-    p.smem_bytes = (size_t)(6 * G) * row_stride(nx) * esz;
+  if ((size_t)(6 * G) * xrow_stride(nx) * esz > p.smem_bytes)
+    p.smem_bytes = (size_t)(6 * G) * xrow_stride(nx) * esz;
   p.nA = 2 * (nx / W);
   p.nB = ny / G;
   p.nC = nx / W;

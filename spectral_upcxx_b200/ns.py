@@ -15,7 +15,11 @@ from .ops import _check_field, _stream
 
 
 class NSStepper:
-    def __init__(self, shape, nu: float, dt: float, dtype=torch.complex128, device="cuda"):
+    """real=True keeps the half spectrum of a real velocity field
+    (sns_ns_create_real); the interface is unchanged."""
+
+    def __init__(self, shape, nu: float, dt: float, dtype=torch.complex128, device="cuda",
+                 real: bool = False):
         nz, ny, nx = shape
         self.shape = tuple(shape)
         self.nu, self.dt = float(nu), float(dt)
@@ -26,8 +30,8 @@ class NSStepper:
         self.prec = N.SNS_C64 if dtype == torch.complex64 else N.SNS_C128
         self._stream = torch.cuda.current_stream(self.device)
         h = C.c_void_p()
-        N.call("sns_ns_create", C.byref(h), nx, ny, nz, self.nu, self.dt, self.prec,
-               C.c_void_p(self._stream.cuda_stream))
+        N.call("sns_ns_create_real" if real else "sns_ns_create", C.byref(h), nx, ny, nz, self.nu,
+               self.dt, self.prec, C.c_void_p(self._stream.cuda_stream))
         self.h = h
 
     def close(self):

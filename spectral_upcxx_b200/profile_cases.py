@@ -1,6 +1,6 @@
 """Small, fixed workloads for profiling the kernels under ncu.
 
-    python -m spectral_upcxx_b200.profile_cases ns128|ns256|ens|closure64|mlp
+    python -m spectral_upcxx_b200.profile_cases ns128|ns256|ns256r|ens|closure64|mlp
 
 Each case builds its inputs on the device, runs a few steps of one path and
 exits; sizes keep every case to a few GB of device memory so that a full ncu
@@ -23,9 +23,11 @@ from . import ic
 def run(case: str) -> None:
     dev = torch.device("cuda", 0)
     if case.startswith("ns"):
-        n = int(case[2:])
+        # a trailing r: the real-field stepper (half spectrum)
+        real = case.endswith("r")
+        n = int(case[2:].rstrip("r"))
         V0 = [x.to(torch.complex64) for x in ic.solenoidal_spectrum_hat(n, 1, dev)]
-        st = NSStepper((n, n, n), 1 / 400, 5e-4, torch.complex64, device=dev)
+        st = NSStepper((n, n, n), 1 / 400, 5e-4, torch.complex64, device=dev, real=real)
         st.bootstrap(V0, curl(V0))
         st.step(3)
     elif case == "ens":
