@@ -330,7 +330,7 @@ bool make_class(const sns_ens* e, int s, int c, const StageCfg& cfg, EnsClass& k
     k.wshift = log2i(W);
     k.nf = s == 3 ? 3 : 6;
     k.tiles = g.TA * g.TB * k.nf;
-    smem = (size_t)lines * row_stride(L) * esz;
+    smem = (size_t)lines * tile_stride(L, W) * esz;
   } else if (s == 2) {
     const int tpl = tpl_of(nx);
     if (T % (6 * tpl)) return false;
@@ -350,7 +350,7 @@ bool make_class(const sns_ens* e, int s, int c, const StageCfg& cfg, EnsClass& k
     k.L = nz;
     k.W = W;
     k.tiles = cols / W;
-    smem = (size_t)3 * W * row_stride(nz) * esz;
+    smem = (size_t)3 * W * tile_stride(nz, W) * esz;
   }
   k.tw = twiddles(k.L, e->prec);
   return k.tw != nullptr && smem <= 200 * 1024;

@@ -26,13 +26,22 @@ __host__ __device__ constexpr int pad_pos(int p) { return p + (p >> 4); }
 __host__ __device__ constexpr int row_stride(int L) {
   return (pad_pos(L) & 1) ? pad_pos(L) : pad_pos(L) + 1;
 }
-// Row stride of a tile of x lines, whose TPL threads access TPL consecutive
-// positions while 32 / TPL lines share a warp: pad_pos(L) = L + TPL is TPL
-// modulo 16 (8-byte slots), so the lines of a warp tile the banks exactly;
-// lines shorter than 16 (one thread each) keep the odd stride.
-__host__ __device__ constexpr int xrow_stride(int L) {
-  return L >= 16 ? pad_pos(L) : row_stride(L);
+// Row stride of a tile whose half-warps hold 16 / J lines of J consecutive
+// positions each: J = min(TPL, 16 / W) for runs of W adjacent lines (thread
+// index w fastest; W = 1 for single x lines).  An 8-byte access is served per
+// half-warp, so its 16 lanes must fall on distinct 8-byte slots (modulo 16): a
+// stride of J times an odd number does that.  J = 1 is the odd stride of
+// row_stride.
+__host__ __device__ constexpr int tile_stride(int L, int W) {
+  const int tpl = L >= 16 ? L / 16 : 1;
+  const int J = W >= 16 ? 1 : (16 / W < tpl ? 16 / W : tpl);
+  int rs = pad_pos(L);
+  if (J >= 16) return rs;
+  while (rs % J != 0 || ((rs / J) & 1) == 0) rs++;
+  return rs;
 }
+// Tiles of x lines: pad_pos(L) = 17 TPL for L >= 16.
+__host__ __device__ constexpr int xrow_stride(int L) { return tile_stride(L, 1); }
 
 template <int L>
 struct LinePlan {

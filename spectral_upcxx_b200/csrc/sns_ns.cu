@@ -248,7 +248,7 @@ int launch_zcurl(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
   g.sa = g.W;
   g.sb = (int64_t)g.G * pl.nx;
   const int threads = 3 * g.W * g.G * TPL;
-  const size_t smem = (size_t)6 * g.W * g.G * row_stride(L) * sizeof(C);
+  const size_t smem = (size_t)6 * g.W * g.G * tile_stride(L, g.W) * sizeof(C);
   static bool attr[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -333,7 +333,7 @@ int launch_update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
   constexpr int TPL = LinePlan<L>::TPL;
   constexpr int NF = SGS ? 9 : 3;
   const int threads = NF * a.W * TPL;
-  const size_t smem = (size_t)NF * a.W * row_stride(L) * sizeof(C);
+  const size_t smem = (size_t)NF * a.W * tile_stride(L, a.W) * sizeof(C);
   const int blocks = (int)(((int64_t)pl.nx * pl.ny) / a.W);
   static bool attr[64] = {false};
   int dev = 0;
@@ -433,23 +433,30 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
   {
     // 16 adjacent lines keep the half-warps of the exchanges on distinct banks;
     // the two row sets of a 16-line tile take 210 KB at 256 (opt-in limit 227 KB)
+    // Two CTAs per SM (112 KB each), so that one CTA's loads overlap the
+    // other's transforms; tile_stride keeps narrower runs free of bank
+    // conflicts.  SNS_K1_SMEM_KB overrides the cap (220: one CTA per SM).
     const int TPL = nz / elems(nz);
     const int cap = max_threads(prec);
-    const size_t smem_cap = 220 * 1024;
+    size_t smem_cap = 112 * 1024;
+    if (const char* e = getenv("SNS_K1_SMEM_KB")) {
+      const int v = atoi(e);
+      if (v >= 16 && v <= 220) smem_cap = (size_t)v * 1024;
+    }
     int W = 1;
     const int Wmax = prec == PREC_C128 ? 8 : 16;
     while (W * 2 <= Wmax && nx % (W * 2) == 0 && 3 * (W * 2) * TPL <= cap &&
-           (size_t)6 * (W * 2) * row_stride(nz) * esz <= smem_cap)
+           (size_t)6 * (W * 2) * tile_stride(nz, W * 2) * esz <= smem_cap)
       W *= 2;
     int G = 1;
     while (ny % (G * 2) == 0 && 3 * W * (G * 2) * TPL <= 384 &&
-           (size_t)6 * W * (G * 2) * row_stride(nz) * esz <= smem_cap)
+           (size_t)6 * W * (G * 2) * tile_stride(nz, W) * esz <= smem_cap)
       G *= 2;
     pl.k1W = W;
     pl.k1G = G;
     const char* e = getenv("SNS_K1_SPLIT");
     pl.k1_fused = !(e && e[0] == '1') && 3 * W * G * TPL <= cap &&
-                  (size_t)6 * W * G * row_stride(nz) * esz <= smem_cap;
+                  (size_t)6 * W * G * tile_stride(nz, W) * esz <= smem_cap;
   }
   // K5 tile: W adjacent z lines of three fields
   {
@@ -463,7 +470,7 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
       if (v >= 1 && (v & (v - 1)) == 0) Wmax = v;
     }
     while (W * 2 <= Wmax && nx % (W * 2) == 0 && 3 * (W * 2) * TPL <= max_threads(prec) &&
-           (size_t)3 * W * 2 * row_stride(nz) * esz <= 110 * 1024)
+           (size_t)3 * W * 2 * tile_stride(nz, W * 2) * esz <= 110 * 1024)
       W *= 2;
     pl.zW = W;
     pl.update_blocks = (nx / W) * ny;
@@ -471,7 +478,7 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
     const int cap = std::min(576, max_threads(prec));
     int Ws = 1;
     while (Ws * 2 <= Wmax && ((int64_t)nx * ny) % (Ws * 2) == 0 && 9 * (Ws * 2) * TPL <= cap &&
-           (size_t)9 * Ws * 2 * row_stride(nz) * esz <= 110 * 1024)
+           (size_t)9 * Ws * 2 * tile_stride(nz, Ws * 2) * esz <= 110 * 1024)
       Ws *= 2;
     pl.sgs_W = Ws;
     pl.sgs_blocks = (int)(((int64_t)nx * ny) / Ws);

@@ -87,8 +87,7 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
   const int s = threadIdx.x >> wshift;
   const int j = s & (TPL - 1);
   const int g = s / TPL;
-  // single lines (x) share warps line by line; runs of W > 1 read columns
-  const int RS = W == 1 ? xrow_stride(L) : row_stride(L);
+  const int RS = tile_stride(L, W);
   C* row = sm + (w + W * g) * RS;
   const LineCoord lc = line_coord(geo, base, w, g, j, TPL);
 
@@ -150,8 +149,9 @@ __device__ __forceinline__ void curl_zpass_tile(const LineGeo& geo, const Fields
                                                 int64_t blk, cx_t<T>* sm) {
   using C = cx_t<T>;
   using P = LinePlan<L>;
-  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(L);
+  constexpr int E = P::E, TPL = P::TPL;
   const int W = geo.W, G = geo.G, lines = W * G;
+  const int RS = tile_stride(L, W);
   const int64_t base = (blk % geo.TA) * geo.sa + (blk / geo.TA) * geo.sb;
   const int w = threadIdx.x & (W - 1);
   const int s = threadIdx.x >> wshift;
@@ -324,9 +324,10 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
                                                  int nthr, cx_t<T>* sm, double (*red)[32]) {
   using C = cx_t<T>;
   using P = LinePlan<L>;
-  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(L);
+  constexpr int E = P::E, TPL = P::TPL;
 
   const int W = a.W;
+  const int RS = tile_stride(L, W);
   const int64_t nxy = (int64_t)a.nx * a.ny;
   const int64_t base = blk * W;
   const int per = W * L;

@@ -102,8 +102,9 @@ __device__ __forceinline__ void item_ylines(const XYArgs& a, cx_t<T>* sm, int f0
                                             const cx_t<T>* tw, T sg) {
   using C = cx_t<T>;
   using P = LinePlan<LY>;
-  constexpr int E = P::E, TPL = P::TPL, RS = row_stride(LY);
+  constexpr int E = P::E, TPL = P::TPL;
   const int W = a.W;
+  const int RS = tile_stride(LY, W);
   const int t = threadIdx.x;
   const int fi = t / (W * TPL), rest = t - fi * (W * TPL);
   const int w = rest % W, j = rest / W;
@@ -310,7 +311,7 @@ int xy_plan(XYPlan& p, int nx, int ny, int nz, int prec) {
   p.W = W;
   p.G = G;
   p.threads = 3 * W * tply;
-  p.smem_bytes = (size_t)(3 * W) * row_stride(ny) * esz;
+  p.smem_bytes = (size_t)(3 * W) * tile_stride(ny, W) * esz;
   if ((size_t)(6 * G) * xrow_stride(nx) * esz > p.smem_bytes)
     p.smem_bytes = (size_t)(6 * G) * xrow_stride(nx) * esz;
   p.nA = 2 * (nx / W);
