@@ -774,15 +774,25 @@ def closure_bench(S, torch, dev, args, world, rank, hbm, peak_src, clocks):
     samples = X.shape[0]
     del X, nut, w
     torch.cuda.empty_cache()
-    # output scale fitted a posteriori on the first training seed (not held out)
-    calib_errs = CL.calibrate(S, model, calib, NU, DT, c["steps"], c["kc"])
+    # output scale and band of the eddy force fitted a posteriori on the first
+    # training seed (not held out), at the coarse time step; the same fit for
+    # the Smagorinsky constant and band
+    cdt = DT * c["coarse_dt_factor"]
+    csteps = c["steps"] // c["coarse_dt_factor"]
+    t0 = time.perf_counter()
+    calib_errs, band = CL.calibrate(S, model, calib, NU, cdt, csteps, c["kc"])
+    smag_errs, (smag_band, cs) = CL.calibrate_smagorinsky(S, calib, NU, cdt, csteps, c["kc"])
+    t_cal = time.perf_counter() - t0
+    # the textbook Smagorinsky (Cs = 0.17 on every mode) as a further baseline
+    extra = {"smagorinsky_cs017_all_modes":
+             {"csd2": CL.smagorinsky_cs_delta2(c["cs"], c["kc"]), "band": (0.0, 0.0)}}
     res = CL.evaluate(S, model, c["nf"], c["nc"], c["kc"], c["eval_seeds"], NU, DT, c["steps"],
-                      cs=c["cs"], device=dev)
+                      cs=cs, device=dev, band=band, smag_band=smag_band, extra=extra)
     # the same runs with the coarse grid at a larger time step (the cutoff kc
     # relaxes the CFL limit), judged at the same physical time
-    cdt = DT * c["coarse_dt_factor"]
     res_dt = CL.evaluate(S, model, c["nf"], c["nc"], c["kc"], c["eval_seeds"], NU, DT, c["steps"],
-                         cs=c["cs"], device=dev, coarse_dt=cdt)
+                         cs=cs, device=dev, coarse_dt=cdt, band=band, smag_band=smag_band,
+                         extra=extra)
     # device-timed steps/s of the coarse MLP run and of the plain coarse run
     nc = c["nc"]
     Vc0 = CL.truncate([x.to(torch.complex64) for x in ic.solenoidal_spectrum_hat(
@@ -792,6 +802,7 @@ def closure_bench(S, torch, dev, args, world, rank, hbm, peak_src, clocks):
         st = S.NSStepper((nc, nc, nc), NU, DT, torch.complex64, device=dev)
         if name == "mlp":
             st.set_closure(S._native.SNS_CLOSURE_MLP, mlp=model.packed, kc=c["kc"])
+            st.set_sgs_band(*band)
         else:
             st.set_closure(S._native.SNS_CLOSURE_NONE, kc=c["kc"])
         st.bootstrap(Vc0, S.curl(Vc0))
@@ -832,8 +843,17 @@ def closure_bench(S, torch, dev, args, world, rank, hbm, peak_src, clocks):
         "value": world * timing["mlp"], "unit": "steps/s", "ms_per_step": 1000.0 / timing["mlp"],
         "dtype": "fp32 fields + bf16/fp32 MLP", "snapshots": snaps,
         "spectrum_error": {"plain": res["plain"], "smagorinsky": res["smagorinsky"],
-                           "mlp": res["mlp"], "shells": f"1..{c['kc'] - 1}", "target": 0.05,
+                           "mlp": res["mlp"],
+                           "smagorinsky_cs017_all_modes": res["smagorinsky_cs017_all_modes"],
+                           "shells": f"1..{c['kc'] - 1}", "target": 0.05,
+                           "held_out_seeds": c["eval_seeds"],
                            "spectra_first_seed": res["spectra_first_seed"]},
+        "closure_fit": {"on": f"training seed {c['train_seeds'][0]}, coarse dt {cdt}",
+                        "seconds": t_cal,
+                        "mlp_band": band, "mlp_output_scale": model.s_out / s_out,
+                        "smagorinsky_band": smag_band, "smagorinsky_cs": cs,
+                        "mlp_errors": {f"{k[0]}x{k[1]}": v for k, v in calib_errs.items()},
+                        "smagorinsky_errors": {f"{k[0]}x{k[1]}": v for k, v in smag_errs.items()}},
         "throughput": {"mlp_coarse_steps_per_s": timing["mlp"],
                        "plain_coarse_steps_per_s": timing["plain"],
                        "dns_steps_per_s": res["dns_steps_per_s"],
@@ -843,13 +863,14 @@ def closure_bench(S, torch, dev, args, world, rank, hbm, peak_src, clocks):
                        (res["dns_steps_per_s"] * DT)},
         "spectrum_error_at_coarse_dt": {"coarse_dt": cdt, "plain": res_dt["plain"],
                                         "smagorinsky": res_dt["smagorinsky"],
-                                        "mlp": res_dt["mlp"], "all_finite": res_dt["all_finite"]},
+                                        "mlp": res_dt["mlp"],
+                                        "smagorinsky_cs017_all_modes":
+                                        res_dt["smagorinsky_cs017_all_modes"],
+                                        "all_finite": res_dt["all_finite"]},
         "training": {"samples": samples, "steps": c["train_steps"], "batch": c["batch"],
                      "seconds": t_train, "dataset_seconds": t_data,
                      "loss_first": losses[0][1], "loss_last": losses[-1][1],
-                     "s_in": s_in, "s_out": s_out,
-                     "output_scale_calibration": {str(k): v for k, v in calib_errs.items()},
-                     "output_scale": model.s_out / s_out},
+                     "s_in": s_in, "s_out": s_out},
         "roofline": {"bound": "tensor", "kernel": "MLP inference (k_mlp_infer, 64^3 points)",
                      "achieved": achieved, "unit": "TFLOP/s", "peak": tpeak,
                      "frac": achieved / tpeak, "traffic": None,

@@ -211,6 +211,14 @@ int sns_ns_pass_times(sns_ns* handle, double* total_ms, int* launches, int max);
 #define SNS_CLOSURE_SMAGORINSKY 1
 #define SNS_CLOSURE_MLP 2
 int sns_ns_set_closure(sns_ns* handle, int model, double cs_delta2, const void* mlp, double kc);
+/* Spectral weight of the closure's eddy-stress divergence: mode k receives it
+ * times clamp((|k| - k_lo) / (k_hi - k_lo), 0, 1), a ramp from k_lo to k_hi
+ * (k_hi <= k_lo: a sharp split, every |k| > k_lo at full weight; the default
+ * k_lo = k_hi = 0 applies it to every mode).  The damping then acts on the
+ * small resolved scales, as in a variational multiscale split, while nu_t
+ * (MLP or Smagorinsky) still comes from the full resolved gradient.  No
+ * reference counterpart. */
+int sns_ns_set_sgs_band(sns_ns* handle, double k_lo, double k_hi);
 
 /* ---- learned closure: MLP 9 -> 64 -> 64 -> 1 on the tensor cores ----------
  * No reference counterpart.  FP32 master parameters (nparams floats: W1[64][16]

@@ -14,8 +14,11 @@ LES step (ns.cpp:167-217 with an eddy-viscosity term):
   u = inverse(V1), A_ij = inverse(i k_j V1_i)          (A_ij = d_j u_i)
   omega = (A_zy - A_yz, A_xz - A_zx, A_yx - A_xy)
   nu_t = model(Re A) >= 0,  S_ij = (A_ij + A_ji) / 2,  tau_ij = 2 nu_t S_ij
-  cross1_i = zeroNyquist(fftn(u x omega)_i + sum_j i k_j fftn(tau_ij))
+  cross1_i = zeroNyquist(fftn(u x omega)_i + b(|k|) sum_j i k_j fftn(tau_ij))
   then the AB2 / projection / Crank-Nicolson update of ns.cpp:170-187.
+The band weight b(|k|) = clip((|k| - k_lo) / (k_hi - k_lo), 0, 1) (k_hi <= k_lo:
+1 for |k| > k_lo, else 0) confines the eddy force to the small resolved
+scales; the default band (0, 0) is 1 on every mode but k = 0.
 The bootstrap is the plain one of ns.cpp:132-153.
 
 Models: 'plain' (nu_t = 0), 'smagorinsky' (nu_t = (Cs Delta)^2 sqrt(2 S:S)),
@@ -178,7 +181,17 @@ def model_nut(model, Ar, params=None):
 
 
 # --------------------------------------------------------------------- LES step
-def nonlinear(V, model="plain", params=None):
+def band_weight(shape, band):
+    """b(|k|) of the module docstring on the grid of `shape`."""
+    KX, KY, KZ = kgrid(shape)
+    km = np.sqrt(KX ** 2 + KY ** 2 + KZ ** 2)
+    lo, hi = band
+    if hi > lo:
+        return np.clip((km - lo) / (hi - lo), 0.0, 1.0)
+    return (km > lo).astype(np.float64)
+
+
+def nonlinear(V, model="plain", params=None, band=(0.0, 0.0)):
     """cross1 of the LES step (module docstring)."""
     K = kgrid(V[0].shape)
     u = [inverse(v) for v in V]
@@ -188,10 +201,11 @@ def nonlinear(V, model="plain", params=None):
     out = [np.fft.fftn(x) for x in c]
     if model != "plain":
         nut = model_nut(model, [[a.real for a in row] for row in A], params)
+        b = band_weight(V[0].shape, band)
         for i in range(3):
             for j in range(3):
                 tau = 2.0 * nut * 0.5 * (A[i][j] + A[j][i])
-                out[i] = out[i] + 1j * K[j] * np.fft.fftn(tau)
+                out[i] = out[i] + b * (1j * K[j] * np.fft.fftn(tau))
     return [zero_nyquist(x) for x in out]
 
 
@@ -225,8 +239,9 @@ def update(V1, c0, c1, nu, dt, kc=None):
 class LES:
     """FP64 LES stepper: state (V1, cross0) as in exec/ns.cpp."""
 
-    def __init__(self, nu, dt, model="plain", params=None, kc=None):
+    def __init__(self, nu, dt, model="plain", params=None, kc=None, band=(0.0, 0.0)):
         self.nu, self.dt, self.model, self.params, self.kc = nu, dt, model, params, kc
+        self.band = band
         self.V1 = self.c0 = None
 
     def set_state(self, V1, cross0):
@@ -235,7 +250,7 @@ class LES:
 
     def step(self, n=1):
         for _ in range(n):
-            c1 = nonlinear(self.V1, self.model, self.params)
+            c1 = nonlinear(self.V1, self.model, self.params, self.band)
             if self.kc is None:
                 self.V1 = update(self.V1, self.c0, c1, self.nu, self.dt)
             else:

@@ -78,6 +78,7 @@ SIGNATURES = {
     "sns_ns_profile": ([_vp, _int], _int),
     "sns_ns_pass_times": ([_vp, C.POINTER(_dbl), C.POINTER(_int), _int], _int),
     "sns_ns_set_closure": ([_vp, _int, _dbl, _vp, _dbl], _int),
+    "sns_ns_set_sgs_band": ([_vp, _dbl, _dbl], _int),
     "sns_mlp_sizes": ([C.POINTER(_i64), C.POINTER(_i64)], _int),
     "sns_mlp_pack": ([_vp, _dbl, _dbl, _vp, _vp], _int),
     "sns_mlp_infer": ([_vp, _vp, _i64, _vp, _vp], _int),

@@ -173,21 +173,48 @@ def spectrum_error(E, Eref, kmax):
     return float(np.mean(np.abs(E[k] - Eref[k]) / Eref[k]))
 
 
-def calibrate(S, model, calib, nu, dt, steps, kc, scales=(0.5, 1.0, 1.5, 2.0, 3.0, 4.0),
-              dtype=torch.complex64):
-    """Scale the model's output by the factor of `scales` whose coarse run from
-    a training seed's filtered field (calib from dns_dataset) ends with the
-    smallest spectrum error against that seed's filtered DNS.  Returns
-    {scale: error} and leaves the best scale applied."""
+# bands (k_lo, k_hi) of the eddy force tried by the calibrations, in units of
+# the cutoff kc: none, ramps from 2/3 kc to just below and to the cutoff, a
+# sharp split at 3/4 kc
+BANDS = ((0.0, 0.0), (2 / 3, 20 / 21), (2 / 3, 1.0), (4 / 7, 1.0), (16 / 21, 20 / 21),
+         (16 / 21, 0.0))
+
+
+def _bands(kc, bands):
+    return [(round(lo * kc, 6), round(hi * kc, 6)) for lo, hi in bands]
+
+
+def calibrate(S, model, calib, nu, dt, steps, kc, scales=(1.0, 1.5, 2.0, 3.0, 4.0, 5.0, 6.0, 8.0),
+              bands=BANDS, dtype=torch.complex64):
+    """Choose the model's output scale (a factor of `scales`) and the band of
+    the eddy force (`bands`, fractions of kc) whose coarse run from a training
+    seed's filtered field (calib from dns_dataset) ends with the smallest
+    spectrum error against that seed's filtered DNS.  `steps` steps of `dt`.
+    Leaves the best scale applied; returns ({(band, scale): error}, band)."""
     s_out0 = model.s_out
     errs = {}
-    for c in scales:
-        model.set_scales(model.s_in, s_out0 * c)
-        V = coarse_run(S, calib["Vc0"], nu, dt, steps, model=model, kc=kc, dtype=dtype)
-        errs[c] = spectrum_error(spectrum(V), calib["Eref"], int(kc))
-    best = min(errs, key=errs.get)
+    for band in _bands(kc, bands):
+        for c in scales:
+            model.set_scales(model.s_in, s_out0 * c)
+            V = coarse_run(S, calib["Vc0"], nu, dt, steps, model=model, kc=kc, dtype=dtype,
+                           band=band)
+            errs[(band, c)] = spectrum_error(spectrum(V), calib["Eref"], int(kc))
+    band, best = min(errs, key=errs.get)
     model.set_scales(model.s_in, s_out0 * best)
-    return errs
+    return errs, band
+
+
+def calibrate_smagorinsky(S, calib, nu, dt, steps, kc, cs=(0.08, 0.1, 0.13, 0.17, 0.2, 0.25),
+                          bands=BANDS, dtype=torch.complex64):
+    """The same choice for the Smagorinsky constant Cs and the band; returns
+    ({(band, cs): error}, (band, cs))."""
+    errs = {}
+    for band in _bands(kc, bands):
+        for c in cs:
+            V = coarse_run(S, calib["Vc0"], nu, dt, steps, csd2=smagorinsky_cs_delta2(c, kc),
+                           kc=kc, dtype=dtype, band=band)
+            errs[(band, c)] = spectrum_error(spectrum(V), calib["Eref"], int(kc))
+    return errs, min(errs, key=errs.get)
 
 
 def smagorinsky_cs_delta2(cs: float, kc: float) -> float:
@@ -259,10 +286,12 @@ def train(model, X, nut, steps, batch, lr, weight=None, seed=0, log=None):
     return losses
 
 
-def coarse_run(S, Vc0, nu, dt, steps, model=None, csd2=0.0, kc=0.0, dtype=torch.complex64):
+def coarse_run(S, Vc0, nu, dt, steps, model=None, csd2=0.0, kc=0.0, dtype=torch.complex64,
+               band=(0.0, 0.0)):
     """Coarse run from the filtered field Vc0 over the modes |k| <= kc (all
     modes when kc = 0) with no closure, Smagorinsky (csd2 > 0, model None) or
-    the MLP (model).  Returns the final velocity."""
+    the MLP (model), the eddy force weighted by `band` (NSStepper.set_sgs_band).
+    Returns the final velocity."""
     n = Vc0[0].shape[0]
     st = S.NSStepper((n, n, n), nu, dt, dtype, device=Vc0[0].device)
     if model is not None:
@@ -271,6 +300,7 @@ def coarse_run(S, Vc0, nu, dt, steps, model=None, csd2=0.0, kc=0.0, dtype=torch.
         st.set_closure(N.SNS_CLOSURE_SMAGORINSKY, cs_delta2=csd2, kc=kc)
     else:
         st.set_closure(N.SNS_CLOSURE_NONE, kc=kc)
+    st.set_sgs_band(*band)
     st.bootstrap(Vc0, S.curl(Vc0))
     st.step(steps)
     V = st.velocity()
@@ -279,16 +309,19 @@ def coarse_run(S, Vc0, nu, dt, steps, model=None, csd2=0.0, kc=0.0, dtype=torch.
 
 
 def evaluate(S, model, nf, nc, kc, seeds, nu, dt, steps, cs=0.17, dtype=torch.complex64,
-             device="cuda", coarse_dt=None):
+             device="cuda", coarse_dt=None, band=(0.0, 0.0), smag_band=(0.0, 0.0), extra=None):
     """Spectrum errors (shells 1..kc-1) at the end of `steps` steps against the
-    filtered fine DNS, for the plain, Smagorinsky and MLP coarse runs, plus
-    the steps/s of the coarse MLP run and of the fine DNS.  The coarse runs
-    take time step coarse_dt (default dt) and end at the same time."""
+    filtered fine DNS, for the plain, Smagorinsky (cs, smag_band) and MLP
+    (band) coarse runs and any `extra` runs ({name: coarse_run keywords}),
+    plus the steps/s of the coarse MLP run and of the fine DNS.  The coarse
+    runs take time step coarse_dt (default dt) and end at the same time."""
     coarse_dt = dt if coarse_dt is None else coarse_dt
     coarse_steps = int(round(steps * dt / coarse_dt))
-    res = {"plain": [], "smagorinsky": [], "mlp": []}
+    runs = {"plain": {}, "smagorinsky": {"csd2": smagorinsky_cs_delta2(cs, kc), "band": smag_band},
+            "mlp": {"model": model, "band": band}}
+    runs.update(extra or {})
+    res = {name: [] for name in runs}
     spectra = {}
-    csd2 = smagorinsky_cs_delta2(cs, kc)
     t_dns = t_les = 0.0
     for seed in seeds:
         V0 = _initial(nf, seed, dtype, device)
@@ -302,7 +335,7 @@ def evaluate(S, model, nf, nc, kc, seeds, nu, dt, steps, cs=0.17, dtype=torch.co
         t_dns += time.perf_counter() - t0
         Eref = spectrum(truncate(st.velocity(), nc, kc))
         st.close()
-        for name, kw in (("plain", {}), ("smagorinsky", {"csd2": csd2}), ("mlp", {"model": model})):
+        for name, kw in runs.items():
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             V = coarse_run(S, Vc0, nu, coarse_dt, coarse_steps, kc=kc, dtype=dtype, **kw)

@@ -943,4 +943,17 @@ int sns_ns_set_closure(sns_ns* h, int model, double cs_delta2, const void* mlp, 
   return OK;
 }
 
+int sns_ns_set_sgs_band(sns_ns* h, double k_lo, double k_hi) {
+  if (!nonnull(h, "sns_ns_set_sgs_band")) return ERR_ARG;
+  if (!(k_lo >= 0) || !(k_hi >= 0)) {
+    set_error("sns_ns_set_sgs_band: k_lo and k_hi must be >= 0");
+    return ERR_ARG;
+  }
+  h->pl.sgs_klo = k_lo;
+  h->pl.sgs_kinv = k_hi > k_lo ? 1.0 / (k_hi - k_lo) : 1e30;
+  drop_graph(h);
+  h->eager_done = false;
+  return OK;
+}
+
 }  // extern "C"

@@ -273,6 +273,8 @@ int les_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* c
   a.nuhK = nu * dt / 2;
   a.stats = stats;
   a.kc2 = pl.kc2;
+  a.sgs_klo = pl.sgs_klo;
+  a.sgs_kinv = pl.sgs_kinv;
   return ns_update(pl, a, true, s);
 }
 

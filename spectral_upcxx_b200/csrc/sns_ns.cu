@@ -497,6 +497,8 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
   pl.passes = (pl.use_xy || (pl.xy_chunk > 0 && pl.xy_chunk < nz)) ? 3 : 5;
   pl.lineW = lineW > 0 ? lineW : 0;
   pl.kc2 = 1e300;
+  pl.sgs_klo = 0;
+  pl.sgs_kinv = 1e30;
   return OK;
 }
 

@@ -24,6 +24,7 @@ struct NSPlan {
   bool real;          // half-spectrum fields of a real velocity (R2C / C2R along x)
   int nx_phys;        // physical nx (= nx, or 2 nx for a real-field run)
   double kc2;         // spectral cutoff |k|^2 <= kc2 of the evolved modes (1e300: none)
+  double sgs_klo, sgs_kinv;  // closure: stress divergence weight clamp((|k|-klo) kinv, 0, 1)
 };
 
 // zW > 0 and lineW > 0 select tuned tile widths (0 = defaults).

@@ -301,6 +301,8 @@ struct UpdateArgs {
   const void* tau[6];
   double kc2;  // spectral cutoff |k|^2 <= kc2 of an LES run (1e300: none)
   int kx_half;  // half-spectrum fields (see LineGeo::kx_half)
+  // SGS: the stress divergence is weighted by clamp((|k| - sgs_klo) sgs_kinv, 0, 1)
+  double sgs_klo, sgs_kinv;
 };
 
 // Field f of the update's z-forward: the cross product (f < 3) or, with the
@@ -375,14 +377,18 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
 #pragma unroll
     for (int d = 0; d < 3; d++) c1[d] = nyq ? mk((T)0, (T)0) : sm[(d * W + w) * RS + pad_pos(z)];
     if constexpr (SGS) {
-      if (!nyq) {
+      const T ws = (T)fmin(1.0, fmax(0.0, (sqrt(k2d) - a.sgs_klo) * a.sgs_kinv));
+      if (!nyq && ws > (T)0) {
         C t6[6];
 #pragma unroll
         for (int q = 0; q < 6; q++) t6[q] = sm[((3 + q) * W + w) * RS + pad_pos(z)];
         // (div tau)_i = i (kx tau_ix + ky tau_iy + kz tau_iz)
-        c1[0] = cadd(c1[0], cadd(cadd(ikmul(kx, t6[0]), ikmul(ky, t6[3])), ikmul(kz, t6[4])));
-        c1[1] = cadd(c1[1], cadd(cadd(ikmul(kx, t6[3]), ikmul(ky, t6[1])), ikmul(kz, t6[5])));
-        c1[2] = cadd(c1[2], cadd(cadd(ikmul(kx, t6[4]), ikmul(ky, t6[5])), ikmul(kz, t6[2])));
+        const C f0 = cadd(cadd(ikmul(kx, t6[0]), ikmul(ky, t6[3])), ikmul(kz, t6[4]));
+        const C f1 = cadd(cadd(ikmul(kx, t6[3]), ikmul(ky, t6[1])), ikmul(kz, t6[5]));
+        const C f2 = cadd(cadd(ikmul(kx, t6[4]), ikmul(ky, t6[5])), ikmul(kz, t6[2]));
+        c1[0] = cadd(c1[0], cscale(ws, f0));
+        c1[1] = cadd(c1[1], cscale(ws, f1));
+        c1[2] = cadd(c1[2], cscale(ws, f2));
       }
     }
     const T kk[3] = {kx, ky, kz};

@@ -76,6 +76,12 @@ class NSStepper:
         N.call("sns_ns_set_closure", self.h, int(model), float(cs_delta2),
                C.c_void_p(mlp.data_ptr()) if mlp is not None else None, float(kc))
 
+    def set_sgs_band(self, k_lo: float = 0.0, k_hi: float = 0.0):
+        """Weight the closure's eddy-stress divergence by the ramp
+        clamp((|k| - k_lo) / (k_hi - k_lo), 0, 1); k_hi <= k_lo: the modes
+        |k| > k_lo at full weight (default: every mode)."""
+        N.call("sns_ns_set_sgs_band", self.h, float(k_lo), float(k_hi))
+
     def velocity(self, out=None):
         """The Fourier velocity V1 (into `out`, three device fields, if given)."""
         if out is None:

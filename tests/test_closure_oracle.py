@@ -109,3 +109,31 @@ def test_sgs_target_of_a_resolved_field_vanishes(C):
     X, nut, w, Vc = C.sgs_sample(V, nc, kc, s_in=1.0)
     assert X.shape == (nc ** 3, C.KPAD)
     assert np.max(np.abs(nut)) < 1e-10
+
+
+def test_band_weight_and_band_restricted_force(C):
+    """The default band weighs every mode but k = 0 by 1; a ramp and a sharp
+    split leave the eddy force only on the small scales."""
+    n = 16
+    KX, KY, KZ = C.kgrid((n, n, n))
+    km = np.sqrt(KX ** 2 + KY ** 2 + KZ ** 2)
+    b0 = C.band_weight((n, n, n), (0, 0))
+    assert b0[0, 0, 0] == 0 and np.all(b0[km > 0] == 1)
+    br = C.band_weight((n, n, n), (2, 6))
+    assert np.all(br[km <= 2] == 0) and np.all(br[km >= 6] == 1)
+    mid = (km > 2) & (km < 6)
+    assert np.allclose(br[mid], (km[mid] - 2) / 4)
+    bs = C.band_weight((n, n, n), (3, 0))
+    assert np.array_equal(bs, (km > 3).astype(float))
+    # the Smagorinsky force of a smooth field with a sharp split at 3: below
+    # the split the LES nonlinear term is the plain one
+    V = _field(n, 4)
+    p = {"cs": 0.2, "delta": np.pi / 5}
+    plain = C.nonlinear(V, "plain")
+    full = C.nonlinear(V, "smagorinsky", p)
+    split = C.nonlinear(V, "smagorinsky", p, band=(3, 0))
+    low = km <= 3
+    for d in range(3):
+        assert np.allclose(split[d][low], plain[d][low], rtol=0, atol=1e-9)
+        assert np.allclose(split[d][~low], full[d][~low], rtol=0, atol=1e-9)
+        assert not np.allclose(full[d][low], plain[d][low], rtol=0, atol=1e-9)

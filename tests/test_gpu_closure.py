@@ -161,16 +161,19 @@ def _les_pair(CO, S, cuda, n, nu, dt, seed):
     return st, [host(x) for x in s0["V1"]], [host(x) for x in s0["cross0"]]
 
 
-@pytest.mark.parametrize("kc", [0.0, 10.0])
-def test_smagorinsky_step_matches_oracle(CO, CL, sns, cuda, kc):
-    """complex128 closure step (with and without the spectral cutoff)."""
+@pytest.mark.parametrize("kc,band", [(0.0, (0, 0)), (10.0, (0, 0)), (10.0, (4, 8.5)),
+                                     (0.0, (6, 0))])
+def test_smagorinsky_step_matches_oracle(CO, CL, sns, cuda, kc, band):
+    """complex128 closure step (with and without the spectral cutoff, and with
+    the eddy force on a ramp or a sharp band of small scales)."""
     n, nu, dt = 32, 1 / 400, 1e-3
     csd2 = CL.smagorinsky_cs_delta2(0.17, 10.0)
     st, V1, c0 = _les_pair(CO, sns, cuda, n, nu, dt, 10)
     st.set_closure(sns._native.SNS_CLOSURE_SMAGORINSKY, cs_delta2=csd2, kc=kc)
+    st.set_sgs_band(*band)
     assert st.launches_per_step() == 5
     les = CO.LES(nu, dt, "smagorinsky", {"cs": 0.17, "delta": np.pi / 10.0},
-                 kc=kc if kc > 0 else None)
+                 kc=kc if kc > 0 else None, band=band)
     les.set_state(V1, c0)
     st.step(3)
     les.step(3)
@@ -239,12 +242,22 @@ def test_trained_mlp_beats_the_unclosed_coarse_run(CL, sns, cuda):
     held-out seed judged by their energy spectrum against the filtered DNS
     (shells 1..9)."""
     nf, nc, kc, nu, dt = 128, 32, 10, 1 / 400, 1e-3
+    calib = {}
     X, nut, w, s_in, snaps = CL.dns_dataset(sns, nf, nc, kc, seeds=[1, 2], nu=nu, dt=dt,
-                                            steps=400, every=10, device=cuda)
+                                            steps=400, every=10, device=cuda, calib=calib)
     assert snaps == 80 and X.shape[0] == 80 * nc ** 3
     s_out = float((nut * w).mean() / w.mean())
     model = CL.MLPModel.init(0, s_in=s_in, s_out=s_out, device=cuda)
     losses = CL.train(model, X, nut, steps=600, batch=16384, lr=2e-3, weight=w)
     assert losses[-1][1] < losses[0][1]
     res = CL.evaluate(sns, model, nf, nc, kc, seeds=[7], nu=nu, dt=dt, steps=400, device=cuda)
+    assert res["mlp"] < res["plain"], res
+    # the band and output scale fitted on the training seed (6 runs), then the
+    # held-out seed: still ahead of the unclosed run
+    errs, band = CL.calibrate(sns, model, calib, nu, dt, 400, kc, scales=(1.0, 2.0, 4.0),
+                              bands=((0.0, 0.0), (2 / 3, 1.0)))
+    assert len(errs) == 6 and band in ((0.0, 0.0), (round(2 / 3 * kc, 6), float(kc)))
+    assert abs(model.s_out / s_out - min(errs, key=errs.get)[1]) < 1e-12
+    res = CL.evaluate(sns, model, nf, nc, kc, seeds=[7], nu=nu, dt=dt, steps=400, device=cuda,
+                      band=band)
     assert res["mlp"] < res["plain"], res
