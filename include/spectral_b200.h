@@ -228,8 +228,14 @@ int sns_ns_set_sgs_band(sns_ns* handle, double k_lo, double k_hi);
  * nu_t = s_out * softplus(z), ReLU hidden layers, FP32 accumulation. */
 int sns_mlp_sizes(int64_t* nparams, int64_t* packed_bytes);
 int sns_mlp_pack(const float* master, double s_in, double s_out, void* packed, void* stream);
-/* nut[M] = the model at the M rows of X (device pointers). */
+/* nut[M] = the model at the M rows of X (device pointers, 16-byte aligned),
+ * on the tcgen05 tensor cores (128 points per tile, accumulators in tensor
+ * memory). */
 int sns_mlp_infer(const void* packed, const void* X, int64_t M, float* nut, void* stream);
+/* Synchronises the device; SNS_ERR_TIMEOUT (and clears the record) if a
+ * tensor-core MLP kernel stopped waiting for its MMAs since the last call,
+ * else SNS_OK.  No reference counterpart. */
+int sns_mlp_status(void);
 /* Gradient of the mean weighted squared error w (softplus(z) - target)^2
  * (target in model units, i.e. nu_t / s_out; weight NULL = 1) over B samples
  * (rows idx[0..B) of X, target and weight, or rows 0..B when idx is NULL).

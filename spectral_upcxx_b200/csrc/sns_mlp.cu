@@ -22,6 +22,7 @@
 #include "sns_common.cuh"
 #include "sns_ens.cuh"
 #include "sns_mlp.cuh"
+#include "sns_tc.cuh"
 
 namespace sns {
 
@@ -362,6 +363,187 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Inference on the fifth-generation tensor cores: a CTA of 128 threads takes
+// tiles of 128 points; thread m owns point m of the tile (its input row, its
+// accumulator lane in tensor memory and its output).  The biases ride in the
+// MMAs: input columns 9 and 10 (padding) are set to 1 in the A tile and the
+// matching columns of W1 hold b1 split into two BF16 terms (hi + lo = b1 to
+// 16 bits); layer 2 gets a fifth K-slice whose A rows are (1, 1, 0, ...) and
+// whose B rows are (b2 hi, b2 lo, 0, ...).  Per tile: layer 1 is one
+// tcgen05.mma (M 128, N 64, K 16) into 64 tensor-memory columns, the epilogue
+// reads them back (ReLU, BF16) into the layer-2 A tile, layer 2 is five MMAs
+// into the same columns, and the output epilogue forms
+// s_out softplus(relu(.) . w3 + b3) per lane.  Rounding points as in the
+// mma.sync path: hidden layer 1 rounded to BF16, layer 2 kept in FP32.
+constexpr int kTcRows = 128;
+constexpr int kTcCols = 64;  // tensor-memory columns: the accumulator of either layer
+
+struct __align__(128) TcSmem {
+  unsigned char W1[kMlpHidden * kMlpK1 * 2];       // B of layer 1 (b1 in columns 9, 10)
+  unsigned char W2[kMlpHidden * kMlpHidden * 2];   // B of layer 2, K-slices 0..3
+  unsigned char B2[kMlpHidden * 16 * 2];           // B of layer 2, bias slice
+  unsigned char X[kTcRows * kMlpK1 * 2];           // A of layer 1
+  unsigned char H[kTcRows * kMlpHidden * 2];       // A of layer 2, K-slices 0..3
+  unsigned char ONES[kTcRows * 16 * 2];            // A of layer 2, bias slice
+  float w3[kMlpHidden];
+  float b3, s_out;
+  uint64_t mbar;
+  uint32_t tmem;
+  int abort;
+};
+
+__device__ int g_mlp_tc_status;  // nonzero: a tensor-core wait ran out
+
+__device__ __forceinline__ uint32_t bf16_bits(float x) {
+  __nv_bfloat16 h = __float2bfloat16_rn(x);
+  return (uint32_t)*reinterpret_cast<unsigned short*>(&h);
+}
+
+__global__ void __launch_bounds__(kTcRows)
+    k_mlp_infer_tc(const MlpPacked* __restrict__ P, const __nv_bfloat16* __restrict__ X,
+                   int64_t M, float* __restrict__ nut) {
+  extern __shared__ __align__(128) unsigned char tc_raw[];
+  TcSmem& S = *reinterpret_cast<TcSmem*>(tc_raw);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  // weights into the K-major operand layouts, 16 bytes (8 bf16 along k) at a time
+  for (int i = tid; i < kMlpHidden * kMlpK1 / 8; i += kTcRows) {
+    const int n = i / (kMlpK1 / 8), c = i % (kMlpK1 / 8);
+    uint4 v = reinterpret_cast<const uint4*>(P->W1)[i];
+    if (c == 1) {
+      // W1 columns 9, 10 (zero in the model) carry b1 = hi + lo
+      const float b = P->b1[n];
+      const float hi = __bfloat162float(__float2bfloat16_rn(b));
+      v.x = (v.x & 0xFFFFu) | (bf16_bits(hi) << 16);
+      v.y = (v.y & 0xFFFF0000u) | bf16_bits(b - hi);
+    }
+    *reinterpret_cast<uint4*>(S.W1 + tc::kmajor_off(n, 8 * c, kMlpK1)) = v;
+  }
+  for (int i = tid; i < kMlpHidden * kMlpHidden / 8; i += kTcRows) {
+    const int n = i / (kMlpHidden / 8), c = i % (kMlpHidden / 8);
+    *reinterpret_cast<uint4*>(S.W2 + tc::kmajor_off(n, 8 * c, kMlpHidden)) =
+        reinterpret_cast<const uint4*>(P->W2)[i];
+  }
+  for (int n = tid; n < kMlpHidden; n += kTcRows) {
+    const float b = P->b2[n];
+    const float hi = __bfloat162float(__float2bfloat16_rn(b));
+    *reinterpret_cast<uint4*>(S.B2 + tc::kmajor_off(n, 0, 16)) =
+        make_uint4(bf16_bits(hi) | (bf16_bits(b - hi) << 16), 0u, 0u, 0u);
+    *reinterpret_cast<uint4*>(S.B2 + tc::kmajor_off(n, 8, 16)) = make_uint4(0u, 0u, 0u, 0u);
+    S.w3[n] = __bfloat162float(P->w3[n]);
+  }
+  {
+    const uint32_t one = bf16_bits(1.f);
+    *reinterpret_cast<uint4*>(S.ONES + tc::kmajor_off(tid, 0, 16)) =
+        make_uint4(one | (one << 16), 0u, 0u, 0u);
+    *reinterpret_cast<uint4*>(S.ONES + tc::kmajor_off(tid, 8, 16)) = make_uint4(0u, 0u, 0u, 0u);
+  }
+  if (tid == 0) {
+    S.b3 = P->b3;
+    S.s_out = P->s_out;
+    S.abort = 0;
+    tc::mbar_init(&S.mbar, 1);
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(&S.tmem, kTcCols);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = S.tmem;
+  const uint32_t lane_base = (uint32_t)(32 * warp) << 16;  // this warp's accumulator lanes
+  const uint32_t sX = tc::smem_u32(S.X), sH = tc::smem_u32(S.H), sO = tc::smem_u32(S.ONES);
+  const uint32_t sW1 = tc::smem_u32(S.W1), sW2 = tc::smem_u32(S.W2), sB2 = tc::smem_u32(S.B2);
+  constexpr uint32_t id = tc::idesc_bf16(kTcRows, kMlpHidden);
+  const uint32_t one2 = bf16_bits(1.f) * 0x10001u;
+  uint32_t phase = 0;
+  const int64_t tiles = (M + kTcRows - 1) / kTcRows;
+  for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int64_t row = tile * kTcRows + tid;
+    {
+      uint4 x0 = make_uint4(0, 0, 0, 0), x1 = x0;
+      if (row < M) {
+        const uint4* src = reinterpret_cast<const uint4*>(X + row * kMlpK1);
+        x0 = src[0];
+        x1 = src[1];
+      }
+      // columns 9, 10: the constant 1 of the b1 terms
+      x1.x = (x1.x & 0xFFFFu) | (one2 & 0xFFFF0000u);
+      x1.y = (x1.y & 0xFFFF0000u) | (one2 & 0xFFFFu);
+      *reinterpret_cast<uint4*>(S.X + tc::kmajor_off(tid, 0, kMlpK1)) = x0;
+      *reinterpret_cast<uint4*>(S.X + tc::kmajor_off(tid, 8, kMlpK1)) = x1;
+    }
+    tc::fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+      tc::mma_bf16(tmem, tc::sdesc(sX, 128, 16 * kMlpK1), tc::sdesc(sW1, 128, 16 * kMlpK1), id, 0);
+      tc::commit(&S.mbar);
+    }
+    if (!tc::mbar_wait(&S.mbar, phase, tc::kWaitCycles)) S.abort = 1;
+    phase ^= 1;
+    tc::fence_after_sync();
+    __syncthreads();
+    if (S.abort) break;
+    // layer-1 epilogue: h1 = bf16(relu(acc)) into the layer-2 A tile
+#pragma unroll
+    for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+      uint32_t r[16];
+      tc::tmem_ld16(tmem + lane_base + c0, r);
+      uint32_t h[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        h[j] = pack_bf16(fmaxf(__uint_as_float(r[2 * j]), 0.f),
+                         fmaxf(__uint_as_float(r[2 * j + 1]), 0.f));
+      *reinterpret_cast<uint4*>(S.H + tc::kmajor_off(tid, c0, kMlpHidden)) =
+          make_uint4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<uint4*>(S.H + tc::kmajor_off(tid, c0 + 8, kMlpHidden)) =
+          make_uint4(h[4], h[5], h[6], h[7]);
+    }
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int s = 0; s < kMlpHidden / 16; s++)
+        tc::mma_bf16(tmem, tc::sdesc(sH + 256 * s, 128, 16 * kMlpHidden),
+                     tc::sdesc(sW2 + 256 * s, 128, 16 * kMlpHidden), id, s > 0);
+      tc::mma_bf16(tmem, tc::sdesc(sO, 128, 256), tc::sdesc(sB2, 128, 256), id, 1);
+      tc::commit(&S.mbar);
+    }
+    if (!tc::mbar_wait(&S.mbar, phase, tc::kWaitCycles)) S.abort = 1;
+    phase ^= 1;
+    tc::fence_after_sync();
+    __syncthreads();
+    if (S.abort) break;
+    // output epilogue
+    float z = 0.f;
+#pragma unroll
+    for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+      uint32_t r[16];
+      tc::tmem_ld16(tmem + lane_base + c0, r);
+#pragma unroll
+      for (int j = 0; j < 16; j++) z += fmaxf(__uint_as_float(r[j]), 0.f) * S.w3[c0 + j];
+    }
+    if (row < M) nut[row] = S.s_out * softplus_f(z + S.b3);
+    tc::fence_before_sync();
+  }
+  __syncthreads();
+  if (S.abort) {
+    // the MMA whose wait ran out may still be in flight: one more bounded wait
+    tc::mbar_wait(&S.mbar, phase ^ 1, tc::kWaitCycles);
+    if (tid == 0) atomicExch(&g_mlp_tc_status, 1);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, kTcCols);
+  }
+}
+
 namespace {
 
 int grad_launch(const void* packed, const void* X, const float* t, const float* w,
@@ -433,12 +615,56 @@ int sns_mlp_infer(const void* packed, const void* X, int64_t M, float* nut, void
     return ERR_ARG;
   }
   if (M == 0) return OK;
-  const int64_t tiles = (M + 15) / 16;
-  const int blocks = (int)std::min<int64_t>((tiles + 7) / 8, 4 * 148 * 8);
-  k_mlp_infer<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+  if (reinterpret_cast<uintptr_t>(X) % 16 || reinterpret_cast<uintptr_t>(packed) % 16) {
+    set_error("sns_mlp_infer: X and the packed model must be 16-byte aligned");
+    return ERR_ARG;
+  }
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr[dev & 63]) {
+    int rc = cuda_status(cudaFuncSetAttribute(k_mlp_infer_tc,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)sizeof(TcSmem)),
+                         "cudaFuncSetAttribute(k_mlp_infer_tc)");
+    if (rc) return rc;
+    attr[dev & 63] = true;
+  }
+  // one persistent wave: the resident CTAs per SM (at most eight share an SM's
+  // 512 tensor-memory columns)
+  // (shared memory sets it: registers and threads allow more)
+  static int per_sm[64] = {0};
+  if (!per_sm[dev & 63]) {
+    int smem_sm = 0, resv = 0;
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    const int occ = smem_sm / (int)(sizeof(TcSmem) + resv);
+    per_sm[dev & 63] = std::max(1, std::min(occ, 512 / kTcCols));
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t tiles = (M + kTcRows - 1) / kTcRows;
+  const int blocks = (int)std::min<int64_t>(tiles, (int64_t)per_sm[dev & 63] * sms);
+  k_mlp_infer_tc<<<blocks, kTcRows, sizeof(TcSmem), reinterpret_cast<cudaStream_t>(stream)>>>(
       reinterpret_cast<const MlpPacked*>(packed), reinterpret_cast<const __nv_bfloat16*>(X), M,
       nut);
-  SNS_CHECK_LAUNCH("k_mlp_infer");
+  SNS_CHECK_LAUNCH("k_mlp_infer_tc");
+  return OK;
+}
+
+int sns_mlp_status(void) {
+  int v = 0;
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpyFromSymbol(&v, g_mlp_tc_status, sizeof(int));
+  if (e == cudaSuccess && v) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbol(g_mlp_tc_status, &zero, sizeof(int));
+  }
+  if (e != cudaSuccess) return cuda_status(e, "sns_mlp_status");
+  if (v) {
+    set_error("a tensor-core MLP kernel gave up waiting for its MMAs");
+    return ERR_TIMEOUT;
+  }
   return OK;
 }
 

@@ -70,6 +70,20 @@ def test_mlp_inference_matches_oracle(CO, CL, cuda):
     assert rel_l2(got, ref) < 2e-3
 
 
+def test_mlp_inference_tensor_memory_path_large(CO, CL, sns, cuda):
+    """sns_mlp_infer on the tcgen05 path at 300,001 points (a ragged last
+    tile, more tiles than CTAs) against the oracle; no MMA wait ran out."""
+    net = _random_net(CO, 7)
+    net.s_out = 0.25
+    model = _gpu_model(CL, net, cuda, s_out=0.25)
+    X = _features(CO, 300001, 8)
+    got = model.infer(dev(X, torch.bfloat16, cuda)).cpu().double().numpy()
+    ref = net.nut(X)
+    assert rel_l2(got, ref) < 2e-3
+    assert np.abs(got - ref).max() < 1e-2 * np.abs(ref).max()
+    assert sns._native.lib().sns_mlp_status() == 0
+
+
 def test_mlp_gradient_matches_oracle(CO, CL, cuda):
     net = _random_net(CO, 3)
     model = _gpu_model(CL, net, cuda)
