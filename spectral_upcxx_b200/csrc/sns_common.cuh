@@ -1,6 +1,8 @@
 // Shared device helpers: complex types, error plumbing, grid sizing.
 #pragma once
 
+#include <stdlib.h>
+
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -94,6 +96,53 @@ inline cudaError_t allow_max_dynamic_smem(K* kernel) {
 int sm_count();
 
 }  // namespace sns
+
+// Programmatic dependent launch.  A kernel started by launch_pdl inside a
+// PdlScope may begin while its predecessor in the stream is still draining:
+// it first lets its own dependents be scheduled (pdl_trigger: they start once
+// every CTA of this grid has started, so they never take an SM slot this grid
+// still needs), then waits for the predecessor grid to complete with its
+// memory visible (pdl_wait) before reading anything that grid wrote.  Both are
+// no-ops after an ordinary launch.  Measured on B200: the 64^3 closure step
+// gains 2.4 %, the 256^3 steps are unchanged and the 64^3 plain step loses
+// 16 %, so only the closure step opens a scope.  SNS_PDL=0 turns it off.
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+inline bool& pdl_scope_flag() {
+  static thread_local bool on = false;
+  return on;
+}
+struct PdlScope {
+  bool prev;
+  PdlScope() : prev(pdl_scope_flag()) { pdl_scope_flag() = true; }
+  ~PdlScope() { pdl_scope_flag() = prev; }
+};
+inline bool pdl_enabled() {
+  static const bool allowed = [] {
+    const char* e = getenv("SNS_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return allowed && pdl_scope_flag();
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
 
 #define SNS_CHECK_LAUNCH(where)                                    \
   do {                                                             \

@@ -92,6 +92,8 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
     k_line_pass(const LineGeo geo, const FieldPtrs f, const cx_t<T>* __restrict__ tw, T sg,
                 T scale, int flags, int wshift) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_trigger();
+  pdl_wait();
   line_pass_tile<T, L, PRO>(geo, ParamFields{f}, f.n, tw, sg, scale, flags, wshift,
                             (int64_t)blockIdx.x, reinterpret_cast<cx_t<T>*>(smem_raw));
 }
@@ -146,9 +148,9 @@ static int launch_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int fla
     set_error("line pass: grid too large");
     return ERR_UNSUPPORTED;
   }
-  k_line_pass<T, L, PRO><<<(unsigned)blocks, threads, smem, stream>>>(geo, f, tw, (T)sign, (T)scale,
-                                                                 flags, wshift);
-  SNS_CHECK_LAUNCH("k_line_pass");
+  cudaError_t e = launch_pdl(k_line_pass<T, L, PRO>, dim3((unsigned)blocks), dim3(threads), smem,
+                             stream, geo, f, tw, (T)sign, (T)scale, flags, wshift);
+  if (e != cudaSuccess) return cuda_status(e, "k_line_pass");
   return OK;
 }
 
@@ -200,7 +202,7 @@ int run_line_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags, d
       return dispatch_pass<double, PRO_GRAD12>(geo, f, sign, flags, scale, stream);
     return dispatch_pass<float, PRO_GRAD12>(geo, f, sign, flags, scale, stream);
   }
-  if (prologue != PRO_LOAD) {
+  if (prologue != PRO_LOAD && prologue != PRO_IKAXIS) {
     set_error("line pass: unknown prologue");
     return ERR_ARG;
   }
@@ -209,6 +211,11 @@ int run_line_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags, d
       set_error("line pass: null field pointer");
       return ERR_ARG;
     }
+  if (prologue == PRO_IKAXIS) {
+    if (prec == PREC_C128)
+      return dispatch_pass<double, PRO_IKAXIS>(geo, f, sign, flags, scale, stream);
+    return dispatch_pass<float, PRO_IKAXIS>(geo, f, sign, flags, scale, stream);
+  }
   if (prec == PREC_C128) return dispatch_pass<double, PRO_LOAD>(geo, f, sign, flags, scale, stream);
   return dispatch_pass<float, PRO_LOAD>(geo, f, sign, flags, scale, stream);
 }

@@ -5,11 +5,13 @@
 // step adds the divergence of the eddy stress tau_ij = 2 nu_t S_ij to the
 // nonlinear term cross1 (ns.cpp:203-206) and is otherwise the ns.cpp step:
 //
-//   z-inverse of V and grad V (i k_j V_i)   1 launch x 12 fields
-//   y-inverse                               1 x 12
-//   x-inverse, closure (nu_t by Smagorinsky or the MLP on the tensor cores,
-//   u x omega and tau_ij per point), x-forward of the 9 results: one fused
-//   pass through shared memory             1
+//   z-inverse of V and of d_z V = i k_z V (derivative on the way in)   6 out
+//   y-inverse of those and of d_y V (i k_y times the z-inverted V)     9 out
+//   x-inverse of the 9 and of d_x V (i k_x times the y-inverted V),
+//   closure (nu_t by Smagorinsky or the MLP on the tensor cores, u x omega
+//   and tau_ij per point), x-forward of the 9 results: one fused pass
+//   (k_x, k_y are constant along z lines and k_x along y lines, so each
+//   derivative is transformed only from the pass of its own axis on)
 //   y-forward of u x omega, tau             1 x 9
 //   z-forward of u x omega and tau, + i k_j tau_ij, then the AB2 /
 //   projection / CN update                  1 x 9 in, 6 out
@@ -34,7 +36,8 @@ namespace sns {
 constexpr int kXlesThreads = 384;
 
 struct XlesArgs {
-  FieldPtrs f;  // in: u (3), A_ij = d_j u_i (9) after the z and y inverses; out: u x omega, tau
+  FieldPtrs f;  // in: u (3), A_ij = d_j u_i (9) after the z and y inverses (lines of
+                // f.ikmask: i k_x times the input, the x derivative); out: u x omega, tau
   double invN;
   double csd2;
   const MlpPacked* mlp;
@@ -80,13 +83,20 @@ __global__ void __launch_bounds__(kXlesThreads)
   const int j = threadIdx.x % TPL, line = threadIdx.x / TPL;
   const int fld = line / G, gl = line - fld * G;
   C* row = sm + line * RS;
+  pdl_trigger();
+  // the model does not depend on the previous launch: load it before the wait
   if constexpr (MODEL == CLOSURE_MLP) mlp_load_smem(a.mlp, S, threadIdx.x, blockDim.x);
+  pdl_wait();
   C v[E];
   {
     const C* __restrict__ src = reinterpret_cast<const C*>(select_ptr(a.f.in, fld));
     const int64_t i0 = (row0 + gl) * L + j;
+    const bool ik = (a.f.ikmask >> fld) & 1u;
 #pragma unroll
-    for (int e = 0; e < E; e++) v[e] = src[i0 + TPL * e];
+    for (int e = 0; e < E; e++) {
+      const C x = src[i0 + TPL * e];
+      v[e] = ik ? ikmul((T)freq_i(j + TPL * e, L), x) : x;
+    }
   }
   line_fft<L>(v, row, j, tw, (T)1);
 #pragma unroll
@@ -185,8 +195,9 @@ int launch_xles_l(const XlesArgs& a, int64_t rows, cudaStream_t s) {
     set_error("twiddle table allocation failed");
     return ERR_ALLOC;
   }
-  k_xles<T, L, MODEL><<<(unsigned)(rows / G), kXlesThreads, smem, s>>>(a, tw);
-  SNS_CHECK_LAUNCH("k_xles");
+  cudaError_t e = launch_pdl(k_xles<T, L, MODEL>, dim3((unsigned)(rows / G)), dim3(kXlesThreads),
+                             smem, s, a, tw);
+  if (e != cudaSuccess) return cuda_status(e, "k_xles");
   return OK;
 }
 
@@ -222,29 +233,53 @@ int les_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* c
     set_error("closure step: no MLP model set");
     return ERR_ARG;
   }
+  const PdlScope pdl;  // the five launches overlap their neighbours' edges
   int rc;
-  auto pass = [&](int axis, int first, int count, int sign, int pro, bool from_v) -> int {
-    FieldPtrs f{};
-    f.n = count;
-    f.first = first;
-    for (int i = 0; i < count; i++) {
-      f.out[i] = U[first + i];
-      f.in[i] = from_v ? (i < 3 ? V[i] : nullptr) : U[first + i];
-    }
+  auto pass = [&](int axis, const FieldPtrs& f, int sign, int pro) -> int {
     LineGeo g = axis_geo(axis, nx, ny, nz, prec, pl.lineW);
     return run_line_pass(g, f, sign, 0, 1.0, prec, s, pro);
   };
-  // inverse of V (3) and grad V (9): z with the gradient prologue, then y
-  if ((rc = pass(2, 0, kLESWork, +1, PRO_GRAD12, true))) return rc;
-  if ((rc = pass(1, 0, kLESWork, +1, PRO_LOAD, false))) return rc;
-  // x-inverse, closure, x-forward of u x omega (U[0..2]) and tau (U[3..8])
+  // z-inverse: U[0..2] = V, U[3..5] = d_z V
+  {
+    FieldPtrs f{};
+    f.n = 6;
+    for (int q = 0; q < 6; q++) {
+      f.in[q] = V[q % 3];
+      f.out[q] = U[q];
+    }
+    f.ikmask = 0x38u;
+    if ((rc = pass(2, f, +1, PRO_IKAXIS))) return rc;
+  }
+  // y-inverse: U[6..8] = V, U[3..5] = d_z V (in place), U[9..11] = d_y V;
+  // U[0..2] is only read
+  {
+    FieldPtrs f{};
+    f.n = 9;
+    for (int i = 0; i < 3; i++) {
+      f.in[i] = U[i];
+      f.out[i] = U[6 + i];
+      f.in[3 + i] = U[3 + i];
+      f.out[3 + i] = U[3 + i];
+      f.in[6 + i] = U[i];
+      f.out[6 + i] = U[9 + i];
+    }
+    f.ikmask = 0x1C0u;
+    if ((rc = pass(1, f, +1, PRO_IKAXIS))) return rc;
+  }
+  // x-inverse (line 3 + 3 i + 0 = d_x V_i from U[6 + i]), closure, x-forward
+  // of u x omega (into U[0..2]) and tau (U[3..8]); every CTA reads its rows
+  // of all inputs before it writes them
   {
     XlesArgs a{};
     a.f.n = kLESWork;
-    for (int q = 0; q < kLESWork; q++) {
-      a.f.in[q] = U[q];
-      a.f.out[q] = U[q];
+    for (int i = 0; i < 3; i++) {
+      a.f.in[i] = U[6 + i];
+      a.f.in[3 + 3 * i + 0] = U[6 + i];
+      a.f.in[3 + 3 * i + 1] = U[9 + i];
+      a.f.in[3 + 3 * i + 2] = U[3 + i];
+      a.f.ikmask |= 1u << (3 + 3 * i);
     }
+    for (int q = 0; q < kLESWork; q++) a.f.out[q] = U[q];
     a.invN = 1.0 / (double)n;
     a.csd2 = cl.csd2;
     a.mlp = reinterpret_cast<const MlpPacked*>(cl.mlp);
@@ -254,7 +289,12 @@ int les_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* c
     if (rc) return rc;
   }
   // y-forward of the 9 results
-  if ((rc = pass(1, 0, 9, -1, PRO_LOAD, false))) return rc;
+  {
+    FieldPtrs f{};
+    f.n = 9;
+    for (int q = 0; q < 9; q++) f.in[q] = f.out[q] = U[q];
+    if ((rc = pass(1, f, -1, PRO_LOAD))) return rc;
+  }
   // z-forward of u x omega + div tau + update
   UpdateArgs a{};
   for (int d = 0; d < 3; d++) {

@@ -36,6 +36,8 @@ template <typename T, int L>
 __global__ void __launch_bounds__(MaxThreads<T>::value)
     k_xcross(FieldPtrs f, const cx_t<T>* __restrict__ tw, int G, T scale2) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_trigger();
+  pdl_wait();
   xcross_tile<T, L>(ParamFields{f}, tw, G, scale2, (int64_t)blockIdx.x, (int)blockDim.x,
                     reinterpret_cast<cx_t<T>*>(smem_raw));
 }
@@ -60,6 +62,8 @@ __global__ void __launch_bounds__(384, sizeof(T) == 4 ? 2 : 1)
   constexpr int E = P::E, TPL = P::TPL, RS = xrow_stride(M);
   static_assert(TPL <= 32, "a line's threads share a warp");
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_trigger();
+  pdl_wait();
   C* sm = reinterpret_cast<C*>(smem_raw);
   const int64_t row0 = (int64_t)blockIdx.x * G;
   const int per = G * M;
@@ -157,6 +161,8 @@ template <typename T, int L>
 __global__ void __launch_bounds__(MaxThreads<T>::value)
     k_zcurl(const LineGeo geo, const FieldPtrs f, const cx_t<T>* __restrict__ tw, int wshift) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_trigger();
+  pdl_wait();
   curl_zpass_tile<T, L>(geo, ParamFields{f}, tw, wshift, (int64_t)blockIdx.x,
                         reinterpret_cast<cx_t<T>*>(smem_raw));
 }
@@ -169,6 +175,8 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
     k_zfwd_update(const UpdateArgs a, const cx_t<T>* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[4][32];
+  pdl_trigger();
+  pdl_wait();
   zfwd_update_tile<T, L, SGS>(a, tw, (int64_t)blockIdx.x, (int)blockDim.x,
                               reinterpret_cast<cx_t<T>*>(smem_raw), red);
 }
@@ -223,8 +231,9 @@ int launch_xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream
   const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
   const double N = (double)pl.nx * pl.ny * pl.nz;
   const int blocks = (int)(rows / G);
-  k_xcross<T, L><<<blocks, threads, smem, s>>>(f, tw, G, (T)(1.0 / (N * N)));
-  SNS_CHECK_LAUNCH("k_xcross");
+  cudaError_t e = launch_pdl(k_xcross<T, L>, dim3(blocks), dim3(threads), smem, s, f, tw, G,
+                             (T)(1.0 / (N * N)));
+  if (e != cudaSuccess) return cuda_status(e, "k_xcross");
   return OK;
 }
 
@@ -264,8 +273,9 @@ int launch_zcurl(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
   }
   int wshift = 0;
   while ((1 << wshift) < g.W) wshift++;
-  k_zcurl<T, L><<<(unsigned)(g.TA * g.TB), threads, smem, s>>>(g, f, tw, wshift);
-  SNS_CHECK_LAUNCH("k_zcurl");
+  cudaError_t e = launch_pdl(k_zcurl<T, L>, dim3((unsigned)(g.TA * g.TB)), dim3(threads), smem, s,
+                             g, f, tw, wshift);
+  if (e != cudaSuccess) return cuda_status(e, "k_zcurl");
   return OK;
 }
 
@@ -292,9 +302,9 @@ int launch_xcross_r2c(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaSt
     return ERR_ALLOC;
   }
   const double N = (double)pl.nx_phys * pl.ny * pl.nz;
-  k_xcross_r2c<T, M><<<(unsigned)(rows / G), threads, smem, s>>>(f, twN, twM, G,
-                                                                   (T)(1.0 / (N * N)));
-  SNS_CHECK_LAUNCH("k_xcross_r2c");
+  cudaError_t e = launch_pdl(k_xcross_r2c<T, M>, dim3((unsigned)(rows / G)), dim3(threads), smem,
+                             s, f, twN, twM, G, (T)(1.0 / (N * N)));
+  if (e != cudaSuccess) return cuda_status(e, "k_xcross_r2c");
   return OK;
 }
 
@@ -344,8 +354,9 @@ int launch_update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
     attr[dev & 63] = true;
   }
   const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
-  k_zfwd_update<T, L, SGS><<<blocks, threads, smem, s>>>(a, tw);
-  SNS_CHECK_LAUNCH("k_zfwd_update");
+  cudaError_t e = launch_pdl(k_zfwd_update<T, L, SGS>, dim3(blocks), dim3(threads), smem, s, a,
+                             tw);
+  if (e != cudaSuccess) return cuda_status(e, "k_zfwd_update");
   return OK;
 }
 

@@ -109,12 +109,19 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
             ky0 = (T)freq_i(lc.y, geo.ny),
             kz0 = (T)freq_i(lc.z, geo.nz);
     const int naxis = geo.axis == 0 ? geo.nx : geo.axis == 1 ? geo.ny : geo.nz;
+    bool ik = false;
+    if constexpr (PRO == PRO_IKAXIS) ik = (f.ikmask() >> field) & 1u;
 #pragma unroll
     for (int e = 0; e < E; e++) {
       const T kp = (T)freq_i(j + TPL * e, naxis);
-      v[e] = pro_load<PRO, C>(src, v0, v1, v2, field, q, lc.idx0 + e * lc.step,
-                              geo.axis == 0 ? kp : kx0, geo.axis == 1 ? kp : ky0,
-                              geo.axis == 2 ? kp : kz0);
+      if constexpr (PRO == PRO_IKAXIS) {
+        const C x = src[lc.idx0 + e * lc.step];
+        v[e] = ik ? ikmul(kp, x) : x;
+      } else {
+        v[e] = pro_load<PRO, C>(src, v0, v1, v2, field, q, lc.idx0 + e * lc.step,
+                                geo.axis == 0 ? kp : kx0, geo.axis == 1 ? kp : ky0,
+                                geo.axis == 2 ? kp : kz0);
+      }
     }
   }
   line_fft<L, true>(v, row, j, tw, sg);
@@ -516,6 +523,7 @@ struct ParamFields {
   __device__ __forceinline__ const void* in(int i) const { return select_ptr(f.in, i); }
   __device__ __forceinline__ void* out(int i) const { return select_ptr(f.out, i); }
   __device__ __forceinline__ int first() const { return f.first; }
+  __device__ __forceinline__ unsigned ikmask() const { return f.ikmask; }
 };
 
 }  // namespace sns
