@@ -871,7 +871,7 @@ def closure_bench(S, torch, dev, args, world, rank, hbm, peak_src, clocks):
                      "seconds": t_train, "dataset_seconds": t_data,
                      "loss_first": losses[0][1], "loss_last": losses[-1][1],
                      "s_in": s_in, "s_out": s_out},
-        "roofline": {"bound": "tensor", "kernel": "MLP inference (k_mlp_infer, 64^3 points)",
+        "roofline": {"bound": "tensor", "kernel": "MLP inference (k_mlp_infer_tc, tcgen05, 64^3 points)",
                      "achieved": achieved, "unit": "TFLOP/s", "peak": tpeak,
                      "frac": achieved / tpeak, "traffic": None,
                      "peak_source": f"{tsrc} bf16_tflops (burst)",

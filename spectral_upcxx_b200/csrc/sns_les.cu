@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kXlesThreads)
       xa[2] = t == 0 ? pack_bf16(feat(pa, 8), 0.f) : 0u;
       xa[3] = t == 0 ? pack_bf16(feat(pb, 8), 0.f) : 0u;
       MlpTile tile;
-      mlp_tile_forward<false>(S, xa, tile);
+      mlp_tile_forward(S, xa, tile);
       if (t == 0) {
         nus[pa] = S.s_out * softplus_f(tile.z[0]);
         nus[pb] = S.s_out * softplus_f(tile.z[1]);

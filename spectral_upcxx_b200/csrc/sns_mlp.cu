@@ -1,15 +1,14 @@
 // Training and inference of the eddy-viscosity MLP (sns_mlp.cuh) on the
-// tensor cores.  No reference counterpart.
+// fifth-generation tensor cores (tcgen05, sns_tc.cuh).  No reference
+// counterpart.
 //
+//   k_mlp_infer_tc  nu_t of M points, tiles of 128 points per CTA
 // One training step over a batch of B samples is three launches:
-//   k_mlp_grad    CTAs of 128 samples (4 warps x 2 tiles of 16 rows): forward,
-//                 loss, backward through the three layers with mma.sync
-//                 (dH1 = dPre2 W2), then the weight gradients as GEMMs over the
-//                 CTA's samples (dW2 = dPre2^T H1, dW1 = dPre1^T X) from
-//                 transposed bf16 copies in shared memory; per-CTA partial
-//                 gradients go to a work array
-//   k_mlp_reduce  sums the partials in a fixed order (deterministic)
-//   k_mlp_adam    Adam on the FP32 masters, then the bf16 inference copy
+//   k_mlp_grad_tc   persistent CTAs walking tiles of 128 samples: forward,
+//                   loss, backward, the weight gradients accumulated in
+//                   tensor memory; one partial gradient per CTA
+//   k_mlp_reduce    sums the partials in a fixed order (deterministic)
+//   k_mlp_adam      Adam on the FP32 masters, then the bf16 inference copy
 // Rounding points: inputs, W1, W2, w3, the layer-1 activations and the
 // backward operands dPre2, dPre1 are bf16; everything else is FP32.
 #include <cuda_bf16.h>
@@ -26,253 +25,7 @@
 
 namespace sns {
 
-constexpr int kTrainWarps = 4;
-constexpr int kTrainRows = kTrainWarps * 32;  // samples per CTA
-constexpr int kTS = kTrainRows + 8;           // bf16 stride of the transposed tiles
-constexpr int kPart = kMlpParams + 1;         // gradients + loss sum
-
-struct TrainSmem {
-  MlpSmem m;
-  __nv_bfloat16 XT[kMlpK1 * kTS];             // inputs, [feature][sample]
-  __nv_bfloat16 H1T[kMlpHidden * kTS];        // layer-1 activations, [unit][sample]
-  __nv_bfloat16 P2T[kMlpHidden * kTS];        // dPre2, [unit][sample]
-  __nv_bfloat16 P1T[kMlpHidden * kTS];        // dPre1, [unit][sample]
-  float vec[kTrainWarps][3][kMlpHidden];      // per-warp db1, db2, dw3
-  float scal[kTrainWarps][2];                 // per-warp db3, loss sum
-};
-
-__global__ void __launch_bounds__(kTrainRows)
-    k_mlp_grad(const MlpPacked* __restrict__ P, const __nv_bfloat16* __restrict__ X,
-               const float* __restrict__ target, const float* __restrict__ weight,
-               const int* __restrict__ idx, int64_t B, float inv_batch,
-               float* __restrict__ part) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
-  mlp_load_smem(P, S.m, tid, blockDim.x);
-  __syncthreads();
-  const int lm = lane >> 3, lr = lane & 7;
-
-  float db1[8][2], db2[8][2], dw3[8][2];
-#pragma unroll
-  for (int nt = 0; nt < 8; nt++)
-#pragma unroll
-    for (int q = 0; q < 2; q++) db1[nt][q] = db2[nt][q] = dw3[nt][q] = 0.f;
-  float db3 = 0.f, loss = 0.f;
-
-  for (int tile = 0; tile < 2; tile++) {
-    const int s0 = warp * 32 + tile * 16;  // first sample (CTA-local) of the tile
-    const int64_t b0 = (int64_t)blockIdx.x * kTrainRows + s0;
-    // rows g and g + 8 of this tile
-    const int64_t ra = b0 + g, rb = b0 + g + 8;
-    const bool va = ra < B, vb = rb < B;
-    const int64_t xa_row = va ? (idx ? idx[ra] : ra) : 0;
-    const int64_t xb_row = vb ? (idx ? idx[rb] : rb) : 0;
-    uint32_t xa[4];
-    {
-      const uint32_t* pa = reinterpret_cast<const uint32_t*>(X + xa_row * kMlpK1);
-      const uint32_t* pb = reinterpret_cast<const uint32_t*>(X + xb_row * kMlpK1);
-      xa[0] = va ? pa[t] : 0u;
-      xa[1] = vb ? pb[t] : 0u;
-      xa[2] = va ? pa[t + 4] : 0u;
-      xa[3] = vb ? pb[t + 4] : 0u;
-      // transposed copy for dW1
-      S.XT[(2 * t) * kTS + s0 + g] = __ushort_as_bfloat16((unsigned short)(xa[0] & 0xffff));
-      S.XT[(2 * t + 1) * kTS + s0 + g] = __ushort_as_bfloat16((unsigned short)(xa[0] >> 16));
-      S.XT[(2 * t) * kTS + s0 + g + 8] = __ushort_as_bfloat16((unsigned short)(xa[1] & 0xffff));
-      S.XT[(2 * t + 1) * kTS + s0 + g + 8] = __ushort_as_bfloat16((unsigned short)(xa[1] >> 16));
-      S.XT[(2 * t + 8) * kTS + s0 + g] = __ushort_as_bfloat16((unsigned short)(xa[2] & 0xffff));
-      S.XT[(2 * t + 9) * kTS + s0 + g] = __ushort_as_bfloat16((unsigned short)(xa[2] >> 16));
-      S.XT[(2 * t + 8) * kTS + s0 + g + 8] = __ushort_as_bfloat16((unsigned short)(xa[3] & 0xffff));
-      S.XT[(2 * t + 9) * kTS + s0 + g + 8] = __ushort_as_bfloat16((unsigned short)(xa[3] >> 16));
-    }
-    MlpTile T;
-    mlp_tile_forward<true>(S.m, xa, T);
-    // loss and dL/dz for rows g and g + 8 (the four lanes of a row agree)
-    float dz[2];
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const bool v = h ? vb : va;
-      const int64_t r = h ? xb_row : xa_row;
-      const float z = T.z[h];
-      const float y = softplus_f(z);
-      const float d = v ? y - target[r] : 0.f;
-      const float wt = (v && weight) ? weight[r] : 1.f;
-      if (t == 0) loss += wt * d * d;
-      dz[h] = 2.f * inv_batch * wt * d / (1.f + expf(-z));
-      if (t == 0) db3 += dz[h];
-    }
-    // layer 3 and layer-2 activation gradients; dPre2 as bf16 A fragments
-    uint32_t p2a[4][4];
-#pragma unroll
-    for (int nt = 0; nt < 8; nt++) {
-      const int col = nt * 8 + 2 * t;
-      const float wl = S.m.w3[col], wh = S.m.w3[col + 1];
-      float h2[4], dp[4];
-#pragma unroll
-      for (int q = 0; q < 4; q++) h2[q] = fmaxf(T.pre2[nt][q], 0.f);
-      dw3[nt][0] += dz[0] * h2[0] + dz[1] * h2[2];
-      dw3[nt][1] += dz[0] * h2[1] + dz[1] * h2[3];
-      dp[0] = T.pre2[nt][0] > 0.f ? dz[0] * wl : 0.f;
-      dp[1] = T.pre2[nt][1] > 0.f ? dz[0] * wh : 0.f;
-      dp[2] = T.pre2[nt][2] > 0.f ? dz[1] * wl : 0.f;
-      dp[3] = T.pre2[nt][3] > 0.f ? dz[1] * wh : 0.f;
-      db2[nt][0] += dp[0] + dp[2];
-      db2[nt][1] += dp[1] + dp[3];
-      const uint32_t lo = pack_bf16(dp[0], dp[1]), hi = pack_bf16(dp[2], dp[3]);
-      p2a[nt >> 1][(nt & 1) ? 2 : 0] = lo;
-      p2a[nt >> 1][(nt & 1) ? 3 : 1] = hi;
-      // transposed copies for the weight gradients
-      S.P2T[col * kTS + s0 + g] = __ushort_as_bfloat16((unsigned short)(lo & 0xffff));
-      S.P2T[(col + 1) * kTS + s0 + g] = __ushort_as_bfloat16((unsigned short)(lo >> 16));
-      S.P2T[col * kTS + s0 + g + 8] = __ushort_as_bfloat16((unsigned short)(hi & 0xffff));
-      S.P2T[(col + 1) * kTS + s0 + g + 8] = __ushort_as_bfloat16((unsigned short)(hi >> 16));
-      const uint32_t h1lo = T.h1[nt >> 1][(nt & 1) ? 2 : 0];
-      const uint32_t h1hi = T.h1[nt >> 1][(nt & 1) ? 3 : 1];
-      S.H1T[col * kTS + s0 + g] = __ushort_as_bfloat16((unsigned short)(h1lo & 0xffff));
-      S.H1T[(col + 1) * kTS + s0 + g] = __ushort_as_bfloat16((unsigned short)(h1lo >> 16));
-      S.H1T[col * kTS + s0 + g + 8] = __ushort_as_bfloat16((unsigned short)(h1hi & 0xffff));
-      S.H1T[(col + 1) * kTS + s0 + g + 8] = __ushort_as_bfloat16((unsigned short)(h1hi >> 16));
-    }
-    // dH1 = dPre2 W2 ([16 x 64] x [64 x 64]); dPre1 = dH1 * (pre1 > 0)
-#pragma unroll
-    for (int nt = 0; nt < 8; nt++) {
-      float c[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-      for (int kp = 0; kp < 2; kp++) {
-        // B[k = n2][n = n1] = W2[n2][n1]: transposed 8x8 matrices of W2's rows
-        // 16 kt + 0..15, columns 8 nt..8 nt+7, for k-tiles 2kp and 2kp+1
-        uint32_t b[4];
-        ldsm_x4_trans(b, &S.m.W2[((2 * kp + (lm >> 1)) * 16 + (lm & 1) * 8 + lr) * kW2Stride +
-                                 nt * 8]);
-        mma_bf16_16816(c, p2a[2 * kp], b[0], b[1]);
-        mma_bf16_16816(c, p2a[2 * kp + 1], b[2], b[3]);
-      }
-      const int col = nt * 8 + 2 * t;
-      float dp[4];
-#pragma unroll
-      for (int q = 0; q < 4; q++) dp[q] = T.pre1[nt][q] > 0.f ? c[q] : 0.f;
-      db1[nt][0] += dp[0] + dp[2];
-      db1[nt][1] += dp[1] + dp[3];
-      const uint32_t lo = pack_bf16(dp[0], dp[1]), hi = pack_bf16(dp[2], dp[3]);
-      S.P1T[col * kTS + s0 + g] = __ushort_as_bfloat16((unsigned short)(lo & 0xffff));
-      S.P1T[(col + 1) * kTS + s0 + g] = __ushort_as_bfloat16((unsigned short)(lo >> 16));
-      S.P1T[col * kTS + s0 + g + 8] = __ushort_as_bfloat16((unsigned short)(hi & 0xffff));
-      S.P1T[(col + 1) * kTS + s0 + g + 8] = __ushort_as_bfloat16((unsigned short)(hi >> 16));
-    }
-  }
-  // per-warp vectors: reduce over the eight row groups g (lanes with equal t)
-#pragma unroll
-  for (int nt = 0; nt < 8; nt++)
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-#pragma unroll
-      for (int o = 4; o < 32; o <<= 1) {
-        db1[nt][q] += __shfl_xor_sync(0xffffffffu, db1[nt][q], o);
-        db2[nt][q] += __shfl_xor_sync(0xffffffffu, db2[nt][q], o);
-        dw3[nt][q] += __shfl_xor_sync(0xffffffffu, dw3[nt][q], o);
-      }
-    }
-#pragma unroll
-  for (int o = 4; o < 32; o <<= 1) {
-    db3 += __shfl_xor_sync(0xffffffffu, db3, o);
-    loss += __shfl_xor_sync(0xffffffffu, loss, o);
-  }
-  if (g == 0) {
-#pragma unroll
-    for (int nt = 0; nt < 8; nt++)
-#pragma unroll
-      for (int q = 0; q < 2; q++) {
-        const int col = nt * 8 + 2 * t + q;
-        S.vec[warp][0][col] = db1[nt][q];
-        S.vec[warp][1][col] = db2[nt][q];
-        S.vec[warp][2][col] = dw3[nt][q];
-      }
-  }
-  if (lane == 0) {
-    S.scal[warp][0] = db3;
-    S.scal[warp][1] = loss;
-  }
-  __syncthreads();
-
-  float* out = part + (int64_t)blockIdx.x * kPart;
-  // dW2[n2][n1] = sum_s dPre2[s][n2] H1[s][n1]: warp w owns rows n2 in [16w, 16w + 16)
-  {
-    float acc[8][4];
-#pragma unroll
-    for (int nt = 0; nt < 8; nt++)
-#pragma unroll
-      for (int q = 0; q < 4; q++) acc[nt][q] = 0.f;
-#pragma unroll
-    for (int ks = 0; ks < kTrainRows / 16; ks++) {
-      uint32_t a[4];
-      load_a_tile(&S.P2T[(16 * warp) * kTS + 16 * ks], kTS, a);
-#pragma unroll
-      for (int nt = 0; nt < 8; nt += 2) {
-        uint32_t b[4];
-        load_b_pair(&S.H1T[(nt * 8) * kTS + 16 * ks], kTS, b);
-        mma_bf16_16816(acc[nt], a, b[0], b[1]);
-        mma_bf16_16816(acc[nt + 1], a, b[2], b[3]);
-      }
-    }
-#pragma unroll
-    for (int nt = 0; nt < 8; nt++) {
-      const int r0 = 16 * warp + g, c0 = nt * 8 + 2 * t;
-      out[kMlpOffW2 + r0 * kMlpHidden + c0] = acc[nt][0];
-      out[kMlpOffW2 + r0 * kMlpHidden + c0 + 1] = acc[nt][1];
-      out[kMlpOffW2 + (r0 + 8) * kMlpHidden + c0] = acc[nt][2];
-      out[kMlpOffW2 + (r0 + 8) * kMlpHidden + c0 + 1] = acc[nt][3];
-    }
-  }
-  // dW1[n1][f] = sum_s dPre1[s][n1] X[s][f]: warp w owns rows n1 in [16w, 16w + 16)
-  {
-    float acc[2][4];
-#pragma unroll
-    for (int nt = 0; nt < 2; nt++)
-#pragma unroll
-      for (int q = 0; q < 4; q++) acc[nt][q] = 0.f;
-#pragma unroll
-    for (int ks = 0; ks < kTrainRows / 16; ks++) {
-      uint32_t a[4];
-      load_a_tile(&S.P1T[(16 * warp) * kTS + 16 * ks], kTS, a);
-      {
-        uint32_t b[4];
-        load_b_pair(&S.XT[16 * ks], kTS, b);
-        mma_bf16_16816(acc[0], a, b[0], b[1]);
-        mma_bf16_16816(acc[1], a, b[2], b[3]);
-      }
-    }
-#pragma unroll
-    for (int nt = 0; nt < 2; nt++) {
-      const int r0 = 16 * warp + g, c0 = nt * 8 + 2 * t;
-      out[kMlpOffW1 + r0 * kMlpK1 + c0] = acc[nt][0];
-      out[kMlpOffW1 + r0 * kMlpK1 + c0 + 1] = acc[nt][1];
-      out[kMlpOffW1 + (r0 + 8) * kMlpK1 + c0] = acc[nt][2];
-      out[kMlpOffW1 + (r0 + 8) * kMlpK1 + c0 + 1] = acc[nt][3];
-    }
-  }
-  // vectors and scalars, summed over the warps in a fixed order
-  for (int i = tid; i < kMlpHidden; i += blockDim.x) {
-    float a = 0.f, b = 0.f, c = 0.f;
-    for (int w = 0; w < kTrainWarps; w++) {
-      a += S.vec[w][0][i];
-      b += S.vec[w][1][i];
-      c += S.vec[w][2][i];
-    }
-    out[kMlpOffB1 + i] = a;
-    out[kMlpOffB2 + i] = b;
-    out[kMlpOffW3 + i] = c;
-  }
-  if (tid == 0) {
-    float a = 0.f, l = 0.f;
-    for (int w = 0; w < kTrainWarps; w++) {
-      a += S.scal[w][0];
-      l += S.scal[w][1];
-    }
-    out[kMlpOffB3] = a;
-    out[kMlpParams] = l;
-  }
-}
+constexpr int kPart = kMlpParams + 1;  // gradients + loss sum
 
 // grad[p] = sum over CTAs of part[cta][p] (fixed order); the loss entry is
 // turned into the batch mean.
@@ -336,31 +89,6 @@ __global__ void k_mlp_pack(const float* __restrict__ w, float s_in, float s_out,
     P->w3[p - kMlpOffW3] = __float2bfloat16_rn(x);
   else
     P->b3 = x;
-}
-
-// nu_t = s_out softplus(z) for M rows of bf16 features (warps of 16 rows).
-__global__ void __launch_bounds__(256)
-    k_mlp_infer(const MlpPacked* __restrict__ P, const __nv_bfloat16* __restrict__ X, int64_t M,
-                float* __restrict__ nut) {
-  __shared__ MlpSmem S;
-  mlp_load_smem(P, S, threadIdx.x, blockDim.x);
-  __syncthreads();
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t r0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 16; r0 < M;
-       r0 += warps * 16) {
-    const int64_t ra = r0 + g, rb = r0 + g + 8;
-    const uint32_t* pa = reinterpret_cast<const uint32_t*>(X + (ra < M ? ra : 0) * kMlpK1);
-    const uint32_t* pb = reinterpret_cast<const uint32_t*>(X + (rb < M ? rb : 0) * kMlpK1);
-    uint32_t xa[4] = {ra < M ? pa[t] : 0u, rb < M ? pb[t] : 0u, ra < M ? pa[t + 4] : 0u,
-                      rb < M ? pb[t + 4] : 0u};
-    MlpTile T;
-    mlp_tile_forward<false>(S, xa, T);
-    if (t == 0) {
-      if (ra < M) nut[ra] = S.s_out * softplus_f(T.z[0]);
-      if (rb < M) nut[rb] = S.s_out * softplus_f(T.z[1]);
-    }
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -544,45 +272,419 @@ __global__ void __launch_bounds__(kTcRows)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Training (loss and gradients) on tcgen05: a persistent CTA of 128 threads
+// walks tiles of 128 samples (thread m owns sample m: its input row, its
+// accumulator lanes and its scalar terms).  Per tile, five MMA groups:
+//   M1  pre1 = X W1^T (+ b1 via the bias columns)       D cols   0..63
+//   M2  pre2 = H1 W2^T + b2 (bias slice)                D cols  64..127
+//   M3  dH1 = dPre2 W2 (W2 read MN-major)               D cols   0..63
+//   M4  dW2 += dPre2^T H1 (M 64, both operands MN-major, K = the samples)
+//                                                       D cols 128..191
+//   M5  dW1 += dPre1^T X (M 64, N 16)                   D cols 192..207
+// dW1 and dW2 accumulate in tensor memory over all the CTA's tiles (M = 64
+// accumulators: row r in lane 32 (r / 16) + r % 16).  The vector gradients
+// (db1, db2, dw3) are FP32 sums over samples, reduced across each warp by a
+// shuffle reduce-scatter (lane l keeps columns 2l, 2l + 1) and across warps
+// in a fixed order at the end; the scalars (db3, loss) likewise.  Rounding
+// points as in the oracle: dPre2 and dPre1 enter the MMAs in BF16, the
+// vector sums use their FP32 values.  The CTA writes one partial (kPart
+// floats) for the deterministic reduce.
+constexpr int kGtRows = 128;
+constexpr int kGtCols = 256;  // tensor-memory columns
+
+struct __align__(128) GradTcSmem {
+  unsigned char W1[kMlpHidden * kMlpK1 * 2];
+  unsigned char W2[kMlpHidden * kMlpHidden * 2];
+  unsigned char B2[kMlpHidden * 16 * 2];
+  unsigned char ONES[kGtRows * 16 * 2];
+  unsigned char X[kGtRows * kMlpK1 * 2];
+  unsigned char H1[kGtRows * kMlpHidden * 2];
+  unsigned char P2[kGtRows * kMlpHidden * 2];  // dPre2 (bf16)
+  unsigned char P1[kGtRows * kMlpHidden * 2];  // dPre1 (bf16)
+  float w3[kMlpHidden];
+  float vec[4][3][kMlpHidden];  // per warp: db1, db2, dw3
+  float scal[4][2];             // per warp: db3, loss
+  float b3;
+  uint64_t mbar;
+  uint32_t tmem;
+  int abort;
+};
+// at most two CTAs per SM (2 x 256 tensor-memory columns): reserve enough
+// shared memory that a third never shares the SM
+constexpr int kGtSmemBytes = 80 * 1024;
+static_assert(sizeof(GradTcSmem) <= kGtSmemBytes, "training tile fits the reservation");
+
+// Sum of v[c] over the 32 lanes of the warp for c = 0..63; lane l returns the
+// sums of columns 2l and 2l + 1.
+__device__ __forceinline__ void warp_colsum64(float (&v)[64], float& c0, float& c1) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 16, n = 32; o >= 1; o >>= 1, n >>= 1) {
+    const bool up = lane & o;
+#pragma unroll
+    for (int i = 0; i < 32; i++) {
+      if (i < n) {
+        const float send = up ? v[i] : v[n + i];
+        const float keep = up ? v[n + i] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+      }
+    }
+  }
+  c0 = v[0];
+  c1 = v[1];
+}
+
+__device__ __forceinline__ bool tc_step(uint64_t* mbar, uint32_t& phase, int& abort_flag) {
+  const bool ok = tc::mbar_wait(mbar, phase, tc::kWaitCycles);
+  phase ^= 1;
+  if (!ok) abort_flag = 1;
+  tc::fence_after_sync();
+  __syncthreads();
+  return !abort_flag;
+}
+
+__global__ void __launch_bounds__(kGtRows)
+    k_mlp_grad_tc(const MlpPacked* __restrict__ P, const __nv_bfloat16* __restrict__ X,
+                  const float* __restrict__ target, const float* __restrict__ weight,
+                  const int* __restrict__ idx, int64_t B, float inv_batch,
+                  float* __restrict__ part) {
+  extern __shared__ __align__(128) unsigned char gt_raw[];
+  GradTcSmem& S = *reinterpret_cast<GradTcSmem*>(gt_raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < kMlpHidden * kMlpK1 / 8; i += kGtRows) {
+    const int n = i / (kMlpK1 / 8), c = i % (kMlpK1 / 8);
+    uint4 v = reinterpret_cast<const uint4*>(P->W1)[i];
+    if (c == 1) {
+      const float b = P->b1[n];
+      const float hi = __bfloat162float(__float2bfloat16_rn(b));
+      v.x = (v.x & 0xFFFFu) | (bf16_bits(hi) << 16);
+      v.y = (v.y & 0xFFFF0000u) | bf16_bits(b - hi);
+    }
+    *reinterpret_cast<uint4*>(S.W1 + tc::kmajor_off(n, 8 * c, kMlpK1)) = v;
+  }
+  for (int i = tid; i < kMlpHidden * kMlpHidden / 8; i += kGtRows) {
+    const int n = i / (kMlpHidden / 8), c = i % (kMlpHidden / 8);
+    *reinterpret_cast<uint4*>(S.W2 + tc::kmajor_off(n, 8 * c, kMlpHidden)) =
+        reinterpret_cast<const uint4*>(P->W2)[i];
+  }
+  for (int n = tid; n < kMlpHidden; n += kGtRows) {
+    const float b = P->b2[n];
+    const float hi = __bfloat162float(__float2bfloat16_rn(b));
+    *reinterpret_cast<uint4*>(S.B2 + tc::kmajor_off(n, 0, 16)) =
+        make_uint4(bf16_bits(hi) | (bf16_bits(b - hi) << 16), 0u, 0u, 0u);
+    *reinterpret_cast<uint4*>(S.B2 + tc::kmajor_off(n, 8, 16)) = make_uint4(0u, 0u, 0u, 0u);
+    S.w3[n] = __bfloat162float(P->w3[n]);
+  }
+  const uint32_t one = bf16_bits(1.f), one2 = one * 0x10001u;
+  *reinterpret_cast<uint4*>(S.ONES + tc::kmajor_off(tid, 0, 16)) = make_uint4(one2 & 0xFFFFFFFFu, 0u, 0u, 0u);
+  *reinterpret_cast<uint4*>(S.ONES + tc::kmajor_off(tid, 8, 16)) = make_uint4(0u, 0u, 0u, 0u);
+  if (tid == 0) {
+    S.b3 = P->b3;
+    S.abort = 0;
+    tc::mbar_init(&S.mbar, 1);
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(&S.tmem, kGtCols);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = S.tmem;
+  const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
+  const uint32_t sX = tc::smem_u32(S.X), sH = tc::smem_u32(S.H1), sP2 = tc::smem_u32(S.P2),
+                 sP1 = tc::smem_u32(S.P1), sO = tc::smem_u32(S.ONES);
+  const uint32_t sW1 = tc::smem_u32(S.W1), sW2 = tc::smem_u32(S.W2), sB2 = tc::smem_u32(S.B2);
+  constexpr uint32_t id_fwd = tc::idesc_bf16(kGtRows, kMlpHidden);          // M1, M2
+  constexpr uint32_t id_dh = tc::idesc_bf16(kGtRows, kMlpHidden, false, true);  // M3
+  constexpr uint32_t id_dw2 = tc::idesc_bf16(64, kMlpHidden, true, true);   // M4
+  constexpr uint32_t id_dw1 = tc::idesc_bf16(64, kMlpK1, true, true);       // M5
+  uint32_t phase = 0;
+  float acc_db1[2] = {0.f, 0.f}, acc_db2[2] = {0.f, 0.f}, acc_dw3[2] = {0.f, 0.f};
+  float acc_db3 = 0.f, acc_loss = 0.f;
+  bool first = true;
+  const int64_t tiles = (B + kGtRows - 1) / kGtRows;
+  for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int64_t b = tile * kGtRows + tid;
+    const bool valid = b < B;
+    const int64_t row = valid ? (idx ? (int64_t)idx[b] : b) : 0;
+    float tgt = 0.f, wt = 0.f;
+    {
+      uint4 x0 = make_uint4(0, 0, 0, 0), x1 = x0;
+      if (valid) {
+        const uint4* src = reinterpret_cast<const uint4*>(X + row * kMlpK1);
+        x0 = src[0];
+        x1 = src[1];
+        tgt = target[row];
+        wt = weight ? weight[row] : 1.f;
+      }
+      x1.x = (x1.x & 0xFFFFu) | (one2 & 0xFFFF0000u);
+      x1.y = (x1.y & 0xFFFF0000u) | (one2 & 0xFFFFu);
+      *reinterpret_cast<uint4*>(S.X + tc::kmajor_off(tid, 0, kMlpK1)) = x0;
+      *reinterpret_cast<uint4*>(S.X + tc::kmajor_off(tid, 8, kMlpK1)) = x1;
+    }
+    // M1
+    tc::fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+      tc::mma_bf16(tmem, tc::sdesc(sX, 128, 16 * kMlpK1), tc::sdesc(sW1, 128, 16 * kMlpK1), id_fwd,
+                   0);
+      tc::commit(&S.mbar);
+    }
+    if (!tc_step(&S.mbar, phase, S.abort)) break;
+    // pre1 -> mask, H1
+    uint32_t mask1[2] = {0u, 0u};
+#pragma unroll
+    for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+      uint32_t r[16];
+      tc::tmem_ld16(tmem + lane_base + c0, r);
+      uint32_t h[8];
+#pragma unroll
+      for (int j = 0; j < 16; j++)
+        if (__uint_as_float(r[j]) > 0.f) mask1[(c0 + j) >> 5] |= 1u << ((c0 + j) & 31);
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        h[j] = pack_bf16(fmaxf(__uint_as_float(r[2 * j]), 0.f),
+                         fmaxf(__uint_as_float(r[2 * j + 1]), 0.f));
+      *reinterpret_cast<uint4*>(S.H1 + tc::kmajor_off(tid, c0, kMlpHidden)) =
+          make_uint4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<uint4*>(S.H1 + tc::kmajor_off(tid, c0 + 8, kMlpHidden)) =
+          make_uint4(h[4], h[5], h[6], h[7]);
+    }
+    // M2
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int s = 0; s < kMlpHidden / 16; s++)
+        tc::mma_bf16(tmem + 64, tc::sdesc(sH + 256 * s, 128, 16 * kMlpHidden),
+                     tc::sdesc(sW2 + 256 * s, 128, 16 * kMlpHidden), id_fwd, s > 0);
+      tc::mma_bf16(tmem + 64, tc::sdesc(sO, 128, 256), tc::sdesc(sB2, 128, 256), id_fwd, 1);
+      tc::commit(&S.mbar);
+    }
+    if (!tc_step(&S.mbar, phase, S.abort)) break;
+    // output, loss, dz; then dw3, dPre2 (-> P2), db2
+    float dz;
+    {
+      float z = S.b3;
+#pragma unroll
+      for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+        uint32_t r[16];
+        tc::tmem_ld16(tmem + lane_base + 64 + c0, r);
+#pragma unroll
+        for (int j = 0; j < 16; j++) z += fmaxf(__uint_as_float(r[j]), 0.f) * S.w3[c0 + j];
+      }
+      const float y = softplus_f(z);
+      const float d = valid ? y - tgt : 0.f;
+      acc_loss += wt * d * d;
+      dz = 2.f * inv_batch * wt * d / (1.f + expf(-z));
+    }
+    float vw3[64], vb2[64];
+#pragma unroll
+    for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+      uint32_t r[16];
+      tc::tmem_ld16(tmem + lane_base + 64 + c0, r);
+      uint32_t h[8];
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const float p2 = __uint_as_float(r[j]);
+        vw3[c0 + j] = dz * fmaxf(p2, 0.f);
+        vb2[c0 + j] = p2 > 0.f ? dz * S.w3[c0 + j] : 0.f;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; j++) h[j] = pack_bf16(vb2[c0 + 2 * j], vb2[c0 + 2 * j + 1]);
+      *reinterpret_cast<uint4*>(S.P2 + tc::kmajor_off(tid, c0, kMlpHidden)) =
+          make_uint4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<uint4*>(S.P2 + tc::kmajor_off(tid, c0 + 8, kMlpHidden)) =
+          make_uint4(h[4], h[5], h[6], h[7]);
+    }
+    {
+      float a0, a1;
+      warp_colsum64(vw3, a0, a1);
+      acc_dw3[0] += a0;
+      acc_dw3[1] += a1;
+      warp_colsum64(vb2, a0, a1);
+      acc_db2[0] += a0;
+      acc_db2[1] += a1;
+    }
+    {
+      float d3 = dz;
+#pragma unroll
+      for (int o = 16; o >= 1; o >>= 1) d3 += __shfl_xor_sync(0xffffffffu, d3, o);
+      acc_db3 += d3;
+    }
+    // M3 (dH1) and M4 (dW2 += dPre2^T H1)
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int s = 0; s < kMlpHidden / 16; s++)
+        tc::mma_bf16(tmem, tc::sdesc(sP2 + 256 * s, 128, 16 * kMlpHidden),
+                     tc::sdesc(sW2 + 2048 * s, 16 * kMlpHidden, 128), id_dh, s > 0);
+#pragma unroll
+      for (int s = 0; s < kGtRows / 16; s++)
+        tc::mma_bf16(tmem + 128, tc::sdesc(sP2 + 2048 * s, 16 * kMlpHidden, 128),
+                     tc::sdesc(sH + 2048 * s, 16 * kMlpHidden, 128), id_dw2, (!first) || s > 0);
+      tc::commit(&S.mbar);
+    }
+    if (!tc_step(&S.mbar, phase, S.abort)) break;
+    // dPre1 = dH1 * (pre1 > 0) -> P1, db1
+    {
+      float vb1[64];
+#pragma unroll
+      for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+        uint32_t r[16];
+        tc::tmem_ld16(tmem + lane_base + c0, r);
+        uint32_t h[8];
+#pragma unroll
+        for (int j = 0; j < 16; j++)
+          vb1[c0 + j] = ((mask1[(c0 + j) >> 5] >> ((c0 + j) & 31)) & 1u) ? __uint_as_float(r[j])
+                                                                          : 0.f;
+#pragma unroll
+        for (int j = 0; j < 8; j++) h[j] = pack_bf16(vb1[c0 + 2 * j], vb1[c0 + 2 * j + 1]);
+        *reinterpret_cast<uint4*>(S.P1 + tc::kmajor_off(tid, c0, kMlpHidden)) =
+            make_uint4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<uint4*>(S.P1 + tc::kmajor_off(tid, c0 + 8, kMlpHidden)) =
+            make_uint4(h[4], h[5], h[6], h[7]);
+      }
+      float a0, a1;
+      warp_colsum64(vb1, a0, a1);
+      acc_db1[0] += a0;
+      acc_db1[1] += a1;
+    }
+    // M5 (dW1 += dPre1^T X)
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int s = 0; s < kGtRows / 16; s++)
+        tc::mma_bf16(tmem + 192, tc::sdesc(sP1 + 2048 * s, 16 * kMlpHidden, 128),
+                     tc::sdesc(sX + 512 * s, 16 * kMlpK1, 128), id_dw1, (!first) || s > 0);
+      tc::commit(&S.mbar);
+    }
+    if (!tc_step(&S.mbar, phase, S.abort)) break;
+    first = false;
+    tc::fence_before_sync();
+  }
+  __syncthreads();
+  float* out = part + (int64_t)blockIdx.x * kPart;
+  if (S.abort) {
+    tc::mbar_wait(&S.mbar, phase ^ 1, tc::kWaitCycles);
+    if (tid == 0) atomicExch(&g_mlp_tc_status, 1);
+  } else {
+    // dW2 and dW1 from the M = 64 accumulators: lanes 32 w .. 32 w + 15 hold
+    // rows 16 w .. 16 w + 15 (a CTA without tiles writes zeros)
+    const int n = 16 * warp + lane;
+#pragma unroll
+    for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+      uint32_t r[16];
+      tc::tmem_ld16(tmem + lane_base + 128 + c0, r);
+      if (lane < 16)
+#pragma unroll
+        for (int j = 0; j < 16; j++)
+          out[kMlpOffW2 + n * kMlpHidden + c0 + j] = first ? 0.f : __uint_as_float(r[j]);
+    }
+    {
+      uint32_t r[16];
+      tc::tmem_ld16(tmem + lane_base + 192, r);
+      if (lane < 16)
+#pragma unroll
+        for (int j = 0; j < 16; j++)
+          out[kMlpOffW1 + n * kMlpK1 + j] = (first || j >= kMlpIn) ? 0.f : __uint_as_float(r[j]);
+    }
+    S.vec[warp][0][2 * lane] = acc_db1[0];
+    S.vec[warp][0][2 * lane + 1] = acc_db1[1];
+    S.vec[warp][1][2 * lane] = acc_db2[0];
+    S.vec[warp][1][2 * lane + 1] = acc_db2[1];
+    S.vec[warp][2][2 * lane] = acc_dw3[0];
+    S.vec[warp][2][2 * lane + 1] = acc_dw3[1];
+    float l = acc_loss;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if (lane == 0) {
+      S.scal[warp][0] = acc_db3;
+      S.scal[warp][1] = l;
+    }
+  }
+  __syncthreads();
+  if (!S.abort) {
+    for (int i = tid; i < kMlpHidden; i += kGtRows) {
+      float a = 0.f, b2 = 0.f, c = 0.f;
+      for (int w = 0; w < 4; w++) {
+        a += S.vec[w][0][i];
+        b2 += S.vec[w][1][i];
+        c += S.vec[w][2][i];
+      }
+      out[kMlpOffB1 + i] = a;
+      out[kMlpOffB2 + i] = b2;
+      out[kMlpOffW3 + i] = c;
+    }
+    if (tid == 0) {
+      float a = 0.f, l = 0.f;
+      for (int w = 0; w < 4; w++) {
+        a += S.scal[w][0];
+        l += S.scal[w][1];
+      }
+      out[kMlpOffB3] = a;
+      out[kMlpParams] = l;
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, kGtCols);
+  }
+}
+
 namespace {
 
 int grad_launch(const void* packed, const void* X, const float* t, const float* w,
                 const int* idx, int64_t B, float* grad, cudaStream_t s) {
-  const int64_t nb = (B + kTrainRows - 1) / kTrainRows;
-  if (nb > (1 << 24)) {
-    set_error("sns_mlp_grad: batch too large");
-    return ERR_UNSUPPORTED;
+  if (reinterpret_cast<uintptr_t>(X) % 16 || reinterpret_cast<uintptr_t>(packed) % 16) {
+    set_error("sns_mlp_grad: X and the packed model must be 16-byte aligned");
+    return ERR_ARG;
   }
-  void* part = nullptr;
-  int rc = pool_malloc(&part, sizeof(float) * kPart * nb);
-  if (rc) return rc;
   static bool attr[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr[dev & 63]) {
-    rc = cuda_status(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)sizeof(TrainSmem)),
-                     "cudaFuncSetAttribute(k_mlp_grad)");
-    if (rc) {
-      pool_free(part);
-      return rc;
-    }
+    int rc = cuda_status(cudaFuncSetAttribute(k_mlp_grad_tc,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              kGtSmemBytes),
+                         "cudaFuncSetAttribute(k_mlp_grad_tc)");
+    if (rc) return rc;
     attr[dev & 63] = true;
   }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t tiles = (B + kGtRows - 1) / kGtRows;
+  const int nb = (int)std::min<int64_t>(tiles, 2 * (int64_t)sms);
+  void* part = nullptr;
+  int rc = pool_malloc(&part, sizeof(float) * kPart * nb);
+  if (rc) return rc;
   const float inv = (float)(1.0 / (double)B);
-  k_mlp_grad<<<(unsigned)nb, kTrainRows, sizeof(TrainSmem), s>>>(
+  k_mlp_grad_tc<<<(unsigned)nb, kGtRows, kGtSmemBytes, s>>>(
       reinterpret_cast<const MlpPacked*>(packed), reinterpret_cast<const __nv_bfloat16*>(X), t, w,
       idx, B, inv, reinterpret_cast<float*>(part));
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) {
-    k_mlp_reduce<<<(kPart + 255) / 256, 256, 0, s>>>(reinterpret_cast<float*>(part), (int)nb, inv,
+    k_mlp_reduce<<<(kPart + 255) / 256, 256, 0, s>>>(reinterpret_cast<float*>(part), nb, inv,
                                                     grad);
     e = cudaGetLastError();
   }
   // the pool may hand the block to any later caller: wait for the kernels
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   pool_free(part);
-  return cuda_status(e, "k_mlp_grad");
+  return cuda_status(e, "k_mlp_grad_tc");
 }
 
 }  // namespace

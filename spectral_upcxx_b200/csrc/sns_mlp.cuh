@@ -2,7 +2,10 @@
 //
 // No reference counterpart (the reference has no subgrid model).  BF16
 // weights, inputs and hidden activations; FP32 accumulation and biases;
-// ReLU hidden layers; nu_t = s_out * softplus(z).  A warp evaluates 16 points
+// ReLU hidden layers; nu_t = s_out * softplus(z).  The model layout and the
+// warp-level forward used inside the fused x pass of the closure step
+// (k_xles); the standalone inference and training kernels run on tcgen05
+// (sns_mlp.cu, sns_tc.cuh).  The warp-level forward evaluates 16 points
 // at a time with mma.sync m16n8k16 (bf16 in, f32 accumulate): the layer-1
 // accumulators are rounded to bf16 and reused in registers as the layer-2 A
 // operand (the m16n8 accumulator layout of two adjacent n-tiles is the
@@ -91,21 +94,14 @@ __device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a
 }
 
 // ldmatrix: lanes 8m..8m+7 give the row addresses of 8x8 bf16 matrix m; lane
-// l receives row l/4, columns 2(l%4), 2(l%4)+1 of each matrix (transposed
-// matrices with .trans).  Rows must start on 16-byte boundaries.
+// l receives row l/4, columns 2(l%4), 2(l%4)+1 of each matrix.  Rows must
+// start on 16-byte boundaries.
 __device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const void* p) {
   const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
   asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
                : "r"(a));
 }
-__device__ __forceinline__ void ldsm_x4_trans(uint32_t (&r)[4], const void* p) {
-  const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-               : "r"(a));
-}
-
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);  // .x = lo (low half), .y = hi
   return *reinterpret_cast<uint32_t*>(&v);
@@ -118,14 +114,10 @@ __device__ __forceinline__ float softplus_f(float z) {
 // Layer activations of one 16-row tile, in fragment layout.
 struct MlpTile {
   uint32_t h1[4][4];  // layer-1 output (bf16) as the A operand of layer 2, per k-tile
-  float pre1[8][4];   // layer-1 pre-activations (f32), per n-tile (training only)
-  float pre2[8][4];   // layer-2 pre-activations (f32), per n-tile
   float z[2];         // output pre-activation of rows g and g + 8
 };
 
-// Forward of one 16-row tile whose A operand (inputs) is xa.  With KEEP =
-// false the layer-1 pre-activations are not kept (inference).
-template <bool KEEP>
+// Forward of one 16-row tile whose A operand (inputs) is xa.
 __device__ __forceinline__ void mlp_tile_forward(const MlpSmem& s, const uint32_t (&xa)[4],
                                                  MlpTile& T) {
   const int lane = threadIdx.x & 31, t = lane & 3;
@@ -143,10 +135,6 @@ __device__ __forceinline__ void mlp_tile_forward(const MlpSmem& s, const uint32_
     c[1] += bh;
     c[2] += bl;
     c[3] += bh;
-    if constexpr (KEEP) {
-#pragma unroll
-      for (int q = 0; q < 4; q++) T.pre1[nt][q] = c[q];
-    }
     const uint32_t lo = pack_bf16(fmaxf(c[0], 0.f), fmaxf(c[1], 0.f));
     const uint32_t hi = pack_bf16(fmaxf(c[2], 0.f), fmaxf(c[3], 0.f));
     // n-tile nt holds columns 8nt..8nt+7 = k-tile nt/2, half nt%2
@@ -172,8 +160,6 @@ __device__ __forceinline__ void mlp_tile_forward(const MlpSmem& s, const uint32_
     c[1] += bh;
     c[2] += bl;
     c[3] += bh;
-#pragma unroll
-    for (int q = 0; q < 4; q++) T.pre2[nt][q] = c[q];
     // layer 3: dot product with w3 over this lane's columns
     const float wl = s.w3[col], wh = s.w3[col + 1];
     zl += fmaxf(c[0], 0.f) * wl + fmaxf(c[1], 0.f) * wh;
@@ -185,22 +171,6 @@ __device__ __forceinline__ void mlp_tile_forward(const MlpSmem& s, const uint32_
   zh += __shfl_xor_sync(0xffffffffu, zh, 2);
   T.z[0] = zl + s.b3;
   T.z[1] = zh + s.b3;
-}
-
-// A operand of a 16x16 bf16 tile stored row-major with `stride` bf16 per row
-// (rows 16-byte aligned): matrices (rows 0-7 | 8-15) x (columns 0-7 | 8-15).
-__device__ __forceinline__ void load_a_tile(const __nv_bfloat16* base, int stride,
-                                            uint32_t (&a)[4]) {
-  const int lane = threadIdx.x & 31, lm = lane >> 3, lr = lane & 7;
-  ldsm_x4(a, base + ((lm & 1) * 8 + lr) * stride + (lm >> 1) * 8);
-}
-
-// B operands of n-tiles nt, nt+1 (k-tile of 16) from a [n][k] row-major bf16
-// tile: b[0], b[1] for nt and b[2], b[3] for nt + 1.
-__device__ __forceinline__ void load_b_pair(const __nv_bfloat16* base, int stride,
-                                            uint32_t (&b)[4]) {
-  const int lane = threadIdx.x & 31, lm = lane >> 3, lr = lane & 7;
-  ldsm_x4(b, base + ((lm >> 1) * 8 + lr) * stride + (lm & 1) * 8);
 }
 
 }  // namespace sns

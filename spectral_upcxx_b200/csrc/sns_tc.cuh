@@ -12,7 +12,11 @@
 // tile stores row r, element k at
 //     (r / 8) * (16 K) + (k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2
 // bytes, i.e. LBO = 128 and SBO = 16 K; the K-slice [16 s, 16 s + 16) of such
-// a tile starts 256 s bytes after its base.
+// a tile starts 256 s bytes after its base.  The same bytes read as an
+// MN-major operand whose MN index is k and whose K index is r (the transposed
+// matrix: 8 consecutive k contiguous, 8 r per core matrix) have LBO = 16 K
+// (r groups) and SBO = 128 (k groups); its K-slice of rows [16 s, 16 s + 16)
+// starts 32 K s bytes after the base.
 //
 // Every wait on an mbarrier is bounded (a clock budget): the kernels record a
 // timeout in a status word instead of spinning forever.
@@ -42,11 +46,12 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
 }
 
 // Instruction descriptor of tcgen05.mma kind::f16: dense, D in F32 (bits
-// 4-5 = 1), A and B in BF16 (bits 7-9, 10-12 = 1), both K-major (bits 15, 16
-// = 0), N >> 3 in bits 17-22, M >> 4 in bits 24-28.
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
-         ((uint32_t)(M >> 4) << 24);
+// 4-5 = 1), A and B in BF16 (bits 7-9, 10-12 = 1), A and B K-major (bits 15,
+// 16 = 0) or MN-major (= 1), N >> 3 in bits 17-22, M >> 4 in bits 24-28.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool a_mn = false,
+                                                  bool b_mn = false) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
 // D[tmem] (+)= A[smem] B[smem]^T, issued by one thread.

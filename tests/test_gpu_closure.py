@@ -104,6 +104,32 @@ def test_mlp_gradient_matches_oracle(CO, CL, cuda):
         assert rel_l2(g[a:b], np.ravel(ref[name])) < 2e-3, name
 
 
+def test_mlp_gradient_many_tiles_per_cta(CO, CL, sns, cuda):
+    """A batch of 100,000 samples: every CTA of the tcgen05 training kernel
+    accumulates dW1, dW2 in tensor memory over two or three tiles; the last
+    tile is ragged.  Against the oracle; no MMA wait ran out."""
+    net = _random_net(CO, 9)
+    model = _gpu_model(CL, net, cuda)
+    M, B = 120000, 100000
+    X = _features(CO, M, 10)
+    r = np.random.default_rng(11)
+    t = np.abs(r.standard_normal(M)).astype(np.float32)
+    idx = r.integers(0, M, B).astype(np.int32)
+    wt = (0.5 + r.random(M)).astype(np.float32)
+    g = model.gradient(dev(X, torch.bfloat16, cuda), dev(t, torch.float32, cuda),
+                       idx=dev(idx, torch.int32, cuda),
+                       weight=dev(wt, torch.float32, cuda)).cpu().double().numpy()
+    loss, ref = net.loss_and_grads(X[idx], t[idx].astype(np.float64), w=wt[idx])
+    assert abs(g[-1] / loss - 1) < 1e-4
+    o = {"W1": (0, 1024), "b1": (1024, 1088), "W2": (1088, 5184), "b2": (5184, 5248),
+         "w3": (5248, 5312), "b3": (5312, 5313)}
+    for name, (a, b) in o.items():
+        assert rel_l2(g[a:b], np.ravel(ref[name])) < 2e-3, name
+    # the padding columns of W1 carry no gradient
+    assert np.all(g[:1024].reshape(64, 16)[:, CO.NIN:] == 0)
+    assert sns._native.lib().sns_mlp_status() == 0
+
+
 def test_adam_step_and_training_reduce_the_loss(CO, CL, cuda):
     """One Adam step equals the textbook update of the masters; a short run
     fits a smooth synthetic target."""
