@@ -240,6 +240,8 @@ int sns_mlp_status(void);
  * (target in model units, i.e. nu_t / s_out; weight NULL = 1) over B samples
  * (rows idx[0..B) of X, target and weight, or rows 0..B when idx is NULL).
  * grad: nparams + 1 floats (gradients, then the mean loss), device memory.
+ * X and the packed model 16-byte aligned; runs on the tcgen05 tensor cores
+ * (persistent CTAs, weight gradients accumulated in tensor memory).
  * Synchronises the stream. */
 int sns_mlp_grad(const void* packed, const void* X, const float* target, const float* weight,
                  const int* idx, int64_t B, float* grad, void* stream);
