@@ -232,6 +232,16 @@ int sns_mlp_pack(const float* master, double s_in, double s_out, void* packed, v
  * on the tcgen05 tensor cores (128 points per tile, accumulators in tensor
  * memory). */
 int sns_mlp_infer(const void* packed, const void* X, int64_t M, float* nut, void* stream);
+/* Tracer particles: one move of np particles (Particle::move,
+ * src/Particle.cpp:12-46, for the whole population of exec/ns.cpp:157-203 at
+ * once).  loc: np x 3 doubles (x, y, z) in [0, 2 pi], updated in place; vel:
+ * np x 3 doubles receiving the interpolated velocity (Particle::m_v; NULL to
+ * skip); u: the three PHYSICAL velocity fields (after the inverse transform;
+ * real parts are used), nx, ny, nz >= 2.  Cell index, trilinear weights, sum
+ * order and wrap are the reference's; with complex128 fields the positions
+ * equal the reference's bit for bit.  Device pointers. */
+int sns_particles_move(double* loc, double* vel, int64_t np, const void* const u[3], int64_t nx,
+                       int64_t ny, int64_t nz, int prec, double K, void* stream);
 /* Synchronises the device; SNS_ERR_TIMEOUT (and clears the record) if a
  * tensor-core MLP kernel stopped waiting for its MMAs since the last call,
  * else SNS_OK.  No reference counterpart. */

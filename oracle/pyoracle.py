@@ -119,6 +119,9 @@ def ref(zero: bool = True):
         L.ref_ns_steps.argtypes = [C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp), _i64, _i64,
                                    _i64, C.c_double, C.c_double, C.c_int]
         L.ref_ns_steps.restype = C.c_double
+        L.ref_particles.argtypes = [C.c_uint, _i64, C.POINTER(_dp), _i64, _i64, _i64, C.c_double,
+                                    C.c_int, _dp, _dp, _dp]
+        L.ref_particles.restype = None
         _REF[key] = L
     return _REF[key]
 
@@ -313,3 +316,17 @@ def ref_ns_run(V0, omega0, nu, dt, nsteps):
                               _ptr3(V1), _ptr3(w1), _ptr3(c0),
                               divs.ctypes.data_as(_dp))
     return {"V1": V1, "omega1": w1, "cross0": c0, "div_avgs": divs[:nsteps], "seconds": el}
+
+
+def ref_particles(seed, n, u, K, nsteps):
+    """src/Particle.cpp through the reference build: srand(seed), n particles,
+    nsteps moves through the physical velocity u (three complex arrays).
+    Returns (initial positions, final positions, energies)."""
+    u = [np.ascontiguousarray(x, dtype=np.complex128) for x in u]
+    nz, ny, nx = u[0].shape
+    loc0 = np.zeros((n, 3))
+    loc = np.zeros((n, 3))
+    e = np.zeros(n)
+    d = lambda a: a.ctypes.data_as(_dp)
+    ref(True).ref_particles(seed, n, _ptr3(u), nx, ny, nz, K, nsteps, d(loc0), d(loc), d(e))
+    return loc0, loc, e

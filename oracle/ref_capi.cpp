@@ -9,9 +9,11 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 
 #include "DataObjects.H"
+#include "Particle.H"
 
 namespace {
 
@@ -296,6 +298,30 @@ double ref_ns_steps(double* const V1_io[3], double* const omega1_io[3],
   storev(omega1, omega1_io);
   storev(cross0, cross0_io);
   return el;
+}
+
+// Tracer particles of src/Particle.cpp: srand(seed), np default-constructed
+// particles (random positions), nsteps moves through the physical velocity u
+// (three complex fields); loc0 receives the initial positions, loc the final
+// ones and energy each particle's 0.5 |v|^2 after the last move (np x 3 and np
+// doubles).
+void ref_particles(unsigned seed, int64_t np, const double* const u[3], int64_t nx, int64_t ny,
+                   int64_t nz, double K, int nsteps, double* loc0, double* loc, double* energy) {
+  Vector v(dims_of(nx, ny, nz));
+  loadv(v, u);
+  srand(seed);
+  vector<Particle> parts(np);
+  for (int64_t p = 0; p < np; p++) {
+    array<double, DIM> x = parts[p].position();
+    for (int d = 0; d < DIM; d++) loc0[3 * p + d] = x[d];
+  }
+  for (int t = 0; t < nsteps; t++)
+    for (int64_t p = 0; p < np; p++) parts[p].move(v, K);
+  for (int64_t p = 0; p < np; p++) {
+    array<double, DIM> x = parts[p].position();
+    for (int d = 0; d < DIM; d++) loc[3 * p + d] = x[d];
+    energy[p] = parts[p].energy();
+  }
 }
 
 }  // extern "C"

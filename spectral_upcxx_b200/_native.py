@@ -83,6 +83,7 @@ SIGNATURES = {
     "sns_mlp_pack": ([_vp, _dbl, _dbl, _vp, _vp], _int),
     "sns_mlp_infer": ([_vp, _vp, _i64, _vp, _vp], _int),
     "sns_mlp_status": ([], _int),
+    "sns_particles_move": ([_vp, _vp, _i64, _vp3, _i64, _i64, _i64, _int, _dbl, _vp], _int),
     "sns_mlp_grad": ([_vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp], _int),
     "sns_mlp_adam": ([_vp, _vp, _vp, _vp, _int, _dbl, _dbl, _dbl, _dbl, _vp, _vp], _int),
     "sns_spectral_truncate": ([_vp3, _vp3, _int, _i64, _i64, _dbl, _int, _vp], _int),
