@@ -881,8 +881,8 @@ def closure_bench(S, torch, dev, args, world, rank, hbm, peak_src, clocks):
 
 
 def secondary(S, torch, dev, stream, n, hbm):
-    """FP64 NS step, the real-field (half-spectrum) FP32 step and 3D-FFT GB/s
-    at n^3 (short runs, device events)."""
+    """FP64 NS step, the real-field (half-spectrum) FP32 step, tracer-particle
+    moves and 3D-FFT GB/s at n^3 (short runs, device events)."""
     out = {}
     Vh = initial_velocity_hat(n, 7)
     for prec, dtype, esz in (("c128", torch.complex128, 16),):
@@ -920,6 +920,22 @@ def secondary(S, torch, dev, stream, n, hbm):
     out[f"ns{n}_c64_real_field_frac_of_30N3S"] = 30 * n ** 3 * 8 / (ms / 1e3) / 1e9 / hbm
     st.close()
     del Vd, wd
+    # tracer particles: 2^20 particles through an n^3 complex64 velocity
+    g = torch.Generator(device=dev).manual_seed(4)
+    with torch.cuda.stream(stream):
+        u = [torch.randn((n, n, n), device=dev, generator=g, dtype=torch.complex64)
+             for _ in range(3)]
+        tr = S.Tracers.uniform(1 << 20, seed=1, device=dev)
+        for _ in range(3):
+            tr.move(u, 1e-3)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(20):
+            tr.move(u, 1e-3)
+        e1.record(stream)
+    stream.synchronize()
+    out["particles_2e20_moves_per_s"] = 20 * (1 << 20) / (e0.elapsed_time(e1) / 1e3)
+    del u, tr
     for prec, dtype, esz in (("c64", torch.complex64, 8), ("c128", torch.complex128, 16)):
         g = torch.Generator(device=dev).manual_seed(2)
         with torch.cuda.stream(stream):

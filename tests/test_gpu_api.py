@@ -28,11 +28,11 @@ def _exe(name):
                                os.path.join(B.LIBDIR, "test_drivers", name + ".exe"))
 
 
-def _run(cmd, env_extra=None, timeout=600):
+def _run(cmd, env_extra=None, timeout=600, cwd=None):
     env = dict(os.environ)
     env.update(env_extra or {})
     return subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True,
-                          timeout=timeout, env=env)
+                          timeout=timeout, env=env, cwd=cwd)
 
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
@@ -81,19 +81,19 @@ def _ref_driver(name):
     return p
 
 
-def test_reference_operators_driver_unchanged(cuda):
-    r = _run([_ref_driver("operators"), "32"])
+def test_reference_operators_driver_unchanged(cuda, tmp_path):
+    r = _run([_ref_driver("operators"), "32"], cwd=tmp_path)
     assert r.returncode == 0, r.stdout
     assert r.stdout.count("passed") == 10 and "failed" not in r.stdout, r.stdout
 
 
-def test_reference_ns_driver_unchanged(cuda):
-    r = _run([_ref_driver("ns"), "32"])
+def test_reference_ns_driver_unchanged(cuda, tmp_path):
+    r = _run([_ref_driver("ns"), "32"], cwd=tmp_path)
     assert r.returncode == 0, r.stdout
     assert "Wtime" in r.stdout and "avg div" not in r.stdout, r.stdout
 
 
-def test_reference_fft_driver_unchanged(cuda):
-    r = _run([_ref_driver("fft"), "64", "3"])
+def test_reference_fft_driver_unchanged(cuda, tmp_path):
+    r = _run([_ref_driver("fft"), "64", "3"], cwd=tmp_path)
     assert r.returncode == 0, r.stdout
     assert "min time" in r.stdout, r.stdout
