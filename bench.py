@@ -71,8 +71,8 @@ WORKLOADS = {
     "fft128_c128": dict(kind="fft", n=128, prec="c128"),
     "fft256_c128": dict(kind="fft", n=256, prec="c128"),
     "fft512_c128": dict(kind="fft", n=512, prec="c128"),
-    "ens_config4": dict(kind="ens", n=128, prec="c64"),
-    "closure_config5": dict(kind="closure", n=256, prec="c64"),
+    "ens_64boxes_32_64_128": dict(kind="ens", n=128, prec="c64"),
+    "les64_closure_dns256": dict(kind="closure", n=256, prec="c64"),
 }
 # learned closure: 256^3 DNS (nu = 1/400, dt = 5e-4 as the plain benchmark)
 # filtered at kc = 21 onto 64^3; training snapshots every 5 steps of 2000 from
@@ -90,7 +90,7 @@ ENS_DT = 1e-3
 ENS_NU_RANGE = (1.0 / 800, 1.0 / 100)
 ENS_STAGES = ["S1 z-inverse+curl", "S2 y-inverse x6", "S3 x-inv+cross+x-fwd", "S4 y-forward x3",
               "S5 z-forward+update"]
-# config 3: nu = 1/400; dt = 5e-4 because the stated dt = 2e-3 makes the reference's
+# 256^3 spectrum-seeded run: nu = 1/400; dt = 5e-4 because dt = 2e-3 makes the reference's
 # AB2/CN scheme diverge at 256^3 (FP64 energy -> NaN within 75 steps)
 NU, DT = 1.0 / 400, 5e-4
 
@@ -196,7 +196,7 @@ def dist_setup(args):
 
 
 def initial_velocity_hat(n, seed):
-    """Config-3 input: spectrum-seeded solenoidal field, Fourier, Nyquist zeroed."""
+    """The 256^3 benchmark input: spectrum-seeded solenoidal field, Fourier, Nyquist zeroed."""
     from spectral_upcxx_b200 import ic
     u = ic.solenoidal_spectrum(n, seed=seed)
     h = n // 2
@@ -307,7 +307,7 @@ def run_reference(args, rank, world):
             "ms_per_step": 1000.0 * sum(c for _, c in ENS_BOXES) / cb["value"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)",
-            "config": {"workload": "ens_config4: boxes run one after another by the reference "
+            "config": {"workload": "ens_64boxes_32_64_128: boxes run one after another by the reference "
                                    "loop body", "dt": ENS_DT},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0,
@@ -529,7 +529,7 @@ def run_b200(args, rank, world, local):
                    12 * field_bytes / 1e9)}
     elif wl["kind"] == "closure":
         result.update(closure_bench(S, torch, dev, args, world, rank, hbm, peak_src, clocks))
-        cfg = {"workload": "closure_config5: %d^3 DNS (nu=1/400, dt=5e-4) sharp-spectral filtered "
+        cfg = {"workload": "les64_closure_dns256: %d^3 DNS (nu=1/400, dt=5e-4) sharp-spectral filtered "
                            "at kc=%d onto %d^3; MLP 9-64-64-1 trained on %d snapshots of %d "
                            "seeds; %d^3 runs (modes |k| <= kc) of %d held-out seeds over %d "
                            "steps" % (CLOSURE["nf"], CLOSURE["kc"], CLOSURE["nc"],
@@ -542,7 +542,7 @@ def run_b200(args, rank, world, local):
                                 barrier, max_over_ranks))
         if rank == 0 and world == 1 and not args.no_cpu:
             result["cpu_baseline"] = cpu_ens_sample()
-        cfg = {"workload": "ens_config4: 32 boxes of 32^3 + 24 of 64^3 + 8 of 128^3 "
+        cfg = {"workload": "ens_64boxes_32_64_128: 32 boxes of 32^3 + 24 of 64^3 + 8 of 128^3 "
                            "(24,117,248 points), spectrum-seeded solenoidal field per box "
                            "(distinct seeds), nu log-uniform in [1/800, 1/100], dt=1e-3 (2e-3 blows up "
                            "in the 128^3 boxes of smallest nu), complex64",
@@ -753,9 +753,10 @@ def ens_bench(S, torch, dev, stream, args, world, rank, hbm, peak_src, clocks, b
 
 
 def closure_bench(S, torch, dev, args, world, rank, hbm, peak_src, clocks):
-    """Config 5: dataset from filtered DNS, GPU training, coarse runs judged by
-    the filtered DNS energy spectrum.  value = steps/s of the 64^3 MLP-closure
-    run (device time, K steps through a CUDA-event window)."""
+    """The 64^3 closure run against filtered 256^3 DNS: dataset from the
+    filtered DNS, GPU training, coarse runs judged by the filtered DNS energy
+    spectrum.  value = steps/s of the 64^3 MLP-closure run (device time, K
+    steps through a CUDA-event window)."""
     from spectral_upcxx_b200 import closure as CL
     from spectral_upcxx_b200 import ic
     c = CLOSURE
@@ -902,7 +903,7 @@ def secondary(S, torch, dev, stream, n, hbm):
         out[f"ns{n}_{prec}_step_frac_of_hbm"] = 30 * n ** 3 * esz / (ms / 1e3) / 1e9 / hbm
         st.close()
         del Vd, wd
-    # the same config-3 step on the half spectrum of the (real) field, against
+    # the same benchmark step on the half spectrum of the (real) field, against
     # the same 30 N^3 S unit of the complex step
     with torch.cuda.stream(stream):
         Vd = [torch.from_numpy(x).to(dev, torch.complex64) for x in Vh]

@@ -43,7 +43,7 @@ def test_stepper_matches_reference_golden(sns, cuda, case, nu):
     st.close()
 
 
-def test_config1_taylor_green_64_every_field(sns, oracle, cuda):
+def test_taylor_green_64_every_field(sns, oracle, cuda):
     """64^3 Taylor-Green, nu = 0.01, dt = 1e-3, 100 steps: V1, omega1 and
     cross0 against the oracle run of the ns.cpp sequence at steps 1, 10, 100."""
     from spectral_upcxx_b200 import ic
@@ -125,7 +125,7 @@ def test_divergence_free_and_energy_monotone(sns, oracle, cuda):
     s.close()
 
 
-def test_fp32_vs_fp64_256_config3(sns, oracle, cuda):
+def test_fp32_vs_fp64_256_spectrum_seeded(sns, oracle, cuda):
     """Benchmark configuration: 256^3, nu = 1/400, 500 steps at dt = 5e-4.
     Per-field relative L2 of the complex64 path against the complex128 path,
     checked every 50 steps; energy-decay error at the end."""

@@ -98,7 +98,7 @@ def test_real_fp32_tracks_fp64(sns, cuda):
         s.close()
 
 
-def test_real_fp32_vs_fp64_256_config3(sns, cuda):
+def test_real_fp32_vs_fp64_256_spectrum_seeded(sns, cuda):
     """The benchmark configuration on the real-field stepper: 256^3, nu = 1/400,
     500 steps at dt = 5e-4, complex64 half spectrum against the complex128
     complex stepper."""
