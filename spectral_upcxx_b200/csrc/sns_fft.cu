@@ -298,6 +298,21 @@ int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int fla
   f.n = nf;
   for (int i = 0; i < nf; i++) f.in[i] = f.out[i] = fields[i];
   const double N = (double)nx * ny * nz;
+  if (!tw_axes && fft_xy_supported(nx, ny, nz, nf)) {
+    // two passes: xy planes and z lines (forward xy first, inverse z first),
+    // the epilogue on the second
+    const bool z_pass = nz > 1;
+    if (sign < 0) {
+      int rc = fft_xy_pass(f, nx, nz, sign, z_pass ? 0 : flags, 1.0 / N, prec, stream);
+      if (rc || !z_pass) return rc;
+      return run_line_pass(axis_geo(2, nx, ny, nz, prec), f, sign, flags, 1.0 / N, prec, stream);
+    }
+    if (z_pass) {
+      int rc = run_line_pass(axis_geo(2, nx, ny, nz, prec), f, sign, 0, 1.0 / N, prec, stream);
+      if (rc) return rc;
+    }
+    return fft_xy_pass(f, nx, nz, sign, flags, 1.0 / N, prec, stream);
+  }
   // axes of length 1 are identities; the epilogue rides on the last real pass
   int axes[3], na = 0;
   const int order_fwd[3] = {0, 1, 2}, order_inv[3] = {2, 1, 0};
