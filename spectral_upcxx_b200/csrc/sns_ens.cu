@@ -71,13 +71,11 @@ struct BoxCurlFields {  // K1: V in, U out
   const EnsBox* __restrict__ b;
   __device__ __forceinline__ const void* in(int i) const { return i < 3 ? b->V[i] : nullptr; }
   __device__ __forceinline__ void* out(int i) const { return b->U[i]; }
-  __device__ __forceinline__ int first() const { return 0; }
 };
 struct BoxWorkFields {  // K2, K3, K4: in place on U
   const EnsBox* __restrict__ b;
   __device__ __forceinline__ const void* in(int i) const { return b->U[i]; }
   __device__ __forceinline__ void* out(int i) const { return b->U[i]; }
-  __device__ __forceinline__ int first() const { return 0; }
 };
 
 template <typename T, int L, int STAGE>

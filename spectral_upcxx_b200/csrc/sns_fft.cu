@@ -193,15 +193,6 @@ int run_line_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags, d
       return dispatch_pass<double, PRO_CURL6>(geo, f, sign, flags, scale, stream);
     return dispatch_pass<float, PRO_CURL6>(geo, f, sign, flags, scale, stream);
   }
-  if (prologue == PRO_GRAD12) {
-    if (f.first < 0 || f.first + f.n > 12 || !f.in[0] || !f.in[1] || !f.in[2]) {
-      set_error("gradient prologue: outputs 0..11 of a vector of three fields");
-      return ERR_ARG;
-    }
-    if (prec == PREC_C128)
-      return dispatch_pass<double, PRO_GRAD12>(geo, f, sign, flags, scale, stream);
-    return dispatch_pass<float, PRO_GRAD12>(geo, f, sign, flags, scale, stream);
-  }
   if (prologue != PRO_LOAD && prologue != PRO_IKAXIS) {
     set_error("line pass: unknown prologue");
     return ERR_ARG;

@@ -24,8 +24,6 @@ enum PassPrologue : int {
   PRO_LOAD = 0,   // field f reads in[f]
   PRO_CURL6 = 1,  // in[0..2] = a Fourier vector V; fields 0..2 read V, fields
                   // 3..5 form (i k x V) on the fly (src/Vector.cpp:92-122)
-  PRO_GRAD12 = 2,  // in[0..2] = a Fourier vector V; output q = first + field is
-                   // V_q for q < 3, else i k_j V_i with q - 3 = 3 i + j
   PRO_IKAXIS = 3,  // field f reads in[f], times i k (the wavenumber along the
                    // line) when bit f of ikmask is set: a derivative along the
                    // pass axis taken on the way in
@@ -54,7 +52,6 @@ struct FieldPtrs {
   void* in[kMaxFields];
   void* out[kMaxFields];
   int n;
-  int first;        // PRO_GRAD12: output index of field 0
   unsigned ikmask;  // PRO_IKAXIS: fields whose input is multiplied by i k_axis
 };
 

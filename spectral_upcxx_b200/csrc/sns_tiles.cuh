@@ -48,22 +48,16 @@ __device__ __forceinline__ LineCoord line_coord(const LineGeo& geo, int64_t base
   return c;
 }
 
-// Element of the thread's line as the prologue forms it (q: the output index
-// of the field for PRO_GRAD12, block-uniform).
+// Element of the thread's line as the prologue forms it.
 template <int PRO, typename C, typename T>
 __device__ __forceinline__ C pro_load(const C* __restrict__ src, const C* __restrict__ v0,
                                       const C* __restrict__ v1, const C* __restrict__ v2,
-                                      int field, int q, int64_t idx, T kx, T ky, T kz) {
+                                      int field, int64_t idx, T kx, T ky, T kz) {
   if constexpr (PRO == PRO_CURL6) {
     if (field < 3) return src[idx];
     if (field == 3) return csub(ikmul(ky, v2[idx]), ikmul(kz, v1[idx]));
     if (field == 4) return csub(ikmul(kz, v0[idx]), ikmul(kx, v2[idx]));
     return csub(ikmul(kx, v1[idx]), ikmul(ky, v0[idx]));
-  } else if constexpr (PRO == PRO_GRAD12) {
-    if (q < 3) return (q == 0 ? v0 : q == 1 ? v1 : v2)[idx];
-    const int i = (q - 3) / 3, j = (q - 3) - 3 * ((q - 3) / 3);
-    const C* __restrict__ vi = i == 0 ? v0 : i == 1 ? v1 : v2;
-    return ikmul(j == 0 ? kx : j == 1 ? ky : kz, vi[idx]);
   } else {
     return src[idx];
   }
@@ -93,17 +87,15 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
 
   C v[E];
   {
-    const C* __restrict__ src =
-        PRO == PRO_GRAD12 ? nullptr : reinterpret_cast<const C*>(f.in(field));
+    const C* __restrict__ src = reinterpret_cast<const C*>(f.in(field));
     const C* __restrict__ v0 = nullptr;
     const C* __restrict__ v1 = nullptr;
     const C* __restrict__ v2 = nullptr;
-    if constexpr (PRO == PRO_CURL6 || PRO == PRO_GRAD12) {
+    if constexpr (PRO == PRO_CURL6) {
       v0 = reinterpret_cast<const C*>(f.in(0));
       v1 = reinterpret_cast<const C*>(f.in(1));
       v2 = reinterpret_cast<const C*>(f.in(2));
     }
-    const int q = PRO == PRO_GRAD12 ? f.first() + field : field;
     // wavenumbers of the line: two are fixed, the one along the axis varies
     const T kx0 = geo.kx_half ? (T)lc.x : (T)freq_i(lc.x, geo.nx),
             ky0 = (T)freq_i(lc.y, geo.ny),
@@ -118,7 +110,7 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
         const C x = src[lc.idx0 + e * lc.step];
         v[e] = ik ? ikmul(kp, x) : x;
       } else {
-        v[e] = pro_load<PRO, C>(src, v0, v1, v2, field, q, lc.idx0 + e * lc.step,
+        v[e] = pro_load<PRO, C>(src, v0, v1, v2, field, lc.idx0 + e * lc.step,
                                 geo.axis == 0 ? kp : kx0, geo.axis == 1 ? kp : ky0,
                                 geo.axis == 2 ? kp : kz0);
       }
@@ -522,7 +514,6 @@ struct ParamFields {
   const FieldPtrs& f;
   __device__ __forceinline__ const void* in(int i) const { return select_ptr(f.in, i); }
   __device__ __forceinline__ void* out(int i) const { return select_ptr(f.out, i); }
-  __device__ __forceinline__ int first() const { return f.first; }
   __device__ __forceinline__ unsigned ikmask() const { return f.ikmask; }
 };
 
