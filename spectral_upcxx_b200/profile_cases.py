@@ -1,6 +1,6 @@
 """Small, fixed workloads for profiling the kernels under ncu.
 
-    python -m spectral_upcxx_b200.profile_cases ns128|ns256|ns256r|ens|closure64|mlp
+    python -m spectral_upcxx_b200.profile_cases ns128|ns256|ns256r|ens|closure64|mlp|misc
 
 Each case builds its inputs on the device, runs a few steps of one path and
 exits; sizes keep every case to a few GB of device memory so that a full ncu
@@ -14,7 +14,8 @@ import sys
 import numpy as np
 import torch
 
-from . import NSEnsemble, NSStepper, curl, ENS_EAGER
+from . import NSEnsemble, NSStepper, Tracers, curl, ENS_EAGER
+from . import ops
 from . import _native as N
 from . import closure as CL
 from . import ic
@@ -56,6 +57,38 @@ def run(case: str) -> None:
         t = torch.rand(M, device=dev)
         m.infer(X)
         m.gradient(X, t, batch=M)
+        m.adam(1e-3)
+    elif case == "misc":
+        # the kernels outside the steppers, each launched once in this order:
+        # 3D FFT forward + inverse at 128^3 (cluster plane pass + z pass) and
+        # 256^3 (three line passes each), tracer particles, the eager
+        # operators at 128^3, the closure data kernels (256^3 -> 64^3), Adam
+        g = torch.Generator(device=dev).manual_seed(5)
+        for n in (128, 256):
+            x = torch.randn((n, n, n), device=dev, generator=g, dtype=torch.complex64)
+            ops.forward(x)
+            ops.inverse(x)
+            del x
+        u = [torch.randn((256, 256, 256), device=dev, generator=g, dtype=torch.complex64)
+             for _ in range(3)]
+        tr = Tracers.uniform(1 << 20, seed=1, device=dev)
+        tr.move(u, 1e-3)
+        del u
+        V = [torch.randn((128, 128, 128), device=dev, generator=g, dtype=torch.complex64)
+             for _ in range(3)]
+        gr = ops.gradient(V[0])
+        w = ops.curl(V)
+        cr = ops.cross(V, w)
+        dv = ops.divergence(V)
+        ops.laplacian_inverse(dv)
+        ops.average(dv)
+        del gr, w, cr, dv, V
+        Vf = [x.to(torch.complex64) for x in ic.solenoidal_spectrum_hat(256, 2, dev)]
+        Vc = CL.truncate(Vf, 64, 21)
+        CL.pad(Vc, 256)
+        CL.sgs_sample(Vf, 64, 21, 1.0)
+        CL.spectrum(Vc)
+        m = CL.MLPModel.init(0, s_in=1.0, s_out=1.0, device=dev)
         m.adam(1e-3)
     else:
         raise SystemExit(f"unknown case {case}")
