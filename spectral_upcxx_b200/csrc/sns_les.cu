@@ -19,6 +19,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <string>
 
 #include "../../include/spectral_b200.h"
@@ -26,6 +27,7 @@
 #include "sns_fft.cuh"
 #include "sns_les.cuh"
 #include "sns_mlp.cuh"
+#include "sns_tc.cuh"
 #include "sns_ops.cuh"
 #include "sns_tiles.cuh"
 
@@ -34,6 +36,30 @@ namespace sns {
 // Rows of x lines per CTA of the fused x pass: 12 fields x G rows x TPL
 // threads = 384 whatever the line length (TPL = L / 16).
 constexpr int kXlesThreads = 384;
+
+// The MLP of the x pass on tcgen05: the CTA's 512 points as four tiles of
+// 128, run by warps 0-3 (thread m owns point m of the tile): features into the
+// K-major A tile, layer 1 (one MMA, b1 through the bias columns), ReLU/BF16
+// epilogue into the layer-2 A tile, layer 2 (four MMAs + the b2 slice), output
+// epilogue; 64 tensor-memory columns per CTA, bounded mbarrier waits.
+struct __align__(128) XlesTcSmem {
+  unsigned char W1[kMlpHidden * kMlpK1 * 2];
+  unsigned char W2[kMlpHidden * kMlpHidden * 2];
+  unsigned char B2[kMlpHidden * 16 * 2];
+  unsigned char ONES[128 * 16 * 2];
+  unsigned char X[128 * kMlpK1 * 2];
+  unsigned char H[128 * kMlpHidden * 2];
+  float w3[kMlpHidden];
+  float b3, s_in, s_out;
+  uint64_t mbar;
+  uint32_t tmem;
+  int abort;
+};
+struct XlesNoSmem {};
+
+__device__ int g_xles_tc_status;  // nonzero: a tensor-core wait of k_xles ran out
+
+__device__ __forceinline__ void mlp_warps_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
 struct XlesArgs {
   FieldPtrs f;  // in: u (3), A_ij = d_j u_i (9) after the z and y inverses (lines of
@@ -61,7 +87,7 @@ __device__ __forceinline__ void closure_point(const cx_t<T> (&u)[3], const cx_t<
 }
 
 // The closure's x pass: x-inverse of the 12 fields of G rows into shared
-// memory, nu_t per point (the MLP as 16-point tiles on the tensor cores, or
+// memory, nu_t per point (the MLP as four 128-point tcgen05 tiles, or
 // Smagorinsky (Cs Delta)^2 sqrt(2 S:S) from the real gradient), u x omega and
 // tau written over the rows, x-forward of the 9 results.  Rows are
 // field-major (line = field * G + row), so the warps that hold only the
@@ -77,7 +103,8 @@ __global__ void __launch_bounds__(kXlesThreads)
   static_assert(TPL <= 32 && 12 * G * TPL == kXlesThreads, "tile shape");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* sm = reinterpret_cast<C*>(smem_raw);
-  __shared__ MlpSmem S;
+  using MS = typename std::conditional<MODEL == CLOSURE_MLP, XlesTcSmem, XlesNoSmem>::type;
+  __shared__ MS S;
   __shared__ float nus[PTS];
   const int64_t row0 = (int64_t)blockIdx.x * G;
   const int j = threadIdx.x % TPL, line = threadIdx.x / TPL;
@@ -85,7 +112,21 @@ __global__ void __launch_bounds__(kXlesThreads)
   C* row = sm + line * RS;
   pdl_trigger();
   // the model does not depend on the previous launch: load it before the wait
-  if constexpr (MODEL == CLOSURE_MLP) mlp_load_smem(a.mlp, S, threadIdx.x, blockDim.x);
+  if constexpr (MODEL == CLOSURE_MLP) {
+    mlp_tc_load_weights(a.mlp, S.W1, S.W2, S.B2, S.w3, threadIdx.x, blockDim.x);
+    mlp_tc_fill_ones(S.ONES, 128, threadIdx.x, blockDim.x);
+    if (threadIdx.x == 0) {
+      S.b3 = a.mlp->b3;
+      S.s_in = a.mlp->s_in;
+      S.s_out = a.mlp->s_out;
+      S.abort = 0;
+      tc::mbar_init(&S.mbar, 1);
+    }
+    if (threadIdx.x < 32) {
+      tc::tmem_alloc(&S.tmem, 64);
+      tc::tmem_relinquish();
+    }
+  }
   pdl_wait();
   C v[E];
   {
@@ -101,31 +142,106 @@ __global__ void __launch_bounds__(kXlesThreads)
   line_fft<L>(v, row, j, tw, (T)1);
 #pragma unroll
   for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
+  if constexpr (MODEL == CLOSURE_MLP) tc::fence_before_sync();
   __syncthreads();
+  if constexpr (MODEL == CLOSURE_MLP) tc::fence_after_sync();
 
   const T invN = (T)a.invN;
   auto at = [&](int field, int p) -> C& {
     return sm[(field * G + p / L) * RS + pad_pos(p % L)];
   };
   if constexpr (MODEL == CLOSURE_MLP) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    const float s_in = S.s_in;
-    auto feat = [&](int p, int q) -> float {
-      return (float)(at(3 + q, p).x * invN) * s_in;
-    };
-    for (int mt = warp; mt < PTS / 16; mt += kXlesThreads / 32) {
-      const int pa = 16 * mt + g, pb = pa + 8;
-      // A operand: rows = points, columns = the 9 features (zero padded to 16)
-      uint32_t xa[4];
-      xa[0] = pack_bf16(feat(pa, 2 * t), feat(pa, 2 * t + 1));
-      xa[1] = pack_bf16(feat(pb, 2 * t), feat(pb, 2 * t + 1));
-      xa[2] = t == 0 ? pack_bf16(feat(pa, 8), 0.f) : 0u;
-      xa[3] = t == 0 ? pack_bf16(feat(pb, 8), 0.f) : 0u;
-      MlpTile tile;
-      mlp_tile_forward(S, xa, tile);
-      if (t == 0) {
-        nus[pa] = S.s_out * softplus_f(tile.z[0]);
-        nus[pb] = S.s_out * softplus_f(tile.z[1]);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (warp < 4) {
+      const uint32_t tmem = S.tmem;
+      const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
+      const uint32_t sX = tc::smem_u32(S.X), sH = tc::smem_u32(S.H), sO = tc::smem_u32(S.ONES);
+      const uint32_t sW1 = tc::smem_u32(S.W1), sW2 = tc::smem_u32(S.W2),
+                     sB2 = tc::smem_u32(S.B2);
+      constexpr uint32_t id = tc::idesc_bf16(128, kMlpHidden);
+      const float s_in = S.s_in;
+      const uint32_t one2 = bf16_bits(1.f) * 0x10001u;
+      uint32_t phase = 0;
+      for (int tile = 0; tile < PTS / 128; tile++) {
+        const int p = 128 * tile + tid;
+        // features s_in Re(A_ij) / N (columns 0..8), the bias columns 9, 10 = 1
+        {
+          float fv[kMlpIn];
+#pragma unroll
+          for (int q = 0; q < kMlpIn; q++) fv[q] = (float)(at(3 + q, p).x * invN) * s_in;
+          const uint4 x0 = make_uint4(pack_bf16(fv[0], fv[1]), pack_bf16(fv[2], fv[3]),
+                                      pack_bf16(fv[4], fv[5]), pack_bf16(fv[6], fv[7]));
+          const uint4 x1 = make_uint4((bf16_bits(fv[8]) & 0xFFFFu) | (one2 & 0xFFFF0000u),
+                                      one2 & 0xFFFFu, 0u, 0u);
+          *reinterpret_cast<uint4*>(S.X + tc::kmajor_off(tid, 0, kMlpK1)) = x0;
+          *reinterpret_cast<uint4*>(S.X + tc::kmajor_off(tid, 8, kMlpK1)) = x1;
+        }
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+        mlp_warps_sync();
+        if (tid == 0) {
+          tc::fence_after_sync();
+          tc::mma_bf16(tmem, tc::sdesc(sX, 128, 16 * kMlpK1), tc::sdesc(sW1, 128, 16 * kMlpK1),
+                       id, 0);
+          tc::commit(&S.mbar);
+        }
+        if (!tc::mbar_wait(&S.mbar, phase, tc::kWaitCycles)) S.abort = 1;
+        phase ^= 1;
+        tc::fence_after_sync();
+        mlp_warps_sync();
+        if (S.abort) break;
+#pragma unroll
+        for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+          uint32_t r[16];
+          tc::tmem_ld16(tmem + lane_base + c0, r);
+          uint32_t h[8];
+#pragma unroll
+          for (int q = 0; q < 8; q++)
+            h[q] = pack_bf16(fmaxf(__uint_as_float(r[2 * q]), 0.f),
+                             fmaxf(__uint_as_float(r[2 * q + 1]), 0.f));
+          *reinterpret_cast<uint4*>(S.H + tc::kmajor_off(tid, c0, kMlpHidden)) =
+              make_uint4(h[0], h[1], h[2], h[3]);
+          *reinterpret_cast<uint4*>(S.H + tc::kmajor_off(tid, c0 + 8, kMlpHidden)) =
+              make_uint4(h[4], h[5], h[6], h[7]);
+        }
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+        mlp_warps_sync();
+        if (tid == 0) {
+          tc::fence_after_sync();
+#pragma unroll
+          for (int s = 0; s < kMlpHidden / 16; s++)
+            tc::mma_bf16(tmem, tc::sdesc(sH + 256 * s, 128, 16 * kMlpHidden),
+                         tc::sdesc(sW2 + 256 * s, 128, 16 * kMlpHidden), id, s > 0);
+          tc::mma_bf16(tmem, tc::sdesc(sO, 128, 256), tc::sdesc(sB2, 128, 256), id, 1);
+          tc::commit(&S.mbar);
+        }
+        if (!tc::mbar_wait(&S.mbar, phase, tc::kWaitCycles)) S.abort = 1;
+        phase ^= 1;
+        tc::fence_after_sync();
+        mlp_warps_sync();
+        if (S.abort) break;
+        float z = 0.f;
+#pragma unroll
+        for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+          uint32_t r[16];
+          tc::tmem_ld16(tmem + lane_base + c0, r);
+#pragma unroll
+          for (int q = 0; q < 16; q++) z += fmaxf(__uint_as_float(r[q]), 0.f) * S.w3[c0 + q];
+        }
+        nus[p] = S.s_out * softplus_f(z + S.b3);
+        tc::fence_before_sync();
+      }
+      if (S.abort) {
+        // an MMA whose wait ran out may still be in flight: one more bounded wait
+        tc::mbar_wait(&S.mbar, phase ^ 1, tc::kWaitCycles);
+        if (tid == 0) atomicExch(&g_xles_tc_status, 1);
+      }
+      tc::fence_before_sync();
+      mlp_warps_sync();
+      if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, 64);
       }
     }
     __syncthreads();
@@ -219,6 +335,18 @@ template <typename T>
 int launch_xles(const XlesArgs& a, int model, int nx, int64_t rows, cudaStream_t s) {
   return model == CLOSURE_MLP ? launch_xles_m<T, CLOSURE_MLP>(a, nx, rows, s)
                               : launch_xles_m<T, CLOSURE_SMAGORINSKY>(a, nx, rows, s);
+}
+
+int les_tc_status_take(int* timed_out) {
+  int v = 0;
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpyFromSymbol(&v, g_xles_tc_status, sizeof(int));
+  if (e == cudaSuccess && v) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbol(g_xles_tc_status, &zero, sizeof(int));
+  }
+  *timed_out = v;
+  return cuda_status(e, "les_tc_status_take");
 }
 
 int les_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* const U[kLESWork],

@@ -20,6 +20,7 @@
 #include "../../include/spectral_b200.h"
 #include "sns_common.cuh"
 #include "sns_ens.cuh"
+#include "sns_les.cuh"
 #include "sns_mlp.cuh"
 #include "sns_tc.cuh"
 
@@ -103,7 +104,7 @@ __global__ void k_mlp_pack(const float* __restrict__ w, float s_in, float s_out,
 // reads them back (ReLU, BF16) into the layer-2 A tile, layer 2 is five MMAs
 // into the same columns, and the output epilogue forms
 // s_out softplus(relu(.) . w3 + b3) per lane.  Rounding points as in the
-// mma.sync path: hidden layer 1 rounded to BF16, layer 2 kept in FP32.
+// oracle: hidden layer 1 rounded to BF16, layer 2 kept in FP32.
 constexpr int kTcRows = 128;
 constexpr int kTcCols = 64;  // tensor-memory columns: the accumulator of either layer
 
@@ -123,10 +124,6 @@ struct __align__(128) TcSmem {
 
 __device__ int g_mlp_tc_status;  // nonzero: a tensor-core wait ran out
 
-__device__ __forceinline__ uint32_t bf16_bits(float x) {
-  __nv_bfloat16 h = __float2bfloat16_rn(x);
-  return (uint32_t)*reinterpret_cast<unsigned short*>(&h);
-}
 
 __global__ void __launch_bounds__(kTcRows)
     k_mlp_infer_tc(const MlpPacked* __restrict__ P, const __nv_bfloat16* __restrict__ X,
@@ -134,38 +131,8 @@ __global__ void __launch_bounds__(kTcRows)
   extern __shared__ __align__(128) unsigned char tc_raw[];
   TcSmem& S = *reinterpret_cast<TcSmem*>(tc_raw);
   const int tid = threadIdx.x, warp = tid >> 5;
-  // weights into the K-major operand layouts, 16 bytes (8 bf16 along k) at a time
-  for (int i = tid; i < kMlpHidden * kMlpK1 / 8; i += kTcRows) {
-    const int n = i / (kMlpK1 / 8), c = i % (kMlpK1 / 8);
-    uint4 v = reinterpret_cast<const uint4*>(P->W1)[i];
-    if (c == 1) {
-      // W1 columns 9, 10 (zero in the model) carry b1 = hi + lo
-      const float b = P->b1[n];
-      const float hi = __bfloat162float(__float2bfloat16_rn(b));
-      v.x = (v.x & 0xFFFFu) | (bf16_bits(hi) << 16);
-      v.y = (v.y & 0xFFFF0000u) | bf16_bits(b - hi);
-    }
-    *reinterpret_cast<uint4*>(S.W1 + tc::kmajor_off(n, 8 * c, kMlpK1)) = v;
-  }
-  for (int i = tid; i < kMlpHidden * kMlpHidden / 8; i += kTcRows) {
-    const int n = i / (kMlpHidden / 8), c = i % (kMlpHidden / 8);
-    *reinterpret_cast<uint4*>(S.W2 + tc::kmajor_off(n, 8 * c, kMlpHidden)) =
-        reinterpret_cast<const uint4*>(P->W2)[i];
-  }
-  for (int n = tid; n < kMlpHidden; n += kTcRows) {
-    const float b = P->b2[n];
-    const float hi = __bfloat162float(__float2bfloat16_rn(b));
-    *reinterpret_cast<uint4*>(S.B2 + tc::kmajor_off(n, 0, 16)) =
-        make_uint4(bf16_bits(hi) | (bf16_bits(b - hi) << 16), 0u, 0u, 0u);
-    *reinterpret_cast<uint4*>(S.B2 + tc::kmajor_off(n, 8, 16)) = make_uint4(0u, 0u, 0u, 0u);
-    S.w3[n] = __bfloat162float(P->w3[n]);
-  }
-  {
-    const uint32_t one = bf16_bits(1.f);
-    *reinterpret_cast<uint4*>(S.ONES + tc::kmajor_off(tid, 0, 16)) =
-        make_uint4(one | (one << 16), 0u, 0u, 0u);
-    *reinterpret_cast<uint4*>(S.ONES + tc::kmajor_off(tid, 8, 16)) = make_uint4(0u, 0u, 0u, 0u);
-  }
+  mlp_tc_load_weights(P, S.W1, S.W2, S.B2, S.w3, tid, kTcRows);
+  mlp_tc_fill_ones(S.ONES, kTcRows, tid, kTcRows);
   if (tid == 0) {
     S.b3 = P->b3;
     S.s_out = P->s_out;
@@ -763,6 +730,10 @@ int sns_mlp_status(void) {
     e = cudaMemcpyToSymbol(g_mlp_tc_status, &zero, sizeof(int));
   }
   if (e != cudaSuccess) return cuda_status(e, "sns_mlp_status");
+  int w = 0;
+  int rc = les_tc_status_take(&w);
+  if (rc) return rc;
+  v |= w;
   if (v) {
     set_error("a tensor-core MLP kernel gave up waiting for its MMAs");
     return ERR_TIMEOUT;
