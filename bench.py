@@ -188,6 +188,33 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- helpers
+def make_collectives(world, device):
+    """barrier() and max_over_ranks(x) over the initialised process group
+    (any backend; no-ops for one rank).  Timings are taken per rank on the
+    device and the job's time is the slowest rank's."""
+    import torch
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return t.item()
+
+    return barrier, max_over_ranks
+
+
+def whole_job_rate(world, units_per_rank, ms):
+    """Units of all replicas per second over the slowest rank's time."""
+    return world * units_per_rank / (ms / 1e3)
+
+
 def dist_setup(args):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -398,18 +425,7 @@ def run_b200(args, rank, world, local):
     stream = torch.cuda.Stream(dev)
     clocks = ClockSampler(local)
 
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return t.item()
+    barrier, max_over_ranks = make_collectives(world, dev)
 
     result = {}
     if wl["kind"] == "ns":
@@ -443,7 +459,7 @@ def run_b200(args, rank, world, local):
         time.sleep(0.2)
         clocks.stop()
         stats = st.stats()
-        value = world * args.steps / (ms / 1e3)
+        value = whole_job_rate(world, args.steps, ms)
         # dominant kernel
         avg = [tot / max(cnt, 1) for tot, cnt in passes]
         PASS_NAMES, PASS_FIELDS = PASSES[len(avg)]
