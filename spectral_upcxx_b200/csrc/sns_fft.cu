@@ -289,7 +289,7 @@ int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int fla
   f.n = nf;
   for (int i = 0; i < nf; i++) f.in[i] = f.out[i] = fields[i];
   const double N = (double)nx * ny * nz;
-  if (!tw_axes && fft_xy_supported(nx, ny, nz, nf)) {
+  if (!tw_axes && fft_xy_supported(nx, ny, nz, nf, prec)) {
     // two passes: xy planes and z lines (forward xy first, inverse z first),
     // the epilogue on the second
     const bool z_pass = nz > 1;

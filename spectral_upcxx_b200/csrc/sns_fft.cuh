@@ -76,7 +76,7 @@ LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec, int wmax = 0);
 // x and y axes in one pass over each xy plane (thread-block clusters with
 // distributed shared memory, sns_fft_xy.cu): fft3d uses it where nx = ny =
 // 128 (measured faster there); SNS_FFT_XY=0 keeps the three line passes.
-bool fft_xy_supported(int nx, int ny, int nz, int nf);
+bool fft_xy_supported(int nx, int ny, int nz, int nf, int prec);
 int fft_xy_pass(const FieldPtrs& f, int nx, int nz, int sign, int flags, double scale, int prec,
                 cudaStream_t s);
 int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int flags,

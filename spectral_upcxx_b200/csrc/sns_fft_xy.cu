@@ -170,10 +170,48 @@ int launch_xy(const FieldPtrs& f, int nz, int sign, int flags, double scale, cud
 
 }  // namespace
 
-bool fft_xy_supported(int nx, int ny, int nz, int nf) {
+namespace {
+
+// Whether a cluster of the plane pass fits on this device (for example not
+// under a partition too small for an 8-CTA cluster): asked once per device
+// and precision.
+template <typename T, int L>
+bool clusters_fit() {
+  static int known[64] = {0};  // 0: not asked, 1: fits, 2: does not
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!known[dev & 63]) {
+    constexpr size_t smem = xy_smem_bytes<T, L>();
+    int n = 0;
+    cudaError_t e = cudaFuncSetAttribute(k_fft_xy<T, L>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(xy_cluster<L>(), 1);
+      cfg.blockDim = dim3(xy_threads<L>());
+      cfg.dynamicSmemBytes = smem;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = xy_cluster<L>();
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      e = cudaOccupancyMaxActiveClusters(&n, k_fft_xy<T, L>, &cfg);
+    }
+    if (e != cudaSuccess) cudaGetLastError();  // a refused query leaves no error behind
+    known[dev & 63] = (e == cudaSuccess && n > 0) ? 1 : 2;
+  }
+  return known[dev & 63] == 1;
+}
+
+}  // namespace
+
+bool fft_xy_supported(int nx, int ny, int nz, int nf, int prec) {
   const char* env = getenv("SNS_FFT_XY");
   if (env && env[0] == '0') return false;
-  return nx == ny && nx == 128 && nz >= 1 && (int64_t)nz * nf <= 65535;
+  if (!(nx == ny && nx == 128 && nz >= 1 && (int64_t)nz * nf <= 65535)) return false;
+  return prec == PREC_C128 ? clusters_fit<double, 128>() : clusters_fit<float, 128>();
 }
 
 int fft_xy_pass(const FieldPtrs& f, int nx, int nz, int sign, int flags, double scale, int prec,
