@@ -86,6 +86,11 @@ int sns_inverse(void* field, int64_t nx, int64_t ny, int64_t nz, int prec, void*
  * run one strided line per FFTW call; unnormalised. */
 int sns_fft1d_many(void* data, int64_t n, int64_t stride, int64_t howmany, int64_t dist,
                    int dir, int prec, void* stream);
+/* The same lines, each multiplied by `scale` after its transform: FFT1D::inverse
+ * (src/FFT1D.cpp:60-67) is dir = +1 with scale = 1/n (exact for the power-of-two
+ * n supported here, so equal to the reference's division by n). */
+int sns_fft1d_many_scaled(void* data, int64_t n, int64_t stride, int64_t howmany, int64_t dist,
+                          int dir, double scale, int prec, void* stream);
 
 /* ---- spectral operators (Fourier-space fields) ------------------------ */
 /* Scalar::zeroHighModes (src/Scalar.cpp:336-370). */
@@ -122,11 +127,15 @@ int sns_cross(const void* const a[3], const void* const b[3], void* const out[3]
  * tables live in a static array of the library (24 MiB of work space plus
  * 192 KiB of tables), which each GPU that uses this function holds until the
  * process exits.  Boxes of at most 262144 complex128 or 524288 complex64
- * points (64^3 / 64^2*128) are accepted; larger ones return SNS_ERR_ARG.
- * The first call on a device looks up the array's device address, so make it
- * before any stream capture.  All calls share the array: calls that overlap
- * on the GPU (different streams at once) race, so serialise them.  Results
- * equal sns_cross's. */
+ * points (64^3 / 64^2*128) are accepted; larger ones return SNS_ERR_ARG, and
+ * other bad arguments return what sns_cross returns for them.  The first call
+ * on a device sets up the array (its device address is looked up, which is
+ * also when the driver creates it on that GPU): make that call before another
+ * allocator reserves the device memory, where it could fail for lack of
+ * memory, and before any stream capture.  All calls share the array and it
+ * keeps the last call's contents: calls that overlap on the GPU (different
+ * streams at once) race, so serialise them.  Results agree with sns_cross's
+ * to rounding (its twiddle tables are generated on the device). */
 int sns_cross_noalloc(const void* const a[3], const void* const b[3], void* const out[3],
                       int64_t nx, int64_t ny, int64_t nz, int prec, void* stream);
 /* Scalar::average: mean of |f_i| over n values, accumulated in FP64

@@ -32,10 +32,13 @@ _dp = C.POINTER(C.c_double)
 _i64 = C.c_int64
 
 
-def build(ref: bool = False) -> None:
-    """Compile the oracle (and the in-place reference build when asked)."""
-    targets = ["all"] + (["ref"] if ref else [])
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+def build(ref: str | None = None) -> None:
+    """Compile the oracle, and the in-place build of the reference when given
+    the path of its source tree."""
+    cmd = ["make", "-s", "-C", HERE, "all"]
+    if ref:
+        cmd += ["ref", f"REF={ref}"]
+    subprocess.run(cmd, check=True)
 
 
 def _ptr(a: np.ndarray):
@@ -53,7 +56,7 @@ def lib():
     if _LIB is None:
         path = os.path.join(HERE, "_build", "liboracle.so")
         if not os.path.exists(path):
-            build(ref=False)
+            build()
         L = C.CDLL(path)
         L.orc_transform.argtypes = [_dp, _i64, _i64, _i64, C.c_int]
         L.orc_forward.argtypes = [_dp, _i64, _i64, _i64, C.c_int]

@@ -21,14 +21,21 @@ void Particle::move(const Vector& velocity, double K) {
     if (ind[d] + 1 >= dims[d]) ind[d] = dims[d] - 2;
     rd[d] = (m_loc[d] - ind[d] * h[d]) / h[d];
   }
+  // Corners in the order of the reference's sum (src/Particle.cpp:26-35): the
+  // lower z face counter-clockwise from (0,0), then the upper z face; each term
+  // is ((u * wx) * wy) * wz and the terms are added left to right, so the
+  // rounding is the reference's.
+  static const int corner[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                   {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
   for (int d = 0; d < DIM; d++) {
     const Scalar& u = velocity[d];
     double acc = 0;
     for (int c = 0; c < 8; c++) {
-      const int ox = c & 1, oy = (c >> 1) & 1, oz = (c >> 2) & 1;
-      const double w = (ox ? rd[0] : 1 - rd[0]) * (oy ? rd[1] : 1 - rd[1]) *
+      const int ox = corner[c][0], oy = corner[c][1], oz = corner[c][2];
+      const double t = u[array<INT, DIM>{ind[0] + ox, ind[1] + oy, ind[2] + oz}].real() *
+                       (ox ? rd[0] : 1 - rd[0]) * (oy ? rd[1] : 1 - rd[1]) *
                        (oz ? rd[2] : 1 - rd[2]);
-      acc += u[array<INT, DIM>{ind[0] + ox, ind[1] + oy, ind[2] + oz}].real() * w;
+      acc = c == 0 ? t : acc + t;
     }
     m_v[d] = acc;
   }

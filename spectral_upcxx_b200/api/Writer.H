@@ -14,8 +14,15 @@
 // writes nothing.  The master file is created at the first file, not in the
 // constructor, so a writer that never writes leaves no file behind.  With
 // NWRITE defined nothing is written, as in the reference.
+//
+// Final state: with the environment variable SNS_WRITER_FINAL set to a path
+// prefix, every live writer also writes its registered fields once more, at
+// upcxx::finalize() (when a driver's fields still exist), to
+// "<prefix><name>.vtk" in the same format -- whatever the write frequency, so
+// a run made with frequency 0 still leaves its last state behind.
 
 #include <fstream>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
@@ -23,6 +30,9 @@
 #include "DataObjects.H"
 
 using namespace std;
+
+// one registered field copied to the host (defined with the writer)
+struct SnsWriterField;
 
 class Writer {
  public:
@@ -32,9 +42,16 @@ class Writer {
   void add(Vector& a_vector, string a_name);
   void write();
   void setFreq(int a_f);
+  /// write the registered fields now, synchronously, to the file `fname`
+  void writeFile(const string& fname);
+  const string& name() const { return m_name; }
+  /// number of registered scalars and vectors
+  size_t fields() const { return m_scalars.size() + m_vectors.size(); }
 
  private:
   void wait_pending();
+  std::shared_ptr<vector<SnsWriterField>> collect(array<INT, DIM>& dims,
+                                                    array<INT, DIM>& pdims) const;
 
   string m_name;
   int m_count;

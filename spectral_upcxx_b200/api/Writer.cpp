@@ -6,17 +6,18 @@
 #include <cmath>
 #include <cstdio>
 #include <memory>
+#include <set>
 
 #include "sns_api_internal.H"
 
-namespace {
-
 // One field's physical values copied to the host: real parts only are kept
-struct HostField {
+struct SnsWriterField {
   string name;
   int ncomp;               // 1 (scalar) or 3 (vector)
   vector<float> values;    // point-major: ncomp values per point, x fastest
 };
+
+namespace {
 
 // Real parts of a device field (complex64 or complex128) into dst[i * stride]
 void real_parts(const Scalar& s, float* dst, int stride) {
@@ -34,7 +35,7 @@ void real_parts(const Scalar& s, float* dst, int stride) {
 }
 
 void write_vtk(const string& fname, array<INT, DIM> dims, array<INT, DIM> pdims,
-               const vector<HostField>& fields) {
+               const vector<SnsWriterField>& fields) {
   FILE* f = fopen(fname.c_str(), "w");
   if (!f) {
     std::cerr << "ERROR in Writer: cannot open " << fname << std::endl;
@@ -53,7 +54,7 @@ void write_vtk(const string& fname, array<INT, DIM> dims, array<INT, DIM> pdims,
   }
   const INT npts = pdims[0] * pdims[1] * pdims[2];
   fprintf(f, "POINT_DATA %lld\n", (long long)npts);
-  for (const HostField& h : fields) {
+  for (const SnsWriterField& h : fields) {
     if (h.ncomp == 1)
       fprintf(f, "SCALARS %s float\nLOOKUP_TABLE default\n", h.name.c_str());
     else
@@ -66,11 +67,30 @@ void write_vtk(const string& fname, array<INT, DIM> dims, array<INT, DIM> pdims,
   fclose(f);
 }
 
+// Live writers, for the final-state files written at upcxx::finalize()
+std::set<Writer*>& live_writers() {
+  static std::set<Writer*> w;
+  return w;
+}
+
 }  // namespace
 
-Writer::Writer(string name) : m_name(name), m_count(0), m_writes(0), m_f(1) {}
+extern "C" void sns_api_finalize_hooks(void) {
+  // finalize() is also reached from the error exit of the API; run once
+  static bool ran = false;
+  const char* prefix = getenv("SNS_WRITER_FINAL");
+  if (ran || !prefix || !prefix[0]) return;
+  ran = true;
+  for (Writer* w : live_writers())
+    if (w->fields() > 0) w->writeFile(string(prefix) + w->name() + ".vtk");
+}
+
+Writer::Writer(string name) : m_name(name), m_count(0), m_writes(0), m_f(1) {
+  live_writers().insert(this);
+}
 
 Writer::~Writer() {
+  live_writers().erase(this);
   wait_pending();
   if (m_out.is_open()) m_out.close();
 }
@@ -91,25 +111,18 @@ void Writer::add(Vector& a_vector, string a_name) {
 
 void Writer::setFreq(int a_f) { m_f = a_f; }
 
-void Writer::write() {
-#ifndef NWRITE
-  // the reference computes m_count++ % m_f (src/Writer.cpp:39), which faults
-  // for the m_f = 0 that exec/ns.cpp sets; a frequency <= 0 writes nothing
-  if (m_f <= 0) {
-    m_count++;
-    return;
-  }
-  if (m_count++ % m_f != 0) return;
+// Physical values of the registered fields on the host now (the caller may
+// change the fields as soon as this returns): scalars first, then vectors.
+std::shared_ptr<vector<SnsWriterField>> Writer::collect(array<INT, DIM>& dims,
+                                                   array<INT, DIM>& pdims) const {
   const size_t ns = m_scalars.size(), nv = m_vectors.size();
   if (ns + nv == 0) SNS_API_ERROR("variables list is empty");
-  const array<INT, DIM> dims = ns ? m_scalars[0]->getDims() : m_vectors[0]->getDims();
-  const array<INT, DIM> pdims = ns ? m_scalars[0]->getPDims() : m_vectors[0]->getPDims();
+  dims = ns ? m_scalars[0]->getDims() : m_vectors[0]->getDims();
+  pdims = ns ? m_scalars[0]->getPDims() : m_vectors[0]->getPDims();
   const INT npts = pdims[0] * pdims[1] * pdims[2];
-  // physical values on the host now (the caller may change the fields as
-  // soon as write() returns)
-  auto fields = std::make_shared<vector<HostField>>();
+  auto fields = std::make_shared<vector<SnsWriterField>>();
   for (size_t i = 0; i < ns; i++) {
-    HostField h{m_scalar_names[i], 1, vector<float>(npts)};
+    SnsWriterField h{m_scalar_names[i], 1, vector<float>(npts)};
     if (m_scalars[i]->isFourier()) {
       Scalar tmp;
       m_scalars[i]->inverse(tmp);
@@ -120,7 +133,7 @@ void Writer::write() {
     fields->push_back(std::move(h));
   }
   for (size_t i = 0; i < nv; i++) {
-    HostField h{m_vector_names[i], DIM, vector<float>(DIM * npts)};
+    SnsWriterField h{m_vector_names[i], DIM, vector<float>(DIM * npts)};
     if (m_vectors[i]->isFourier()) {
       Vector tmp;
       m_vectors[i]->inverse(tmp);
@@ -130,6 +143,20 @@ void Writer::write() {
     }
     fields->push_back(std::move(h));
   }
+  return fields;
+}
+
+void Writer::write() {
+#ifndef NWRITE
+  // the reference computes m_count++ % m_f (src/Writer.cpp:39), which faults
+  // for the m_f = 0 that exec/ns.cpp sets; a frequency <= 0 writes nothing
+  if (m_f <= 0) {
+    m_count++;
+    return;
+  }
+  if (m_count++ % m_f != 0) return;
+  array<INT, DIM> dims, pdims;
+  auto fields = collect(dims, pdims);
   const string fname = m_name + "0_" + to_string(m_writes++) + ".vtk";
   if (!m_out.is_open()) {
     m_out.open(m_name + ".visit");
@@ -140,4 +167,11 @@ void Writer::write() {
   wait_pending();
   m_job = thread([fname, dims, pdims, fields]() { write_vtk(fname, dims, pdims, *fields); });
 #endif
+}
+
+void Writer::writeFile(const string& fname) {
+  array<INT, DIM> dims, pdims;
+  auto fields = collect(dims, pdims);
+  wait_pending();
+  write_vtk(fname, dims, pdims, *fields);
 }

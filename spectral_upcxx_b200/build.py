@@ -106,7 +106,8 @@ def build_cpp_program(sources, out: str, extra_flags=None) -> str:
         build_library()
     srcs = [sources] if isinstance(sources, str) else list(sources)
     # the API headers fix the class layouts the program is compiled against
-    deps = srcs + [LIBPATH] + sorted(glob.glob(os.path.join(API, "*.H")))
+    deps = srcs + [LIBPATH] + sorted(glob.glob(os.path.join(API, "*.H"))) + sorted(
+        glob.glob(os.path.join(API, "upcxx", "*.hpp")))
     if _newer(out, deps):
         os.makedirs(os.path.dirname(out), exist_ok=True)
         cmd = [_cxx(), "-O2", "-std=c++17", "-w", "-DDIM=3", "-I", API, "-I", INCLUDE] + (

@@ -117,14 +117,14 @@ int pool_free(void* ptr) {
 static inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 static inline size_t esize(int prec) { return prec == PREC_C128 ? 16 : 8; }
 
-static bool check_prec(int prec) {
+bool check_prec(int prec) {
   if (prec != PREC_C64 && prec != PREC_C128) {
     set_error("precision must be SNS_C64 (0) or SNS_C128 (1)");
     return false;
   }
   return true;
 }
-static bool check_dims(int64_t nx, int64_t ny, int64_t nz) {
+bool check_dims(int64_t nx, int64_t ny, int64_t nz) {
   if (nx < 1 || ny < 1 || nz < 1 || nx > (1 << 20) || ny > (1 << 20) || nz > (1 << 20) ||
       nx * ny * nz >= ((int64_t)1 << 32)) {
     set_error("dimensions out of range");
@@ -132,7 +132,7 @@ static bool check_dims(int64_t nx, int64_t ny, int64_t nz) {
   }
   return true;
 }
-static bool nonnull(const void* p, const char* what) {
+bool nonnull(const void* p, const char* what) {
   if (!p) {
     set_error(std::string(what) + ": null pointer");
     return false;
@@ -252,6 +252,16 @@ int ns_bootstrap_fields(Dims d, int prec, double nu, double dt, const void* cons
     if ((rc = op_axpby(1.0, V0[i], dt, V[i], V[i], n, prec, s))) return rc;
   }
   return OK;
+}
+
+bool vec_ok(const void* const v[3], const char* what) {
+  if (!v) {
+    set_error(std::string(what) + ": null vector");
+    return false;
+  }
+  for (int d = 0; d < 3; d++)
+    if (!nonnull(v[d], what)) return false;
+  return true;
 }
 
 }  // namespace sns
@@ -423,13 +433,20 @@ int sns_inverse(void* field, int64_t nx, int64_t ny, int64_t nz, int prec, void*
   return sns_fft3d(field, nx, ny, nz, +1, SNS_FFT_NORMALISE, prec, stream);
 }
 
-int sns_fft1d_many(void* data, int64_t n, int64_t stride, int64_t howmany, int64_t dist,
-                   int dir, int prec, void* stream) {
+namespace {
+// howmany lines of n elements `stride` apart, `dist` between line starts,
+// transformed in place and multiplied by `scale` when it is not 1
+int fft1d_lines(void* data, int64_t n, int64_t stride, int64_t howmany, int64_t dist, int dir,
+                double scale, int prec, cudaStream_t s) {
   if (!check_prec(prec)) return ERR_ARG;
   if (!nonnull(data, "sns_fft1d_many")) return ERR_ARG;
   if (n < 1 || stride < 1 || howmany < 0 || dist < 0 || (dir != 1 && dir != -1)) {
     set_error("sns_fft1d_many: bad arguments");
     return ERR_ARG;
+  }
+  if (n == 1 && scale != 1.0 && howmany > 0) {
+    set_error("sns_fft1d_many_scaled: a scale needs lines of at least two elements");
+    return ERR_UNSUPPORTED;
   }
   if (howmany == 0 || n == 1) return OK;
   if (!line_supported(n)) {
@@ -465,7 +482,18 @@ int sns_fft1d_many(void* data, int64_t n, int64_t stride, int64_t howmany, int64
   FieldPtrs f{};
   f.n = 1;
   f.in[0] = f.out[0] = data;
-  return run_line_pass(g, f, dir, 0, 1.0, prec, S(stream));
+  return run_line_pass(g, f, dir, scale != 1.0 ? PASS_SCALE : 0, scale, prec, s);
+}
+}  // namespace
+
+int sns_fft1d_many(void* data, int64_t n, int64_t stride, int64_t howmany, int64_t dist,
+                   int dir, int prec, void* stream) {
+  return fft1d_lines(data, n, stride, howmany, dist, dir, 1.0, prec, S(stream));
+}
+
+int sns_fft1d_many_scaled(void* data, int64_t n, int64_t stride, int64_t howmany, int64_t dist,
+                          int dir, double scale, int prec, void* stream) {
+  return fft1d_lines(data, n, stride, howmany, dist, dir, scale, prec, S(stream));
 }
 
 #define SNS_DIMS_ARGS(nx, ny, nz) Dims{(int)(nx), (int)(ny), (int)(nz)}
@@ -499,15 +527,6 @@ int sns_laplacian_inverse(void* f, double a, double b, int64_t nx, int64_t ny, i
   return op_laplacian_inverse(f, a, b, SNS_DIMS_ARGS(nx, ny, nz), prec, S(stream));
 }
 
-static bool vec_ok(const void* const v[3], const char* what) {
-  if (!v) {
-    set_error(std::string(what) + ": null vector");
-    return false;
-  }
-  for (int d = 0; d < 3; d++)
-    if (!nonnull(v[d], what)) return false;
-  return true;
-}
 
 int sns_curl(const void* const v[3], void* const out[3], int64_t nx, int64_t ny, int64_t nz,
              int prec, void* stream) {

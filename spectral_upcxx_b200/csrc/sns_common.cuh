@@ -77,6 +77,13 @@ enum Status : int {
 
 int cuda_status(cudaError_t e, const char* where);
 
+// Argument checks shared by the C-ABI entry points; each sets the error text
+// and returns false on a bad argument.
+bool check_prec(int prec);
+bool check_dims(int64_t nx, int64_t ny, int64_t nz);
+bool nonnull(const void* p, const char* what);
+bool vec_ok(const void* const v[3], const char* what);
+
 // Opt a kernel into the largest dynamic shared memory that its static shared
 // memory leaves on this device.
 template <typename K>

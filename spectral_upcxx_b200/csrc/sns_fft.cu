@@ -24,31 +24,6 @@ namespace sns {
 bool is_pow2(int64_t n) { return n >= 1 && (n & (n - 1)) == 0; }
 bool line_supported(int64_t L) { return L == 1 || (is_pow2(L) && L <= kMaxLine); }
 
-// cos/sin(2 pi m / n) in FP64 with reduction of the angle to the first octant.
-static void cis_octant(int64_t m, int64_t n, double* c, double* s) {
-  m %= n;
-  if (m < 0) m += n;
-  const int64_t m8 = 8 * m;
-  const int64_t oct = m8 / n;
-  const int64_t rem = m8 - oct * n;
-  const double t = (oct & 1) ? (M_PI / 4) * ((double)(n - rem) / (double)n)
-                             : (M_PI / 4) * ((double)rem / (double)n);
-  const double ct = cos(t), st = sin(t);
-  double x, y;
-  switch (oct) {
-    case 0: x = ct; y = st; break;
-    case 1: x = st; y = ct; break;
-    case 2: x = -st; y = ct; break;
-    case 3: x = -ct; y = st; break;
-    case 4: x = -ct; y = -st; break;
-    case 5: x = -st; y = -ct; break;
-    case 6: x = st; y = -ct; break;
-    default: x = ct; y = -st; break;
-  }
-  *c = x;
-  *s = y;
-}
-
 void twiddle_host_table(int L, int prec, std::vector<unsigned char>& out) {
   std::vector<double> tab(2 * (size_t)L);
   for (int m = 0; m < L; m++) {

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 
 #include <vector>
@@ -12,6 +13,33 @@ namespace sns {
 
 constexpr int kMaxFields = 12;
 constexpr int kMaxLine = 4096;
+
+// cos and sin of 2 pi m / n in FP64, with the angle reduced to the first
+// octant so that the FP64 sine and cosine see |t| <= pi/4.  The host twiddle
+// tables and the on-device tables of the allocation-free entry point use it.
+__host__ __device__ inline void cis_octant(int64_t m, int64_t n, double* c, double* s) {
+  m %= n;
+  if (m < 0) m += n;
+  const int64_t m8 = 8 * m;
+  const int64_t oct = m8 / n;
+  const int64_t rem = m8 - oct * n;
+  const double t = (oct & 1) ? (M_PI / 4) * ((double)(n - rem) / (double)n)
+                             : (M_PI / 4) * ((double)rem / (double)n);
+  const double ct = cos(t), st = sin(t);
+  double x, y;
+  switch (oct) {
+    case 0: x = ct; y = st; break;
+    case 1: x = st; y = ct; break;
+    case 2: x = -st; y = ct; break;
+    case 3: x = -ct; y = st; break;
+    case 4: x = -ct; y = -st; break;
+    case 5: x = -st; y = -ct; break;
+    case 6: x = st; y = -ct; break;
+    default: x = ct; y = -st; break;
+  }
+  *c = x;
+  *s = y;
+}
 
 // Epilogue flags of a pass.
 enum PassFlags : int {

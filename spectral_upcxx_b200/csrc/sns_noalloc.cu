@@ -1,25 +1,35 @@
 // Vector::cross for callers that cannot allocate device memory.
 //
 // sns_cross takes its six work fields from the library's caching pool, which
-// calls cudaMalloc the first time a size is seen.  Some callers cannot let
-// that happen: a process whose device memory is already fully reserved by
-// another allocator (a framework's caching allocator holding the whole GPU,
-// or a fixed memory budget per process), or a loop that must never take the
-// driver's allocation path at an unpredictable moment.  For them,
-// sns_cross_noalloc runs the same kernels on a work area that is part of the
-// library image itself: a file-scope __device__ array, created once per GPU
-// when this file's code is first used and kept until the process exits.
+// calls cudaMalloc the first time a size is seen, and its twiddle tables from
+// a cache that does the same.  Some callers cannot let that happen: a process
+// whose device memory is already fully reserved by another allocator (a
+// framework's caching allocator holding the whole GPU, or a fixed memory
+// budget per process), or a loop that must never take the driver's
+// allocation path at an unpredictable moment.  For them, sns_cross_noalloc
+// runs the same kernels on a work area that is part of the library image
+// itself: a file-scope __device__ array, kept until the process exits.
 //
-// Because that array is a single static object, every call on a device uses
-// the same bytes: calls that run at the same time on the GPU (on different
-// streams) race with each other and must be serialised by the caller.  Each
-// call rewrites the whole part of the array it reads (work fields and
-// twiddle tables), so nothing carries over from one call to the next.
+// Set-up, once per device: the first call made with a device current looks
+// up the array's device address with cudaGetSymbolAddress (the host-side name
+// of a __device__ array is only a stand-in for it) and caches it.  Under the
+// CUDA default of lazy module loading this lookup is also when the driver
+// creates the array on that GPU, so it can fail with an out-of-memory error
+// if another allocator has already taken the whole device: make the first
+// call before that allocator reserves its memory (a warm-up call at start-up
+// does it), and before any stream capture.
+//
+// Because the array is a single static object, every call on a device uses
+// the same bytes, and the array keeps what the last call left there: calls
+// that run at the same time on the GPU (on different streams) race with each
+// other and must be serialised by the caller.  Each call rewrites every part
+// of the array it reads -- the work fields and the twiddle tables, the latter
+// generated by a kernel on the caller's stream -- so nothing carries over from
+// one call to the next.
 #include <cuda_runtime.h>
 
 #include <mutex>
 #include <string>
-#include <vector>
 
 #include "../../include/spectral_b200.h"
 #include "sns_common.cuh"
@@ -36,9 +46,22 @@ constexpr size_t kScratchBytes = kWorkBytes + 3 * kTwiddleSlot;
 
 static __device__ __align__(256) unsigned char g_cross_scratch[kScratchBytes];
 
-// Device address of g_cross_scratch on the current device.  The host-side
-// name of a __device__ array is only a stand-in, so the address is looked up
-// once per device (with that device current) and cached.
+// Twiddle table tw[m] = exp(-2 pi i m / L), m < L, computed in FP64 and
+// rounded to T: the values of the host-generated tables of the pooled path
+// (the same octant reduction; the device's FP64 sine and cosine in place of
+// the host's).
+template <typename T>
+__global__ void k_twiddle_table(T* __restrict__ out, int L) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= L) return;
+  double c, s;
+  sns::cis_octant(m, L, &c, &s);
+  out[2 * m] = (T)c;
+  out[2 * m + 1] = (T)(-s);
+}
+
+// Device address of g_cross_scratch on the current device, looked up once per
+// device with that device current and cached.
 int scratch_address(unsigned char** out) {
   static std::mutex mu;
   static void* addr[64] = {nullptr};
@@ -53,8 +76,15 @@ int scratch_address(unsigned char** out) {
   if (!addr[dev]) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_cross_scratch);
-    if (e != cudaSuccess)
-      return sns::cuda_status(e, "sns_cross_noalloc: cudaGetSymbolAddress");
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      sns::set_error(std::string("sns_cross_noalloc: the static work area (") +
+                     std::to_string(kScratchBytes) +
+                     " bytes) could not be set up on this device -- the first call must come "
+                     "before another allocator reserves the device memory: " +
+                     cudaGetErrorString(e));
+      return sns::ERR_CUDA;
+    }
     addr[dev] = p;
   }
   *out = static_cast<unsigned char*>(addr[dev]);
@@ -67,24 +97,15 @@ extern "C" int sns_cross_noalloc(const void* const a[3], const void* const b[3],
                                  void* const out[3], int64_t nx, int64_t ny, int64_t nz, int prec,
                                  void* stream) {
   using namespace sns;
-  if (prec != SNS_C64 && prec != SNS_C128) {
-    set_error("sns_cross_noalloc: precision must be SNS_C64 or SNS_C128");
+  // the argument checks and return codes of sns_cross
+  if (!check_prec(prec) || !check_dims(nx, ny, nz) || !vec_ok(a, "sns_cross_noalloc") ||
+      !vec_ok(b, "sns_cross_noalloc") || !vec_ok((const void* const*)out, "sns_cross_noalloc"))
     return ERR_ARG;
-  }
-  if (!a || !b || !out) {
-    set_error("sns_cross_noalloc: null vector");
-    return ERR_ARG;
-  }
-  for (int d = 0; d < 3; d++)
-    if (!a[d] || !b[d] || !out[d]) {
-      set_error("sns_cross_noalloc: null field pointer");
-      return ERR_ARG;
-    }
-  if (nx < 1 || ny < 1 || nz < 1 || !line_supported(nx) || !line_supported(ny) ||
-      !line_supported(nz)) {
+  if (!line_supported(nx) || !line_supported(ny) || !line_supported(nz)) {
     set_error("sns_cross_noalloc: dimensions must be powers of two up to 4096");
-    return ERR_ARG;
+    return ERR_UNSUPPORTED;
   }
+  // the one limit of its own: the size of the static work area
   const size_t esz = prec == SNS_C128 ? 16 : 8;
   const size_t n = (size_t)nx * ny * nz;
   if (6 * n * esz > kWorkBytes) {
@@ -101,16 +122,21 @@ extern "C" int sns_cross_noalloc(const void* const a[3], const void* const b[3],
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   void* work[6];
   for (int i = 0; i < 6; i++) work[i] = base + (size_t)i * n * esz;
-  // twiddle tables of the three axes, written into the static area
+  // twiddle tables of the three axes, generated into the static area
   const void* tw[3] = {nullptr, nullptr, nullptr};
   const int64_t dims[3] = {nx, ny, nz};
   for (int ax = 0; ax < 3; ax++) {
     if (dims[ax] < 2) continue;
-    std::vector<unsigned char> table;
-    twiddle_host_table((int)dims[ax], prec, table);
     unsigned char* slot = base + kWorkBytes + ax * kTwiddleSlot;
-    cudaError_t e = cudaMemcpyAsync(slot, table.data(), table.size(), cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) return cuda_status(e, "sns_cross_noalloc: twiddle upload");
+    const int L = (int)dims[ax];
+    const int threads = L < 256 ? L : 256;
+    if (prec == SNS_C128)
+      k_twiddle_table<double><<<(L + threads - 1) / threads, threads, 0, s>>>(
+          reinterpret_cast<double*>(slot), L);
+    else
+      k_twiddle_table<float><<<(L + threads - 1) / threads, threads, 0, s>>>(
+          reinterpret_cast<float*>(slot), L);
+    SNS_CHECK_LAUNCH("sns_cross_noalloc: twiddle table");
     tw[ax] = slot;
   }
   const Dims d{(int)nx, (int)ny, (int)nz};

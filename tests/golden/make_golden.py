@@ -3,7 +3,8 @@
 Runs the reference's own src/Scalar.cpp / Vector.cpp / Operators.cpp (built
 in place by ``make -C oracle ref`` against the project's UPC++ and FFTW shims)
 on small seeded inputs and stores inputs and outputs as .npz files.  Needs the
-reference tree; the fixtures are committed so the tests do not.
+reference tree (its path from $SNS_REFERENCE or BASELINE.json's
+reference_path); the fixtures are committed so the tests do not.
 
     python tests/golden/make_golden.py
 """
@@ -23,7 +24,11 @@ from spectral_upcxx_b200 import ic  # noqa: E402
 
 
 def main():
-    O.build(ref=True)
+    import __graft_entry__
+    tree = __graft_entry__.reference_tree()
+    if tree is None:
+        sys.exit("the reference source tree is needed: set SNS_REFERENCE")
+    O.build(ref=tree)
     O.ref(True).ref_set_threads(1)
     O.ref(False).ref_set_threads(1)
     out = {}

@@ -87,10 +87,111 @@ def test_reference_operators_driver_unchanged(cuda, tmp_path):
     assert r.stdout.count("passed") == 10 and "failed" not in r.stdout, r.stdout
 
 
-def test_reference_ns_driver_unchanged(cuda, tmp_path):
-    r = _run([_ref_driver("ns"), "32"], cwd=tmp_path)
+def _read_vtk_field(path, name, ncomp, npts):
+    """Values of one point-data field of a legacy-VTK ASCII file."""
+    lines = open(path).read().split("\n")
+    head = ("VECTORS " if ncomp == 3 else "SCALARS ") + name + " float"
+    i = lines.index(head) + (1 if ncomp == 3 else 2)
+    vals = np.array(" ".join(lines[i:i + npts]).split(), dtype=np.float64)
+    return vals.reshape(npts, ncomp)
+
+
+def test_reference_ns_driver_unchanged(cuda, oracle, tmp_path):
+    """The reference's exec/ns.cpp, compiled unchanged against the API, run at
+    N = 32: its printed lines (other than the wall time) equal those of the
+    reference build (oracle/_ref/ns.exe), and the final velocity, vorticity
+    and divergence it leaves behind (the writer's final-state file,
+    SNS_WRITER_FINAL) match the oracle's run of the same ns.cpp sequence:
+    vortex-tube start (ns.cpp:82-153), nu = K = 1e-3, int(0.1 / 1e-3) steps.
+    The file holds FP32 text of the physical fields, hence the 1e-6 bound."""
+    from spectral_upcxx_b200 import ic
+    n = 32
+    r = _run([_ref_driver("ns"), str(n)], {"SNS_WRITER_FINAL": str(tmp_path / "final_")},
+             cwd=tmp_path)
     assert r.returncode == 0, r.stdout
-    assert "Wtime" in r.stdout and "avg div" not in r.stdout, r.stdout
+    assert "Wtime" in r.stdout, r.stdout
+    ours = [ln for ln in r.stdout.splitlines() if "Wtime" not in ln]
+    if oracle.have_ref():
+        rr = _run([os.path.join(ROOT, "oracle", "_ref", "ns.exe"), str(n)], cwd=tmp_path)
+        assert rr.returncode == 0, rr.stdout
+        assert ours == [ln for ln in rr.stdout.splitlines() if "Wtime" not in ln]
+    final = tmp_path / "final_solution.vtk"
+    assert final.exists(), r.stdout
+    # the oracle's run of the same sequence
+    nu = K = 1e-3
+    steps = int(0.1 / 1e-3)
+    wz = oracle.forward(ic.ns_vortex_tubes(n))
+    V0 = oracle.velocity_from_vorticity_z(wz)
+    z = np.zeros_like(wz)
+    w0 = [oracle.forward(z), oracle.forward(z), wz]
+    ns = oracle.NS((n, n, n), nu, K)
+    ns.bootstrap(V0, w0)
+    for _ in range(steps):
+        ns.step()
+    st = ns.state()
+    npts = n ** 3
+    for name, key in (("velocity", "V1"), ("vorticity", "omega1")):
+        got = _read_vtk_field(final, name, 3, npts)
+        for d in range(3):
+            exp = oracle.inverse(st[key][d]).real.ravel()
+            assert rel_l2(got[:, d], exp) < 1e-6, (name, d)
+    div = _read_vtk_field(final, "div", 1, npts)[:, 0]
+    vmax = max(np.abs(oracle.inverse(c)).max() for c in st["V1"])
+    assert np.abs(div).max() < 1e-6 * vmax * n
+
+
+def test_api_fft1d_class_matches_numpy(cuda, tmp_path):
+    """FFT1D (src/FFT1D.cpp:14-101) on host and device lines: init +
+    transform(ptr, DIR), transform(ptr, N, stride, DIR), forward, inverse,
+    strided, against numpy's DFT; elements off the line stay untouched."""
+    out = tmp_path / "fft1d.bin"
+    r = _run([_exe("api_fft1d"), str(out)])
+    assert r.returncode == 0, r.stdout
+    raw = out.read_bytes()
+    off, count = 0, 0
+    while off < len(raw):
+        kase, N, stride, sign, length = np.frombuffer(raw, np.int64, 5, off)
+        off += 40
+        before = np.frombuffer(raw, np.complex128, length, off)
+        off += 16 * length
+        after = np.frombuffer(raw, np.complex128, length, off)
+        off += 16 * length
+        idx = stride * np.arange(N)
+        line = before[idx]
+        exp = np.fft.fft(line) if sign == -1 else np.fft.ifft(line) * N
+        if kase % 10 == 2:  # inverse(): divided by N
+            exp = exp / N
+        assert rel_l2(after[idx], exp) < 1e-13, (kase, N, stride)
+        mask = np.ones(length, bool)
+        mask[idx] = False
+        assert np.array_equal(after[mask], before[mask]), kase
+        count += 1
+    assert count == 16
+
+
+def test_api_particles_match_reference_bit_for_bit(cuda, oracle, tmp_path):
+    """Particle::move through the API (the host mirror of a device Vector)
+    against the reference's src/Particle.cpp built in place: same srand seed,
+    same random start, 30 moves; positions and energies equal to the last bit."""
+    if not oracle.have_ref():
+        pytest.fail("oracle/_ref is missing: build it where the reference sources are present")
+    nx, ny, nz = 16, 8, 12
+    r = np.random.default_rng(7)
+    u = [1.5 * (r.standard_normal((nz, ny, nx)) + 1j * r.standard_normal((nz, ny, nx)))
+         for _ in range(3)]
+    vel = tmp_path / "vel.bin"
+    np.concatenate([x.ravel() for x in u]).astype(np.complex128).tofile(vel)
+    out = tmp_path / "parts.bin"
+    npart, K, steps, seed = 500, 0.04, 30, 13
+    rr = _run([_exe("api_particles"), str(seed), str(npart), str(nx), str(ny), str(nz), repr(K),
+               str(steps), str(vel), str(out)])
+    assert rr.returncode == 0, rr.stdout
+    got = np.fromfile(out, np.float64)
+    loc0, loc, e = got[:3 * npart], got[3 * npart:6 * npart], got[6 * npart:]
+    r_loc0, r_loc, r_e = oracle.ref_particles(seed, npart, u, K, steps)
+    assert np.array_equal(loc0, r_loc0.ravel())
+    assert np.array_equal(loc, r_loc.ravel())
+    assert np.array_equal(e, r_e)
 
 
 def test_reference_fft_driver_unchanged(cuda, tmp_path):
