@@ -142,26 +142,16 @@ __device__ __forceinline__ void line_sync() {
 }
 
 // Transform one line in place.  On entry v[e] holds element j + TPL*e of the
-// line, on exit the transformed element with the same index.  `row` is the
-// line's padded shared-memory row (row_stride(L) elements), `tw` the length-L
-// forward twiddle table, sg = -1 forward, +1 inverse.  The first stage writes
-// the row at once, so the caller synchronises the line after its own reads of
-// the row.  Every thread of the block must call this (it may synchronise the
-// block when TPL > 32).
-//
-// BLOCK = true synchronises the whole block between stages, for layouts in
-// which the threads of a line are not confined to one warp.
-template <int L, bool BLOCK = false, typename C, typename T>
-__device__ __forceinline__ void line_fft(C (&v)[LinePlan<L>::E], C* row, int j,
-                                         const C* __restrict__ tw, T sg) {
+// line, on exit the transformed element with the same index.  Line position p
+// lives at base[idx(p)] in shared memory; `tw` is the length-L forward
+// twiddle table, sg = -1 forward, +1 inverse; `sync()` synchronises the
+// threads that share the line.  The first stage writes the line's slots at
+// once, so the caller synchronises the line after its own reads of them.
+template <int L, typename C, typename T, typename Idx, typename Sync>
+__device__ __forceinline__ void line_fft_at(C (&v)[LinePlan<L>::E], C* base, Idx idx, int j,
+                                            const C* __restrict__ tw, T sg, Sync sync) {
   using P = LinePlan<L>;
   constexpr int E = P::E, TPL = P::TPL;
-  auto sync = [] {
-    if constexpr (BLOCK)
-      __syncthreads();
-    else
-      line_sync<TPL>();
-  };
   int Ns = 1;
 #pragma unroll
   for (int s = 0; s < P::NSTAGE; s++) {
@@ -169,7 +159,7 @@ __device__ __forceinline__ void line_fft(C (&v)[LinePlan<L>::E], C* row, int j,
     const bool last = (s == P::NSTAGE - 1);
     if (s > 0) {
 #pragma unroll
-      for (int e = 0; e < E; e++) v[e] = row[pad_pos(j + TPL * e)];
+      for (int e = 0; e < E; e++) v[e] = base[idx(j + TPL * e)];
       sync();
     }
     // butterflies m = 0 .. E/R-1 of this thread
@@ -204,15 +194,31 @@ __device__ __forceinline__ void line_fft(C (&v)[LinePlan<L>::E], C* row, int j,
         for (int r = 0; r < 16; r++)
           if (r < R) v[m + (E / R) * r] = a[r];
       } else {
-        const int base = (jb / Ns) * Ns * R + (jb % Ns);
+        const int b = (jb / Ns) * Ns * R + (jb % Ns);
 #pragma unroll
         for (int r = 0; r < 16; r++)
-          if (r < R) row[pad_pos(base + r * Ns)] = a[r];
+          if (r < R) base[idx(b + r * Ns)] = a[r];
       }
     }
     if (!last) sync();
     Ns *= R;
   }
+}
+
+// line_fft_at on a padded row: position p at row[pad_pos(p)].  Every thread of
+// the block must call this (it may synchronise the block when TPL > 32).
+// BLOCK = true synchronises the whole block between stages, for layouts in
+// which the threads of a line are not confined to one warp.
+template <int L, bool BLOCK = false, typename C, typename T>
+__device__ __forceinline__ void line_fft(C (&v)[LinePlan<L>::E], C* row, int j,
+                                         const C* __restrict__ tw, T sg) {
+  line_fft_at<L>(
+      v, row, [](int p) { return pad_pos(p); }, j, tw, sg, [] {
+        if constexpr (BLOCK)
+          __syncthreads();
+        else
+          line_sync<LinePlan<L>::TPL>();
+      });
 }
 
 }  // namespace sns

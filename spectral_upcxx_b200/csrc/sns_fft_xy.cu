@@ -19,6 +19,7 @@
 // two cluster barriers and nothing to overlap them: 403 us against 325 us)
 // and fft3d keeps the line passes.
 #include "../../include/spectral_b200.h"
+#include "sns_cluster.cuh"
 #include "sns_common.cuh"
 #include "sns_fft.cuh"
 #include "sns_fft_core.cuh"
@@ -32,32 +33,6 @@ namespace {
 template <int L>
 __host__ __device__ constexpr int xy_cluster() {
   return L == 256 ? 16 : 8;
-}
-
-__device__ __forceinline__ uint32_t cluster_addr(uint32_t saddr, uint32_t rank) {
-  uint32_t r;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
-  return r;
-}
-
-__device__ __forceinline__ void cluster_sync() {
-  asm volatile(
-      "barrier.cluster.arrive.release.aligned;\n\t"
-      "barrier.cluster.wait.acquire.aligned;\n" ::
-          : "memory");
-}
-
-__device__ __forceinline__ float2 ld_cluster(uint32_t a, const float2*) {
-  float2 v;
-  asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a)
-               : "memory");
-  return v;
-}
-__device__ __forceinline__ double2 ld_cluster(uint32_t a, const double2*) {
-  double2 v;
-  asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a)
-               : "memory");
-  return v;
 }
 
 template <int L>

@@ -494,18 +494,23 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
     pl.sgs_W = Ws;
     pl.sgs_blocks = (int)(((int64_t)nx * ny) / Ws);
   }
-  // xy phase: three separate full-domain passes by default.  SNS_XY_PASSES=1
-  // selects the persistent dataflow launch (sns_xy.cu), which moves a third of
-  // the HBM bytes of the separate passes but measured slower on B200 at 256^3
-  // (1.09 vs 0.79 ms): these passes are bound by issue and latency, not HBM.
+  // xy phase: one cluster pass over each plane (sns_xyc.cu) where a cluster
+  // holds a plane's six fields (nx = ny = 128, or 256 in complex64): it moves
+  // a third of the HBM bytes of three separate full-domain passes
+  // (SNS_XYC=0 keeps the separate passes).  SNS_XY_PASSES=1 selects the
+  // persistent dataflow launch (sns_xy.cu), which moves the same bytes as the
+  // cluster pass through L2 but measured slower on B200 at 256^3 than the
+  // separate passes (1.09 vs 0.79 ms).
   const char* env = getenv("SNS_XY_PASSES");
   const bool dataflow = env && env[0] == '1';
   pl.use_xy = !real && dataflow && xy_supported(nx, ny, prec) &&
               xy_plan(pl.xy, nx, ny, nz, prec) == OK;
+  pl.use_xyc = !real && !pl.use_xy && xyc_supported(nx, ny, prec);
   // separate passes run in slabs of xy_chunk planes (SNS_XY_CHUNK; 0 = one slab)
   pl.xy_chunk = 0;
   if (const char* e = getenv("SNS_XY_CHUNK")) pl.xy_chunk = atoi(e);
-  pl.passes = (pl.use_xy || (pl.xy_chunk > 0 && pl.xy_chunk < nz)) ? 3 : 5;
+  if (pl.xy_chunk > 0 && pl.xy_chunk < nz) pl.use_xyc = false;
+  pl.passes = (pl.use_xy || pl.use_xyc || (pl.xy_chunk > 0 && pl.xy_chunk < nz)) ? 3 : 5;
   pl.lineW = lineW > 0 ? lineW : 0;
   pl.kc2 = 1e300;
   pl.sgs_klo = 0;
@@ -544,6 +549,10 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     // K2 + K3 + K4 as one persistent dataflow launch (sns_xy.cu)
     if ((rc = xy_run(pl.xy, U, sync_words, s))) return rc;
     mark();
+  } else if (pl.use_xyc) {
+    // K2 + K3 + K4 as one cluster pass over each plane (sns_xyc.cu)
+    if ((rc = xyc_run(U, nx, ny, nz, prec, s))) return rc;
+    mark();
   }
   // K2, K3, K4 on the planes [z0, z0 + pz): the passes treat the slab as an
   // nx*ny*pz field at an offset pointer (the 1/N^2 scale keeps the full N)
@@ -581,7 +590,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     }
     return OK;
   };
-  if (!pl.use_xy) {
+  if (!pl.use_xy && !pl.use_xyc) {
     if (pl.xy_chunk > 0 && pl.xy_chunk < nz) {
       // slabs of xy_chunk planes, so each slab's intermediates stay in L2
       for (int z0 = 0; z0 < nz; z0 += pl.xy_chunk)

@@ -17,6 +17,7 @@ struct NSPlan {
   int sgs_W;          // adjacent z lines per CTA of the closure update (9 fields)
   int sgs_blocks;     // its CTAs (= diagnostics partials of a closure step)
   bool use_xy;        // xy phase as one persistent dataflow launch
+  bool use_xyc;       // xy phase as one cluster pass over each plane (sns_xyc.cu)
   XYPlan xy;
   int xy_chunk;       // planes per slab of the separate xy passes (0 = all)
   int lineW;          // adjacent lines per tile of the y/z line passes (0 = default)

@@ -40,4 +40,9 @@ size_t xy_sync_words(int nz);
 // y-inverse (6 fields) + x cross + y-forward (3 fields) of U in place.
 int xy_run(const XYPlan& p, void* const U[6], int* sync_words, cudaStream_t s);
 
+// The same phase as one pass over each xy plane on a thread-block cluster
+// (sns_xyc.cu): nx = ny = 128, or 256 in complex64, where a cluster fits.
+bool xyc_supported(int nx, int ny, int prec);
+int xyc_run(void* const U[6], int nx, int ny, int nz, int prec, cudaStream_t s);
+
 }  // namespace sns

@@ -191,3 +191,33 @@ def test_xy_dataflow_and_slabs_match_separate_passes(sns, cuda, dtype, monkeypat
     for name in ("dataflow", "slabs"):
         for a, b in zip(out[name], out["separate"]):
             assert rel_l2(a, b) < tol, name
+
+
+@pytest.mark.parametrize("dtype,n", [(torch.complex128, 128), (torch.complex64, 128),
+                                     (torch.complex64, 256)])
+def test_xy_cluster_pass_matches_separate_passes(sns, cuda, dtype, n, monkeypatch):
+    """The xy phase as one thread-block-cluster pass per plane (the default
+    where a cluster holds a plane) against the three separate passes
+    (SNS_XYC=0): same line FFTs and cross product, so the same step to
+    rounding, over 3 steps of a spectrum-seeded field."""
+    from spectral_upcxx_b200 import ic
+    Vh = ic.solenoidal_spectrum_hat(n, 11, cuda)
+    out = {}
+    for name, env in (("cluster", None), ("separate", "0")):
+        monkeypatch.delenv("SNS_XYC", raising=False)
+        if env is not None:
+            monkeypatch.setenv("SNS_XYC", env)
+        Vd = [x.to(dtype) for x in Vh]
+        st = sns.NSStepper((n, n, n), 1 / 400, 5e-4, dtype)
+        assert st.launches_per_step() == (3 if name == "cluster" else 5)
+        st.bootstrap(Vd, sns.curl(Vd))
+        st.step(3)
+        assert sns._native.lib().sns_ns_check(st.h) == 0
+        out[name] = [x.to(torch.complex128) for x in st.state()["V1"]]
+        del Vd
+        st.close()
+    tol = 1e-14 if dtype == torch.complex128 else 1e-6
+    for a, b in zip(out["cluster"], out["separate"]):
+        err = (torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)).item()
+        assert err < tol, err
+    torch.cuda.empty_cache()
