@@ -43,9 +43,16 @@ FALLBACK_HBM_GBS = 6650.0
 PASSES = {
     5: (["K1 z-inverse+curl", "K2 y-inverse x6", "K3 x-inv+cross+x-fwd", "K4 y-forward x3",
          "K5 z-forward+update"], [3 + 6, 6 + 6, 6 + 3, 3 + 3, 9 + 6]),
-    3: (["K1 z-inverse+curl", "K234 xy dataflow (y-inv x6, x cross, y-fwd x3)",
+    3: (["K1 z-inverse+curl", "K234 xy %s (y-inv x6, x cross, y-fwd x3)",
          "K5 z-forward+update"], [3 + 6, 6 + 3, 9 + 6]),
 }
+
+
+def pass_names(npasses, plan):
+    """Names of the timed passes; the xy phase is named by the plan's mode."""
+    names, fields = PASSES[npasses]
+    mode = "cluster" if "xy=cluster" in plan else "dataflow" if "xy=dataflow" in plan else "slabs"
+    return [nm % mode if "%s" in nm else nm for nm in names], fields
 STEP_FIELDS = 30  # 9 FFTs x 2 + 12 for the spectral update: 30 N^3 S per step
 
 # DRAM bytes (read + write) per launch of each pass at 256^3 complex64, from the
@@ -115,19 +122,51 @@ def bf16_peak():
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during a window."""
+    """SM clock and throttle reasons sampled during a window: NVML every 2 ms
+    from a thread (so even a window of a few milliseconds holds samples), or
+    nvidia-smi every 100 ms where NVML cannot be loaded.  Reads only."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, device=None):
         self.gpu = gpu_index
-        self.samples = []
+        self.device = device
+        self.samples = []  # (time, sm_mhz, max_mhz, set of reason names)
         self.proc = None
+        self.nvml = None
+        self.stop_flag = threading.Event()
+        self.thread = None
         self.t0 = self.t1 = None
 
+    def _nvml_handle(self):
+        import pynvml as N
+        N.nvmlInit()
+        try:  # the device this process runs on, matched by PCI bus id
+            import torch
+            p = torch.cuda.get_device_properties(self.device or 0)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return N, N.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return N, N.nvmlDeviceGetHandleByIndex(self.gpu)
+
     def start(self):
+        self.stop_flag.clear()
+        try:
+            N, h = self._nvml_handle()
+            bits = {"hw_slowdown": N.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": N.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": N.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": N.nvmlClocksEventReasonSwPowerCap}
+            mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+            self.nvml = (N, h, bits, mx)
+            self.thread = threading.Thread(target=self._nvml_loop, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
@@ -136,55 +175,64 @@ class ClockSampler:
         except FileNotFoundError:
             self.proc = None
             return
-        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread = threading.Thread(target=self._smi_loop, daemon=True)
         self.thread.start()
 
-    def _read(self):
+    def _nvml_loop(self):
+        N, h, bits, mx = self.nvml
+        while not self.stop_flag.is_set():
+            try:
+                sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((time.time(), float(sm), float(mx),
+                                     {k for k, b in bits.items() if r & b}))
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def _smi_loop(self):
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
         for line in self.proc.stdout:
-            self.samples.append((time.time(), line.strip()))
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9 or num(p[1]) is None:
+                continue
+            reasons = {k for k, v in zip(self.NAMES, p[5:9])
+                       if v.lower() in ("active", "1", "yes")}
+            self.samples.append((time.time(), num(p[1]), num(p[2]), reasons))
 
     def window(self, t0, t1):
         self.t0, self.t1 = t0, t1
 
     def stop(self):
+        self.stop_flag.set()
         if self.proc is not None:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
 
     def summary(self):
-        if self.proc is None:
+        if self.nvml is None and self.proc is None:
             return None
-        rows = []
-        for t, line in self.samples:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            rows.append((t, parts))
-        inwin = [p for t, p in rows if self.t0 is not None and self.t0 <= t <= self.t1]
-        used = inwin if inwin else [p for _, p in rows]
+        inwin = [s for s in self.samples
+                 if self.t0 is not None and self.t0 <= s[0] <= self.t1]
+        used = inwin if inwin else self.samples
         if not used:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-
-        def num(x):
-            try:
-                return float(x)
-            except ValueError:
-                return None
-
-        sm = [num(p[1]) for p in used if num(p[1]) is not None]
-        mx = [num(p[2]) for p in used if num(p[2]) is not None]
         reasons = set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for p in used:
-            for name, v in zip(names, p[5:9]):
-                if v.strip().lower() in ("active", "1", "yes"):
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
-                "samples": len(used), "in_timed_window": bool(inwin)}
+        for s in used:
+            reasons |= s[3]
+        return {"sm_mhz": statistics.median(s[1] for s in used),
+                "sm_max_mhz": max(s[2] for s in used), "reasons": sorted(reasons),
+                "samples": len(used), "in_timed_window": bool(inwin),
+                "source": "nvml 2 ms" if self.nvml is not None else "nvidia-smi 100 ms"}
 
 
 # ---------------------------------------------------------------- helpers
@@ -423,7 +471,7 @@ def run_b200(args, rank, world, local):
     field_bytes = n ** 3 * esz // (2 if real else 1)
     hbm, peak_src = peaks()
     stream = torch.cuda.Stream(dev)
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(local, dev)
 
     barrier, max_over_ranks = make_collectives(world, dev)
 
@@ -462,7 +510,8 @@ def run_b200(args, rank, world, local):
         value = whole_job_rate(world, args.steps, ms)
         # dominant kernel
         avg = [tot / max(cnt, 1) for tot, cnt in passes]
-        PASS_NAMES, PASS_FIELDS = PASSES[len(avg)]
+        plan = st.describe()
+        PASS_NAMES, PASS_FIELDS = pass_names(len(avg), plan)
         top = int(np.argmax(avg))
         alg = PASS_FIELDS[top] * field_bytes
         achieved = alg / (avg[top] / 1e3) / 1e9
@@ -527,7 +576,12 @@ def run_b200(args, rank, world, local):
         torch.cuda.empty_cache()
         # ---- secondary figures (untimed for the headline)
         if not args.no_secondary and rank == 0:
-            result["secondary"] = secondary(S, torch, dev, stream, n, hbm)
+            sec = secondary(S, torch, dev, stream, n, hbm)
+            key = "closure64_mlp_steps_per_s"
+            if key in sec and not real and n == CLOSURE["nf"]:
+                # the coarse closure run against this DNS step (target 20x)
+                sec["closure64_mlp_vs_dns256_step_ratio"] = sec[key] / (1e3 / step_ms)
+            result["secondary"] = sec
         # ---- CPU baseline (rank 0, N = 1 only)
         if rank == 0 and world == 1 and not args.no_cpu:
             c0 = [np.zeros_like(Vh[0]) for _ in range(3)]
@@ -536,11 +590,15 @@ def run_b200(args, rank, world, local):
             w = [1j * (KY * Vh[2] - KZ * Vh[1]), 1j * (KZ * Vh[0] - KX * Vh[2]),
                  1j * (KX * Vh[1] - KY * Vh[0])]
             result["cpu_baseline"] = cpu_ns_sample(n, Vh, w, c0)
+            if "secondary" in result:
+                # the standalone 3D FFT on the same host cores (exec/fft.cpp)
+                result["secondary"]["fft_cpu_baseline"] = cpu_fft_sample(n)
         cfg = {"workload": f"{args.workload}: plain NS step {n}^3" +
                            (" on the real-field stepper (half spectrum)" if real else "") +
                            ", spectrum-seeded solenoidal field (seed 1+rank), nu=1/400, dt=5e-4 "
                            "(2e-3 diverges in FP64 as well)",
                "grid": f"{n}^3", "precision": wl["prec"], "parallelism": f"replicas x{world}",
+               "plan": plan,
                "l2": "no flush: 12 resident fields (%.2f GB) exceed the 126 MB L2" % (
                    12 * field_bytes / 1e9)}
     elif wl["kind"] == "closure":
@@ -984,6 +1042,77 @@ def secondary(S, torch, dev, stream, n, hbm):
         out[f"cufft{n}_{prec}_fwd_inv_gbs_comparison"] = 4 * n ** 3 * esz / (ms / 1e3) / 1e9
         del x
     torch.cuda.empty_cache()
+    # 3D FFT roofline: the line passes of one forward + inverse pair (three per
+    # transform; 2 N^3 S bytes each) against the copy peak
+    for prec, esz in (("c64", 8), ("c128", 16)):
+        gbs = out[f"fft{n}_{prec}_fwd_inv_gbs"]
+        out[f"fft{n}_{prec}_pass_frac_of_hbm"] = gbs * 6 / 4 / hbm
+    out.update(ensemble_secondary(S, torch, dev, stream, hbm))
+    out.update(closure_secondary(S, torch, dev, stream))
+    torch.cuda.empty_cache()
+    return out
+
+
+def ensemble_secondary(S, torch, dev, stream, hbm, steps=20):
+    """The ensemble workload (32 x 32^3 + 24 x 64^3 + 8 x 128^3 boxes, nu
+    log-uniform in [1/800, 1/100], dt = 1e-3) as one graph replay per ensemble
+    step with the default tiles (no tuning run), timed over `steps` steps."""
+    from spectral_upcxx_b200 import ic
+    r = np.random.default_rng(4)
+    shapes = [(m, m, m) for m, c in ENS_BOXES for _ in range(c)]
+    lo, hi = np.log(ENS_NU_RANGE[0]), np.log(ENS_NU_RANGE[1])
+    nus = list(np.exp(r.uniform(lo, hi, len(shapes))))
+    points = int(sum(np.prod(x) for x in shapes))
+    with torch.cuda.stream(stream):
+        ens = S.NSEnsemble(shapes, nus, ENS_DT, torch.complex64, tune=False, device=dev)
+        for b, sh in enumerate(shapes):
+            Vd = [x.to(torch.complex64) for x in ic.solenoidal_spectrum_hat(sh[0], 1000 + b, dev)]
+            ens.bootstrap(b, Vd, S.curl(Vd))
+        ens.step(3, S.ENS_GRAPH)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ens.step(steps, S.ENS_GRAPH)
+        e1.record(stream)
+    stream.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    finite = sum(1 for x in ens.stats() if np.isfinite(x["energy"]))
+    ens.close()
+    return {"ens_64boxes_box_steps_per_s": len(shapes) * 1e3 / ms,
+            "ens_64boxes_ensemble_steps_per_s": 1e3 / ms,
+            "ens_64boxes_step_frac_of_hbm": STEP_FIELDS * points * 8 / (ms / 1e3) / 1e9 / hbm,
+            "ens_64boxes_boxes_finite": finite}
+
+
+def closure_secondary(S, torch, dev, stream, steps=200):
+    """Step rate of the 64^3 coarse run with the MLP eddy-viscosity closure
+    (cutoff kc = 21, eddy force on the band 14..20; randomly initialised MLP
+    weights -- the step's work does not depend on their values) and of the plain
+    coarse run, device-timed."""
+    from spectral_upcxx_b200 import closure as CL
+    from spectral_upcxx_b200 import ic
+    c = CLOSURE
+    nc = c["nc"]
+    model = CL.MLPModel.init(0, s_in=1.0, s_out=1e-3, device=dev)
+    Vc0 = CL.truncate([x.to(torch.complex64) for x in ic.solenoidal_spectrum_hat(
+        nc, c["eval_seeds"][0], dev)], nc, c["kc"])
+    out = {}
+    for name in ("mlp", "plain"):
+        with torch.cuda.stream(stream):
+            st = S.NSStepper((nc, nc, nc), NU, DT, torch.complex64, device=dev)
+            if name == "mlp":
+                st.set_closure(S._native.SNS_CLOSURE_MLP, mlp=model.packed, kc=c["kc"])
+                st.set_sgs_band(14.0, 20.0)
+            else:
+                st.set_closure(S._native.SNS_CLOSURE_NONE, kc=c["kc"])
+            st.bootstrap(Vc0, S.curl(Vc0))
+            st.step(5)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st.step(steps)
+            e1.record(stream)
+        stream.synchronize()
+        out[f"closure{nc}_{name}_steps_per_s"] = steps / (e0.elapsed_time(e1) / 1e3)
+        st.close()
     return out
 
 

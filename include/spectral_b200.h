@@ -194,6 +194,12 @@ int sns_ns_stats(sns_ns* handle, double* div_avg, double* energy, double* enstro
 int sns_ns_check(sns_ns* handle);
 /* Number of kernel launches one sns_ns_step(h, 1) issues. */
 int sns_ns_launches_per_step(sns_ns* handle);
+/* The stepper's plan as text (no reference counterpart; the reference's
+ * planning is FFTW_MEASURE per line plan, src/FFT1D.cpp:18-22): the pass
+ * structure and tile shapes chosen for this box, e.g.
+ * "passes=3 xy=cluster k1=8x1 zW=16 xG=2".  Writes at most len bytes
+ * (NUL-terminated) to buf; returns the full length. */
+int sns_ns_describe(sns_ns* handle, char* buf, int len);
 /* Per-pass timing (no reference counterpart; the reference times phases with
  * CH_Timer, src/Scalar.cpp:421-617).  While enabled, every step records CUDA
  * events between its passes on the stepper's stream; enabling clears the

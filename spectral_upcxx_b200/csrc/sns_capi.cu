@@ -2,6 +2,7 @@
 // the caching device pool, and the fused NS stepper object.
 #include <cuda_runtime.h>
 #include <stdlib.h>
+#include <string.h>
 
 #include <algorithm>
 #include <map>
@@ -916,6 +917,23 @@ int sns_ns_stats(sns_ns* h, double* div_avg, double* energy, double* enstrophy, 
 int sns_ns_launches_per_step(sns_ns* h) {
   if (!nonnull(h, "sns_ns_launches_per_step")) return ERR_ARG;
   return h->cl.model != CLOSURE_NONE ? kLESLaunches : h->pl.passes;
+}
+
+int sns_ns_describe(sns_ns* h, char* buf, int len) {
+  if (!nonnull(h, "sns_ns_describe")) return ERR_ARG;
+  const NSPlan& p = h->pl;
+  const char* xy = p.use_xyc ? "cluster" : p.use_xy ? "dataflow"
+                   : (p.xy_chunk > 0 && p.xy_chunk < p.nz) ? "slabs" : "separate";
+  char tmp[256];
+  const int n = snprintf(tmp, sizeof(tmp), "passes=%d xy=%s k1=%dx%d%s zW=%d xG=%d%s",
+                         h->cl.model != CLOSURE_NONE ? kLESLaunches : p.passes, xy, p.k1W,
+                         p.k1G, p.k1_fused ? "" : " k1=split", p.zW, p.xG,
+                         p.real ? " real" : "");
+  if (buf && len > 0) {
+    strncpy(buf, tmp, (size_t)len - 1);
+    buf[len - 1] = 0;
+  }
+  return n;
 }
 
 int sns_ns_set_closure(sns_ns* h, int model, double cs_delta2, const void* mlp, double kc) {

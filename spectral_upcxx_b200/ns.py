@@ -98,6 +98,12 @@ class NSStepper:
     def launches_per_step(self) -> int:
         return N.lib().sns_ns_launches_per_step(self.h)
 
+    def describe(self) -> str:
+        """The plan chosen for this box: pass structure and tile shapes."""
+        buf = C.create_string_buffer(256)
+        N.lib().sns_ns_describe(self.h, buf, 256)
+        return buf.value.decode()
+
     def profile(self, enable: bool = True):
         """Record CUDA events between the passes of every following step."""
         N.call("sns_ns_profile", self.h, int(bool(enable)))
