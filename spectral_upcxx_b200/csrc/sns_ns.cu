@@ -494,13 +494,12 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
     pl.sgs_W = Ws;
     pl.sgs_blocks = (int)(((int64_t)nx * ny) / Ws);
   }
-  // xy phase: one cluster pass over each plane (sns_xyc.cu) where a cluster
-  // holds a plane's six fields (nx = ny = 128, or 256 in complex64): it moves
-  // a third of the HBM bytes of three separate full-domain passes
-  // (SNS_XYC=0 keeps the separate passes).  SNS_XY_PASSES=1 selects the
-  // persistent dataflow launch (sns_xy.cu), which moves the same bytes as the
-  // cluster pass through L2 but measured slower on B200 at 256^3 than the
-  // separate passes (1.09 vs 0.79 ms).
+  // xy phase: three separate full-domain passes by default.  Two fused forms
+  // move a third of their HBM bytes but measured slower on B200, the passes
+  // being bound by latency and issue rather than bytes: SNS_XYC=1 selects one
+  // thread-block-cluster pass over each plane (sns_xyc.cu; nx = ny = 128, or
+  // 256 in complex64; 1.28 vs 0.73 ms at 256^3), SNS_XY_PASSES=1 the
+  // persistent dataflow launch through L2 (sns_xy.cu; 1.09 vs 0.79 ms).
   const char* env = getenv("SNS_XY_PASSES");
   const bool dataflow = env && env[0] == '1';
   pl.use_xy = !real && dataflow && xy_supported(nx, ny, prec) &&

@@ -31,6 +31,16 @@
 // stores -- falls on 16 distinct 8-byte slots.  Arithmetic is that of the
 // separate passes (same line FFT, same twiddle tables, same cross-product
 // expression), so both give the same step.
+//
+// Measured on B200 (complex64): the pass is bound by the latency of its
+// serial phases, not by HBM.  At 256^3 seven 16-CTA clusters are resident
+// (112 SMs at one CTA each, 224 KB of shared memory) and one plane takes
+// 39 us whether one cluster or seven run: y-inverse of the six fields with
+// the stores to the row owners 15 us, x-inverse 7.2, x-forward 3.7, y-forward
+// 3.5, product exchange 2.9, cross product 1.4, the four cluster barriers
+// 3.6 us.  The phase takes 1.28 ms against 0.73 ms for the three separate
+// passes (0.158 against 0.109 ms at 128^3), so the stepper uses the separate
+// passes and this pass is opt-in (SNS_XYC=1).
 #include <stdlib.h>
 
 #include "sns_cluster.cuh"
@@ -315,7 +325,7 @@ int launch_xyc(void* const U[6], int nz, double scale2, cudaStream_t s) {
 
 bool xyc_supported(int nx, int ny, int prec) {
   const char* env = getenv("SNS_XYC");
-  if (env && env[0] == '0') return false;
+  if (!(env && env[0] == '1')) return false;
   if (nx != ny) return false;
   if (nx == 128)
     return prec == PREC_C128 ? xyc_clusters_resident<double, 128>() > 0

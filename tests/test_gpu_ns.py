@@ -196,17 +196,15 @@ def test_xy_dataflow_and_slabs_match_separate_passes(sns, cuda, dtype, monkeypat
 @pytest.mark.parametrize("dtype,n", [(torch.complex128, 128), (torch.complex64, 128),
                                      (torch.complex64, 256)])
 def test_xy_cluster_pass_matches_separate_passes(sns, cuda, dtype, n, monkeypatch):
-    """The xy phase as one thread-block-cluster pass per plane (the default
-    where a cluster holds a plane) against the three separate passes
-    (SNS_XYC=0): same line FFTs and cross product, so the same step to
-    rounding, over 3 steps of a spectrum-seeded field."""
+    """The xy phase as one thread-block-cluster pass per plane (SNS_XYC=1)
+    against the three separate passes (the default): same line FFTs and cross
+    product, so the same step to rounding, over 3 steps of a spectrum-seeded
+    field."""
     from spectral_upcxx_b200 import ic
     Vh = ic.solenoidal_spectrum_hat(n, 11, cuda)
     out = {}
-    for name, env in (("cluster", None), ("separate", "0")):
-        monkeypatch.delenv("SNS_XYC", raising=False)
-        if env is not None:
-            monkeypatch.setenv("SNS_XYC", env)
+    for name, env in (("cluster", "1"), ("separate", "0")):
+        monkeypatch.setenv("SNS_XYC", env)
         Vd = [x.to(dtype) for x in Vh]
         st = sns.NSStepper((n, n, n), 1 / 400, 5e-4, dtype)
         assert st.launches_per_step() == (3 if name == "cluster" else 5)
