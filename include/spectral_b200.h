@@ -76,6 +76,15 @@ int sns_fft3d(void* field, int64_t nx, int64_t ny, int64_t nz, int dir, int flag
 /* The same transform over up to 12 fields of equal shape in one batch. */
 int sns_fft3d_many(void* const* fields, int nfields, int64_t nx, int64_t ny, int64_t nz,
                    int dir, int flags, int prec, void* stream);
+/* Choose the plan of sns_fft3d / sns_fft3d_many for nfields fields of
+ * nx*ny*nz by measurement (the counterpart of the reference's FFTW_MEASURE
+ * planning, src/FFT1D.cpp:18-22): per axis the tile width, thread count and
+ * radix order (radix-16 stages with the remainder last or first, or radix-8
+ * stages), and for 128 x 128 planes the plane pass against two line passes.
+ * Runs on scratch fields from the pool; the choice is cached per device and
+ * shape and used by every later transform of that shape (results agree with
+ * the default plan to rounding).  SNS_TUNE=1 tunes each new shape on first use. */
+int sns_fft3d_tune(int64_t nx, int64_t ny, int64_t nz, int nfields, int prec, void* stream);
 /* Scalar::forward(): transform(-1) + zeroHighModes (src/Scalar.cpp:208-215). */
 int sns_forward(void* field, int64_t nx, int64_t ny, int64_t nz, int prec, void* stream);
 /* Scalar::inverse(): transform(+1) then divide by N (src/Scalar.cpp:217-229). */
@@ -194,10 +203,21 @@ int sns_ns_stats(sns_ns* handle, double* div_avg, double* energy, double* enstro
 int sns_ns_check(sns_ns* handle);
 /* Number of kernel launches one sns_ns_step(h, 1) issues. */
 int sns_ns_launches_per_step(sns_ns* handle);
+/* Tune the stepper's plan by measurement (no reference counterpart; the
+ * reference's planning is FFTW_MEASURE per line plan, src/FFT1D.cpp:18-22):
+ * times candidate tile shapes of each pass -- K1 z-inverse + curl tile, the
+ * y passes' run width, thread count and radix order, the x pass's rows per
+ * CTA, the update pass's width -- on the stepper's own fields (seeded data
+ * for the timing, zero again after) and keeps the fastest per pass.  Call it after create and before the first
+ * bootstrap, set_state or step (SNS_ERR_ARG otherwise); the choice is cached
+ * per device and box shape, so later steppers of the same shape reuse it
+ * without measuring.  SNS_TUNE=1 in the environment makes every sns_ns_create
+ * tune.  Tuned and untuned steppers agree to rounding. */
+int sns_ns_tune(sns_ns* handle);
 /* The stepper's plan as text (no reference counterpart; the reference's
  * planning is FFTW_MEASURE per line plan, src/FFT1D.cpp:18-22): the pass
  * structure and tile shapes chosen for this box, e.g.
- * "passes=3 xy=cluster k1=8x1 zW=16 xG=2".  Writes at most len bytes
+ * "passes=5 xy=separate k1=8x1 y=W16/T256/16-first zW=16 xG=4 tuned".  Writes at most len bytes
  * (NUL-terminated) to buf; returns the full length. */
 int sns_ns_describe(sns_ns* handle, char* buf, int len);
 /* Per-pass timing (no reference counterpart; the reference times phases with

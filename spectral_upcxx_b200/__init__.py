@@ -9,12 +9,13 @@ from . import _native
 from ._native import SNS_C64, SNS_C128, SNSError, lib
 from .ns import ENS_EAGER, ENS_GRAPH, ENS_SEQUENTIAL, NSEnsemble, NSStepper
 from .particles import Tracers
-from .ops import (average, axpby, cross, curl, divergence, fft1d_many, fft3d, forward, gradient,
-                  inverse, laplacian, laplacian_inverse, mul, vector_laplacian, zero_high_modes)
+from .ops import (average, axpby, cross, curl, divergence, fft1d_many, fft3d, fft3d_tune, forward,
+                  gradient, inverse, laplacian, laplacian_inverse, mul, vector_laplacian,
+                  zero_high_modes)
 
 __all__ = [
     "SNS_C64", "SNS_C128", "SNSError", "lib", "NSStepper", "NSEnsemble", "Tracers", "ENS_GRAPH", "ENS_EAGER",
     "ENS_SEQUENTIAL", "average", "axpby", "cross", "curl",
-    "divergence", "fft1d_many", "fft3d", "forward", "gradient", "inverse", "laplacian",
+    "divergence", "fft1d_many", "fft3d", "fft3d_tune", "forward", "gradient", "inverse", "laplacian",
     "laplacian_inverse", "mul", "vector_laplacian", "zero_high_modes",
 ]

@@ -51,6 +51,7 @@ SIGNATURES = {
     "sns_fft3d_many": ([_vp3, _int, _i64, _i64, _i64, _int, _int, _int, _vp], _int),
     "sns_forward": ([_vp, _i64, _i64, _i64, _int, _vp], _int),
     "sns_inverse": ([_vp, _i64, _i64, _i64, _int, _vp], _int),
+    "sns_fft3d_tune": ([_i64, _i64, _i64, _int, _int, _vp], _int),
     "sns_fft1d_many": ([_vp, _i64, _i64, _i64, _i64, _int, _int, _vp], _int),
     "sns_fft1d_many_scaled": ([_vp, _i64, _i64, _i64, _i64, _int, _dbl, _int, _vp], _int),
     "sns_zero_high_modes": ([_vp, _i64, _i64, _i64, _int, _vp], _int),
@@ -77,6 +78,7 @@ SIGNATURES = {
     "sns_ns_check": ([_vp], _int),
     "sns_ns_launches_per_step": ([_vp], _int),
     "sns_ns_describe": ([_vp, C.c_char_p, _int], _int),
+    "sns_ns_tune": ([_vp], _int),
     "sns_ns_profile": ([_vp, _int], _int),
     "sns_ns_pass_times": ([_vp, C.POINTER(_dbl), C.POINTER(_int), _int], _int),
     "sns_ns_set_closure": ([_vp, _int, _dbl, _vp, _dbl], _int),

@@ -487,6 +487,11 @@ int fft1d_lines(void* data, int64_t n, int64_t stride, int64_t howmany, int64_t 
 }
 }  // namespace
 
+int sns_fft3d_tune(int64_t nx, int64_t ny, int64_t nz, int nfields, int prec, void* stream) {
+  if (!check_prec(prec) || !check_dims(nx, ny, nz)) return ERR_ARG;
+  return fft3d_tune((int)nx, (int)ny, (int)nz, nfields, prec, S(stream));
+}
+
 int sns_fft1d_many(void* data, int64_t n, int64_t stride, int64_t howmany, int64_t dist,
                    int dir, int prec, void* stream) {
   return fft1d_lines(data, n, stride, howmany, dist, dir, 1.0, prec, S(stream));
@@ -660,6 +665,11 @@ int sns::ns_create(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double n
   h->stepped = false;
   // SNS_GRAPH=0 launches every step's kernels directly
   if (const char* e = getenv("SNS_GRAPH")) h->use_graph = e[0] != '0';
+  // SNS_TUNE=1: every new stepper tunes its plan (cached per device and shape)
+  if (tune_on_first_use() && (rc = sns_ns_tune(h))) {
+    sns_ns_destroy(h);
+    return rc;
+  }
   *handle = h;
   return OK;
 }
@@ -919,16 +929,79 @@ int sns_ns_launches_per_step(sns_ns* h) {
   return h->cl.model != CLOSURE_NONE ? kLESLaunches : h->pl.passes;
 }
 
+namespace {
+// Tuned plans per device and box: (device, nx, ny, nz, precision, real).
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int, int>, NSPlan> g_tuned;
+}  // namespace
+
+int sns_ns_tune(sns_ns* h) {
+  if (!nonnull(h, "sns_ns_tune")) return ERR_ARG;
+  if (h->stepped || h->eager_done) {
+    set_error("sns_ns_tune: tune a stepper before its first bootstrap, state or step");
+    return ERR_ARG;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const NSPlan& p = h->pl;
+  const auto key = std::make_tuple(dev, p.nx, p.ny, p.nz, p.prec, p.real ? 1 : 0);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      // the knobs of the cached plan; the closure settings stay this stepper's
+      NSPlan q = it->second;
+      q.kc2 = p.kc2;
+      q.sgs_klo = p.sgs_klo;
+      q.sgs_kinv = p.sgs_kinv;
+      if (q.update_blocks > p.update_blocks) {
+        void* part = nullptr;
+        int rc = pool_malloc(&part, sizeof(double) * 4 * std::max(q.update_blocks, q.sgs_blocks));
+        if (rc) return rc;
+        pool_free(h->stats_part);
+        h->stats_part = static_cast<double*>(part);
+      }
+      h->pl = q;
+      drop_graph(h);
+      return OK;
+    }
+  }
+  // room for the diagnostics of every candidate width of the update pass
+  const int max_blocks = std::max(std::max(p.update_blocks, p.sgs_blocks), p.nx * p.ny / 2);
+  void* part = nullptr;
+  int rc = pool_malloc(&part, sizeof(double) * 4 * max_blocks);
+  if (rc) return rc;
+  pool_free(h->stats_part);
+  h->stats_part = static_cast<double*>(part);
+  NSPlan q = h->pl;
+  rc = ns_tune_plan(q, h->V, h->C0, h->U, h->stats_part, max_blocks, h->sync_words, h->s);
+  if (rc) return rc;
+  // the timing steps ran on seeded data: the stepper starts from zero fields
+  for (int d = 0; d < 3; d++) {
+    const size_t bytes = esize(q.prec) * (size_t)q.nx * q.ny * q.nz;
+    if ((rc = cuda_status(cudaMemsetAsync(h->V[d], 0, bytes, h->s), "sns_ns_tune"))) return rc;
+    if ((rc = cuda_status(cudaMemsetAsync(h->C0[d], 0, bytes, h->s), "sns_ns_tune"))) return rc;
+  }
+  h->pl = q;
+  drop_graph(h);
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tuned[key] = q;
+  return OK;
+}
+
 int sns_ns_describe(sns_ns* h, char* buf, int len) {
   if (!nonnull(h, "sns_ns_describe")) return ERR_ARG;
   const NSPlan& p = h->pl;
   const char* xy = p.use_xyc ? "cluster" : p.use_xy ? "dataflow"
                    : (p.xy_chunk > 0 && p.xy_chunk < p.nz) ? "slabs" : "separate";
   char tmp[256];
-  const int n = snprintf(tmp, sizeof(tmp), "passes=%d xy=%s k1=%dx%d%s zW=%d xG=%d%s",
+  const char* ord[3] = {"16-first", "remainder-first", "radix-8"};
+  const int n = snprintf(tmp, sizeof(tmp),
+                         "passes=%d xy=%s k1=%dx%d%s y=W%d/T%d/%s zW=%d xG=%d%s%s",
                          h->cl.model != CLOSURE_NONE ? kLESLaunches : p.passes, xy, p.k1W,
-                         p.k1G, p.k1_fused ? "" : " k1=split", p.zW, p.xG,
-                         p.real ? " real" : "");
+                         p.k1G, p.k1_fused ? "" : "(split)", p.lineW, p.lineT,
+                         ord[p.lineOrd % 3], p.zW, p.xG, p.real ? " real" : "",
+                         p.tuned ? " tuned" : "");
   if (buf && len > 0) {
     strncpy(buf, tmp, (size_t)len - 1);
     buf[len - 1] = 0;

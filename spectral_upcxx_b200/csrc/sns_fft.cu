@@ -13,11 +13,13 @@
 
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "sns_fft.cuh"
 #include "sns_fft_core.cuh"
 #include "sns_tiles.cuh"
+#include "sns_ens.cuh"
 
 namespace sns {
 
@@ -62,15 +64,16 @@ const void* twiddles(int L, int prec) {
 }
 
 // One CTA per (field, tile); the tile body is in sns_tiles.cuh.
-template <typename T, int L, int PRO>
+template <typename T, int L, int PRO, int ORD = RADIX16_FIRST>
 __global__ void __launch_bounds__(MaxThreads<T>::value)
     k_line_pass(const LineGeo geo, const FieldPtrs f, const cx_t<T>* __restrict__ tw, T sg,
                 T scale, int flags, int wshift) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   pdl_trigger();
   pdl_wait();
-  line_pass_tile<T, L, PRO>(geo, ParamFields{f}, f.n, tw, sg, scale, flags, wshift,
-                            (int64_t)blockIdx.x, reinterpret_cast<cx_t<T>*>(smem_raw));
+  line_pass_tile<T, L, PRO, ParamFields, ORD>(geo, ParamFields{f}, f.n, tw, sg, scale, flags,
+                                               wshift, (int64_t)blockIdx.x,
+                                               reinterpret_cast<cx_t<T>*>(smem_raw));
 }
 
 // epilogue-only pass (used when every axis has length 1)
@@ -94,7 +97,7 @@ __global__ void k_scale_zero(const FieldPtrs f, int64_t n, int nx, int ny, int n
   }
 }
 
-template <typename T, int L, int PRO>
+template <typename T, int L, int PRO, int ORD = RADIX16_FIRST>
 static int launch_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags,
                        double scale, cudaStream_t stream) {
   using C = cx_t<T>;
@@ -106,7 +109,7 @@ static int launch_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int fla
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_set[dev & 63]) {
-    cudaError_t e = allow_max_dynamic_smem(k_line_pass<T, L, PRO>);
+    cudaError_t e = allow_max_dynamic_smem(k_line_pass<T, L, PRO, ORD>);
     if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_line_pass)");
     attr_set[dev & 63] = true;
   }
@@ -123,10 +126,24 @@ static int launch_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int fla
     set_error("line pass: grid too large");
     return ERR_UNSUPPORTED;
   }
-  cudaError_t e = launch_pdl(k_line_pass<T, L, PRO>, dim3((unsigned)blocks), dim3(threads), smem,
-                             stream, geo, f, tw, (T)sign, (T)scale, flags, wshift);
+  cudaError_t e = launch_pdl(k_line_pass<T, L, PRO, ORD>, dim3((unsigned)blocks), dim3(threads),
+                             smem, stream, geo, f, tw, (T)sign, (T)scale, flags, wshift);
   if (e != cudaSuccess) return cuda_status(e, "k_line_pass");
   return OK;
+}
+
+// Radix orders other than RADIX16_FIRST are built for the plain-load passes
+// of the line lengths where the tuner chooses among them.
+template <typename T, int L, int PRO>
+static int launch_ordered(const LineGeo& geo, const FieldPtrs& f, int sign, int flags,
+                          double scale, cudaStream_t stream) {
+  if constexpr (PRO == PRO_LOAD && L >= 64 && L <= 1024) {
+    if (geo.ord == RADIX_REM_FIRST)
+      return launch_pass<T, L, PRO, RADIX_REM_FIRST>(geo, f, sign, flags, scale, stream);
+    if (geo.ord == RADIX8)
+      return launch_pass<T, L, PRO, RADIX8>(geo, f, sign, flags, scale, stream);
+  }
+  return launch_pass<T, L, PRO>(geo, f, sign, flags, scale, stream);
 }
 
 template <typename T, int PRO>
@@ -138,11 +155,11 @@ static int dispatch_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int f
     case 8: return launch_pass<T, 8, PRO>(geo, f, sign, flags, scale, stream);
     case 16: return launch_pass<T, 16, PRO>(geo, f, sign, flags, scale, stream);
     case 32: return launch_pass<T, 32, PRO>(geo, f, sign, flags, scale, stream);
-    case 64: return launch_pass<T, 64, PRO>(geo, f, sign, flags, scale, stream);
-    case 128: return launch_pass<T, 128, PRO>(geo, f, sign, flags, scale, stream);
-    case 256: return launch_pass<T, 256, PRO>(geo, f, sign, flags, scale, stream);
-    case 512: return launch_pass<T, 512, PRO>(geo, f, sign, flags, scale, stream);
-    case 1024: return launch_pass<T, 1024, PRO>(geo, f, sign, flags, scale, stream);
+    case 64: return launch_ordered<T, 64, PRO>(geo, f, sign, flags, scale, stream);
+    case 128: return launch_ordered<T, 128, PRO>(geo, f, sign, flags, scale, stream);
+    case 256: return launch_ordered<T, 256, PRO>(geo, f, sign, flags, scale, stream);
+    case 512: return launch_ordered<T, 512, PRO>(geo, f, sign, flags, scale, stream);
+    case 1024: return launch_ordered<T, 1024, PRO>(geo, f, sign, flags, scale, stream);
     case 2048: return launch_pass<T, 2048, PRO>(geo, f, sign, flags, scale, stream);
     case 4096: return launch_pass<T, 4096, PRO>(geo, f, sign, flags, scale, stream);
     default:
@@ -189,7 +206,8 @@ int run_line_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags, d
 static int elems_per_thread(int L) { return L >= 16 ? 16 : L; }
 
 // Choose W adjacent lines and G groups for a pass of line length L.
-static void choose_tile(LineGeo& g, int64_t adjacent, int64_t groups, int prec, int wmax) {
+static void choose_tile(LineGeo& g, int64_t adjacent, int64_t groups, int prec, int wmax,
+                        int tmax) {
   const int TPL = g.L / elems_per_thread(g.L);
   const size_t esz = prec == PREC_C128 ? 16 : 8;
   const size_t smem_cap = 200 * 1024;
@@ -205,15 +223,21 @@ static void choose_tile(LineGeo& g, int64_t adjacent, int64_t groups, int prec, 
          (size_t)(W * 2) * tile_stride(g.L, W * 2) * esz <= smem_cap)
     W *= 2;
   int G = 1;
-  while (W * G * 2 * TPL <= 256 && groups % (G * 2) == 0 &&
+  const int tcap = tmax > 0 ? tmax : 256;  // threads per CTA up to which groups are added
+  while (W * G * 2 * TPL <= tcap && W * G * 2 * TPL <= max_threads(prec) &&
+         groups % (G * 2) == 0 &&
          (size_t)(W * G * 2) * tile_stride(g.L, W) * esz <= smem_cap / 2)
     G *= 2;
   g.W = W;
   g.G = G;
 }
 
-LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec, int wmax) {
+LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec, int wmax, int tmax, int ord) {
   LineGeo g{};
+  // radix-order override for tests and sweeps (SNS_RADIX_ORDER = 0, 1, 2)
+  if (ord == 0)
+    if (const char* e = getenv("SNS_RADIX_ORDER")) ord = atoi(e) % kRadixOrders;
+  g.ord = ord;
   g.nx = nx;
   g.axis = axis;
   g.ny = ny;
@@ -223,7 +247,7 @@ LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec, int wmax) {
     g.L = nx;
     g.ps = 1;
     g.gs = nx;
-    choose_tile(g, 1, (int64_t)ny * nz, prec, wmax);
+    choose_tile(g, 1, (int64_t)ny * nz, prec, wmax, tmax);
     g.TA = (int64_t)ny * nz / g.G;
     g.TB = 1;
     g.sa = (int64_t)g.G * nx;
@@ -232,7 +256,7 @@ LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec, int wmax) {
     g.L = ny;
     g.ps = nx;
     g.gs = nxy;
-    choose_tile(g, nx, nz, prec, wmax);
+    choose_tile(g, nx, nz, prec, wmax, tmax);
     g.TA = nx / g.W;
     g.TB = nz / g.G;
     g.sa = g.W;
@@ -241,7 +265,7 @@ LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec, int wmax) {
     g.L = nz;
     g.ps = nxy;
     g.gs = nx;
-    choose_tile(g, nx, ny, prec, wmax);
+    choose_tile(g, nx, ny, prec, wmax, tmax);
     g.TA = nx / g.W;
     g.TB = ny / g.G;
     g.sa = g.W;
@@ -264,17 +288,34 @@ int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int fla
   f.n = nf;
   for (int i = 0; i < nf; i++) f.in[i] = f.out[i] = fields[i];
   const double N = (double)nx * ny * nz;
-  if (!tw_axes && fft_xy_supported(nx, ny, nz, nf, prec)) {
+  // a tuned plan of this shape (callers that pass their own twiddle tables
+  // keep the default plan and never trigger a tuning run)
+  FftChoice tc{};
+  bool tuned = false;
+  if (!tw_axes) {
+    tuned = fft3d_tuned(nx, ny, nz, nf, prec, &tc);
+    if (!tuned && tune_on_first_use()) {
+      int rc = fft3d_tune(nx, ny, nz, nf, prec, stream);
+      if (rc) return rc;
+      tuned = fft3d_tuned(nx, ny, nz, nf, prec, &tc);
+    }
+  }
+  auto geo = [&](int axis) {
+    return tuned ? axis_geo(axis, nx, ny, nz, prec, tc.wmax[axis], tc.tmax[axis], tc.ord[axis])
+                 : axis_geo(axis, nx, ny, nz, prec);
+  };
+  const bool plane = tuned ? tc.plane : true;
+  if (!tw_axes && plane && fft_xy_supported(nx, ny, nz, nf, prec)) {
     // two passes: xy planes and z lines (forward xy first, inverse z first),
     // the epilogue on the second
     const bool z_pass = nz > 1;
     if (sign < 0) {
       int rc = fft_xy_pass(f, nx, nz, sign, z_pass ? 0 : flags, 1.0 / N, prec, stream);
       if (rc || !z_pass) return rc;
-      return run_line_pass(axis_geo(2, nx, ny, nz, prec), f, sign, flags, 1.0 / N, prec, stream);
+      return run_line_pass(geo(2), f, sign, flags, 1.0 / N, prec, stream);
     }
     if (z_pass) {
-      int rc = run_line_pass(axis_geo(2, nx, ny, nz, prec), f, sign, 0, 1.0 / N, prec, stream);
+      int rc = run_line_pass(geo(2), f, sign, 0, 1.0 / N, prec, stream);
       if (rc) return rc;
     }
     return fft_xy_pass(f, nx, nz, sign, flags, 1.0 / N, prec, stream);
@@ -287,7 +328,7 @@ int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int fla
   for (int i = 0; i < 3; i++)
     if (dims[order[i]] > 1) axes[na++] = order[i];
   for (int i = 0; i < na; i++) {
-    LineGeo g = axis_geo(axes[i], nx, ny, nz, prec);
+    LineGeo g = geo(axes[i]);
     if (tw_axes) g.tw = tw_axes[axes[i]];
     int fl = (i == na - 1) ? flags : 0;
     int rc = run_line_pass(g, f, sign, fl, 1.0 / N, prec, stream);
@@ -302,6 +343,147 @@ int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int fla
       k_scale_zero<float><<<grid, 256, 0, stream>>>(f, n, nx, ny, nz, (float)(1.0 / N), flags);
     SNS_CHECK_LAUNCH("k_scale_zero");
   }
+  return OK;
+}
+
+namespace {
+
+std::mutex g_fft_tune_mu;
+std::map<std::tuple<int, int, int, int, int, int>, FftChoice> g_fft_tuned;
+
+std::tuple<int, int, int, int, int, int> fft_key(int nx, int ny, int nz, int nf, int prec) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return std::make_tuple(dev, nx, ny, nz, nf, prec);
+}
+
+}  // namespace
+
+bool tune_on_first_use() {
+  static const bool on = [] {
+    const char* e = getenv("SNS_TUNE");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+bool fft3d_tuned(int nx, int ny, int nz, int nf, int prec, FftChoice* out) {
+  std::lock_guard<std::mutex> lock(g_fft_tune_mu);
+  auto it = g_fft_tuned.find(fft_key(nx, ny, nz, nf, prec));
+  if (it == g_fft_tuned.end()) return false;
+  *out = it->second;
+  return true;
+}
+
+int fft3d_tune(int nx, int ny, int nz, int nf, int prec, cudaStream_t stream) {
+  if (nx < 1 || ny < 1 || nz < 1 || nf < 1 || nf > kMaxFields) {
+    set_error("fft3d_tune: bad dimensions or field count");
+    return ERR_ARG;
+  }
+  if (!line_supported(nx) || !line_supported(ny) || !line_supported(nz)) {
+    set_error("fft3d_tune: dimensions must be powers of two up to 4096");
+    return ERR_UNSUPPORTED;
+  }
+  const size_t bytes = (prec == PREC_C128 ? 16 : 8) * (size_t)nx * ny * nz;
+  void* fld[kMaxFields] = {nullptr};
+  int rc = OK;
+  for (int i = 0; i < nf && rc == OK; i++) {
+    rc = pool_malloc(&fld[i], bytes);
+    if (rc == OK) rc = cuda_status(cudaMemsetAsync(fld[i], 0, bytes, stream), "fft3d_tune");
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (rc == OK) rc = cuda_status(cudaEventCreate(&e0), "fft3d_tune");
+  if (rc == OK) rc = cuda_status(cudaEventCreate(&e1), "fft3d_tune");
+  FieldPtrs f{};
+  f.n = nf;
+  for (int i = 0; i < nf; i++) f.in[i] = f.out[i] = fld[i];
+  // least time of `reps` forward + inverse applications of a launch sequence
+  auto timed = [&](auto&& launch, float* out) -> int {
+    float best = 3.4e38f;
+    for (int r = 0; r < 4; r++) {
+      int e = cuda_status(cudaEventRecord(e0, stream), "fft3d_tune");
+      if (!e) e = launch(-1);
+      if (!e) e = launch(+1);
+      if (!e) e = cuda_status(cudaEventRecord(e1, stream), "fft3d_tune");
+      if (!e) e = cuda_status(cudaEventSynchronize(e1), "fft3d_tune");
+      if (e) return e;
+      float t = 0;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (r) best = std::min(best, t);  // the first run sets the kernels up
+    }
+    *out = best;
+    return OK;
+  };
+  FftChoice c{};
+  for (int a = 0; a < 3; a++) {
+    c.wmax[a] = 0;
+    c.tmax[a] = 0;
+    c.ord[a] = 0;
+  }
+  c.plane = false;
+  const int dims[3] = {nx, ny, nz};
+  for (int a = 0; a < 3 && rc == OK; a++) {
+    if (dims[a] < 2) continue;
+    // run width (y, z) and thread cap, then radix order, of this axis's pass
+    float best = 3.4e38f;
+    FftChoice bc = c;
+    for (int W : {4, 8, 16})
+      for (int T : {128, 256, 512}) {
+        if (a == 0 && W != 16) continue;  // x lines are single lines
+        FftChoice q = c;
+        q.wmax[a] = W;
+        q.tmax[a] = T;
+        float t = 0;
+        rc = timed([&](int sg) {
+          return run_line_pass(axis_geo(a, nx, ny, nz, prec, q.wmax[a], q.tmax[a], q.ord[a]), f,
+                               sg, 0, 1.0, prec, stream);
+        }, &t);
+        if (rc) break;
+        if (t < best) {
+          best = t;
+          bc = q;
+        }
+      }
+    c = bc;
+    if (rc == OK && dims[a] >= 64 && dims[a] <= 1024) {
+      for (int o = 1; o < kRadixOrders && rc == OK; o++) {
+        FftChoice q = c;
+        q.ord[a] = o;
+        float t = 0;
+        rc = timed([&](int sg) {
+          return run_line_pass(axis_geo(a, nx, ny, nz, prec, q.wmax[a], q.tmax[a], q.ord[a]), f,
+                               sg, 0, 1.0, prec, stream);
+        }, &t);
+        if (rc == OK && t < best) {
+          best = t;
+          bc = q;
+        }
+      }
+      c = bc;
+    }
+  }
+  // the xy plane pass against the tuned x and y line passes
+  if (rc == OK && fft_xy_supported(nx, ny, nz, nf, prec)) {
+    float t_lines = 0, t_plane = 0;
+    rc = timed([&](int sg) {
+      int e = run_line_pass(axis_geo(0, nx, ny, nz, prec, c.wmax[0], c.tmax[0], c.ord[0]), f, sg,
+                            0, 1.0, prec, stream);
+      if (!e)
+        e = run_line_pass(axis_geo(1, nx, ny, nz, prec, c.wmax[1], c.tmax[1], c.ord[1]), f, sg, 0,
+                          1.0, prec, stream);
+      return e;
+    }, &t_lines);
+    if (rc == OK)
+      rc = timed([&](int sg) { return fft_xy_pass(f, nx, nz, sg, 0, 1.0, prec, stream); },
+                 &t_plane);
+    c.plane = rc == OK && t_plane < t_lines;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  for (int i = 0; i < nf; i++) pool_free(fld[i]);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lock(g_fft_tune_mu);
+  g_fft_tuned[fft_key(nx, ny, nz, nf, prec)] = c;
   return OK;
 }
 

@@ -7,6 +7,8 @@
 
 #include <vector>
 
+#include <stddef.h>
+
 #include "sns_common.cuh"
 
 namespace sns {
@@ -74,6 +76,8 @@ struct LineGeo {
   // half-spectrum fields of a real-field run: x index i holds kx = i
   // (0 <= i < nx), the kx < 0 half being the complex conjugate; no x-Nyquist
   int kx_half;
+  // radix order of the line FFT (RadixOrder; plain-load passes of 64..1024)
+  int ord;
 };
 
 struct FieldPtrs {
@@ -94,7 +98,11 @@ int run_line_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags, d
 
 // Geometry of the lines along `axis` (0 = x, 1 = y, 2 = z) of nx*ny*nz fields.
 // wmax > 0 caps the adjacent lines per tile at that width (a tuned value).
-LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec, int wmax = 0);
+// Geometry of the lines along `axis`; wmax caps the adjacent lines of a tile,
+// tmax the threads up to which line groups are added (0: defaults), ord is
+// the radix order (RadixOrder).
+LineGeo axis_geo(int axis, int nx, int ny, int nz, int prec, int wmax = 0, int tmax = 0,
+                 int ord = 0);
 
 // Full 3D C2C transform of nf fields in place (the Scalar::transform
 // contract, src/Scalar.cpp:400-646), with optional fused Nyquist zeroing
@@ -109,6 +117,21 @@ int fft_xy_pass(const FieldPtrs& f, int nx, int nz, int sign, int flags, double 
                 cudaStream_t s);
 int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int flags,
           int prec, cudaStream_t stream, const void* const* tw_axes = nullptr);
+
+// Tuned plan of a 3D transform shape: per axis the tile knobs of axis_geo,
+// and whether the xy plane pass is used where it is available.
+struct FftChoice {
+  int wmax[3], tmax[3], ord[3];
+  bool plane;
+};
+// Measure candidate plans for nf fields of nx*ny*nz on pool scratch fields and
+// cache the fastest for this device (the counterpart of FFTW_MEASURE,
+// src/FFT1D.cpp:18-22); fft3d then uses it for that shape.
+int fft3d_tune(int nx, int ny, int nz, int nf, int prec, cudaStream_t stream);
+// The cached choice of a shape, if any (no tuning).
+bool fft3d_tuned(int nx, int ny, int nz, int nf, int prec, FftChoice* out);
+// SNS_TUNE=1: transforms and steppers tune each new shape on first use.
+bool tune_on_first_use();
 
 // Device twiddle table exp(-2 pi i m / L), m < L, generated in FP64 on the
 // host and stored as complex64 or complex128 (cached per device).

@@ -43,24 +43,36 @@ __host__ __device__ constexpr int tile_stride(int L, int W) {
 // Tiles of x lines: pad_pos(L) = 17 TPL for L >= 16.
 __host__ __device__ constexpr int xrow_stride(int L) { return tile_stride(L, 1); }
 
-template <int L>
+// Radix orders of a line (all give the same transform to rounding; the
+// autotuner picks one per line length):
+//   RADIX16_FIRST  radix-16 stages, the remainder (2, 4 or 8) last
+//   RADIX_REM_FIRST  the remainder first, then the radix-16 stages
+//   RADIX8  radix-8 stages, the remainder (2 or 4) last
+enum RadixOrder : int { RADIX16_FIRST = 0, RADIX_REM_FIRST = 1, RADIX8 = 2, kRadixOrders = 3 };
+
+template <int L, int ORD = RADIX16_FIRST>
 struct LinePlan {
   static constexpr int E = (L >= 16) ? 16 : L;  // elements per thread
   static constexpr int TPL = L / E;             // threads per line
+  static constexpr int BIG = (ORD == RADIX8 && L >= 8) ? 8 : 16;  // the repeated radix
   static constexpr int REM = [] {
     int r = L;
-    while (r >= 16 && r % 16 == 0) r /= 16;
+    while (r >= BIG && r % BIG == 0) r /= BIG;
     return r;
   }();
-  static constexpr int N16 = [] {
+  static constexpr int NBIG = [] {
     int c = 0, r = L;
-    while (r >= 16 && r % 16 == 0) { r /= 16; c++; }
+    while (r >= BIG && r % BIG == 0) { r /= BIG; c++; }
     return c;
   }();
-  static constexpr int NSTAGE = N16 + (REM > 1 ? 1 : 0);
-  // radix of stage s: the 16s first, the remainder last
-  __host__ __device__ static constexpr int radix(int s) { return s < N16 ? 16 : REM; }
+  static constexpr int NSTAGE = NBIG + (REM > 1 ? 1 : 0);
+  // radix of stage s
+  __host__ __device__ static constexpr int radix(int s) {
+    if (ORD == RADIX_REM_FIRST && REM > 1) return s == 0 ? REM : BIG;
+    return s < NBIG ? BIG : REM;
+  }
   static_assert(L >= 2 && (L & (L - 1)) == 0, "power-of-two line length");
+  static_assert(E % BIG == 0 || L < BIG, "a thread holds whole butterflies");
 };
 
 // W_R^k for R in {8, 16}: cos and sin(2 pi k / 16) for k = 0..15.
@@ -147,10 +159,10 @@ __device__ __forceinline__ void line_sync() {
 // twiddle table, sg = -1 forward, +1 inverse; `sync()` synchronises the
 // threads that share the line.  The first stage writes the line's slots at
 // once, so the caller synchronises the line after its own reads of them.
-template <int L, typename C, typename T, typename Idx, typename Sync>
+template <int L, int ORD = RADIX16_FIRST, typename C, typename T, typename Idx, typename Sync>
 __device__ __forceinline__ void line_fft_at(C (&v)[LinePlan<L>::E], C* base, Idx idx, int j,
                                             const C* __restrict__ tw, T sg, Sync sync) {
-  using P = LinePlan<L>;
+  using P = LinePlan<L, ORD>;
   constexpr int E = P::E, TPL = P::TPL;
   int Ns = 1;
 #pragma unroll
@@ -209,10 +221,10 @@ __device__ __forceinline__ void line_fft_at(C (&v)[LinePlan<L>::E], C* base, Idx
 // the block must call this (it may synchronise the block when TPL > 32).
 // BLOCK = true synchronises the whole block between stages, for layouts in
 // which the threads of a line are not confined to one warp.
-template <int L, bool BLOCK = false, typename C, typename T>
+template <int L, bool BLOCK = false, int ORD = RADIX16_FIRST, typename C, typename T>
 __device__ __forceinline__ void line_fft(C (&v)[LinePlan<L>::E], C* row, int j,
                                          const C* __restrict__ tw, T sg) {
-  line_fft_at<L>(
+  line_fft_at<L, ORD>(
       v, row, [](int p) { return pad_pos(p); }, j, tw, sg, [] {
         if constexpr (BLOCK)
           __syncthreads();

@@ -511,6 +511,9 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
   if (pl.xy_chunk > 0 && pl.xy_chunk < nz) pl.use_xyc = false;
   pl.passes = (pl.use_xy || pl.use_xyc || (pl.xy_chunk > 0 && pl.xy_chunk < nz)) ? 3 : 5;
   pl.lineW = lineW > 0 ? lineW : 0;
+  pl.lineT = 0;
+  pl.lineOrd = 0;
+  pl.tuned = false;
   pl.kc2 = 1e300;
   pl.sgs_klo = 0;
   pl.sgs_kinv = 1e30;
@@ -564,7 +567,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
       FieldPtrs f{};
       f.n = 6;
       for (int i = 0; i < 6; i++) f.in[i] = f.out[i] = Uc[i];
-      LineGeo g = axis_geo(1, nx, ny, pz, prec, pl.lineW);
+      LineGeo g = axis_geo(1, nx, ny, pz, prec, pl.lineW, pl.lineT, pl.lineOrd);
       int r = run_line_pass(g, f, +1, 0, 1.0, prec, s);
       if (r) return r;
       if (marks) mark();
@@ -583,7 +586,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
       FieldPtrs f{};
       f.n = 3;
       for (int i = 0; i < 3; i++) f.in[i] = f.out[i] = Uc[i];
-      LineGeo g = axis_geo(1, nx, ny, pz, prec, pl.lineW);
+      LineGeo g = axis_geo(1, nx, ny, pz, prec, pl.lineW, pl.lineT, pl.lineOrd);
       int r = run_line_pass(g, f, -1, 0, 1.0, prec, s);
       if (r) return r;
     }
@@ -623,6 +626,175 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     mark();
   }
   return OK;
+}
+
+namespace {
+
+constexpr size_t kTuneSmemCap = 220 * 1024;
+
+// Seeded values in [-1, 1) for the tuner's timing steps, so that every pass
+// runs on data of the magnitude a run has (a counter hash, not a statistical
+// generator).
+template <typename T>
+__global__ void k_fill_tune(cx_t<T>* p, int64_t n, uint32_t seed) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t h = (uint32_t)i * 2654435761u ^ seed;
+    h ^= h >> 15;
+    h *= 2246822519u;
+    h ^= h >> 13;
+    const uint32_t h2 = h * 3266489917u ^ (h >> 16);
+    p[i] = mk((T)((int32_t)h) * (T)4.656612873077393e-10,
+              (T)((int32_t)h2) * (T)4.656612873077393e-10);
+  }
+}
+
+int fill_tune(void* p, int64_t n, int prec, uint32_t seed, cudaStream_t s) {
+  const int grid = std::max(1, std::min(4 * sm_count(), (int)((n + 255) / 256)));
+  if (prec == PREC_C128)
+    k_fill_tune<double><<<grid, 256, 0, s>>>(reinterpret_cast<double2*>(p), n, seed);
+  else
+    k_fill_tune<float><<<grid, 256, 0, s>>>(reinterpret_cast<float2*>(p), n, seed);
+  SNS_CHECK_LAUNCH("k_fill_tune");
+  return OK;
+}
+
+bool k1_ok(const NSPlan& p, int W, int G) {
+  const int TPL = p.nz / elems(p.nz);
+  const size_t esz = p.prec == PREC_C128 ? 16 : 8;
+  return p.nx % W == 0 && p.ny % G == 0 && 3 * W * G * TPL <= max_threads(p.prec) &&
+         (size_t)6 * W * G * tile_stride(p.nz, W) * esz <= kTuneSmemCap;
+}
+bool xg_ok(const NSPlan& p, int G) {
+  const int TPL = p.nx / elems(p.nx);
+  const size_t esz = p.prec == PREC_C128 ? 16 : 8;
+  const int cap = p.real ? 384 : max_threads(p.prec);  // k_xcross_r2c launch bound
+  return ((int64_t)p.ny * p.nz) % G == 0 && 6 * G * TPL <= cap &&
+         (size_t)6 * G * xrow_stride(p.nx) * esz <= kTuneSmemCap;
+}
+bool zw_ok(const NSPlan& p, int W, int max_blocks) {
+  const int TPL = p.nz / elems(p.nz);
+  const size_t esz = p.prec == PREC_C128 ? 16 : 8;
+  return p.nx % W == 0 && 3 * W * TPL <= max_threads(p.prec) &&
+         (size_t)3 * W * tile_stride(p.nz, W) * esz <= kTuneSmemCap &&
+         ((int64_t)p.nx * p.ny) / W <= max_blocks;
+}
+
+}  // namespace
+
+int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[6],
+                 double* stats, int max_blocks, int* sync_words, cudaStream_t s) {
+  if (pl.passes != kNSPasses) return OK;
+  cudaEvent_t ev[kNSPasses + 1];
+  int rc = OK;
+  // the timing steps run on seeded data (with dt = 0 and nu = 0 a step only
+  // projects V, so the values stay bounded); the caller clears them after
+  const int64_t n = (int64_t)pl.nx * pl.ny * pl.nz;
+  for (int d = 0; d < 3 && rc == OK; d++) {
+    rc = fill_tune(V[d], n, pl.prec, 17u + d, s);
+    if (rc == OK) rc = fill_tune(C0[d], n, pl.prec, 29u + d, s);
+  }
+  int made = 0;
+  for (; made < kNSPasses + 1 && rc == OK; made++)
+    rc = cuda_status(cudaEventCreate(&ev[made]), "ns_tune_plan(events)");
+  // time of pass `pass` (or of passes 1 + 3) of a candidate plan: one step to
+  // set the kernels up, then the least of five timed steps
+  auto measure = [&](const NSPlan& c, int pass, bool y_pair, float* out) -> int {
+    float best = 3.4e38f;
+    for (int r = 0; r < 6; r++) {
+      int e = ns_step_once(c, V, C0, U, stats, sync_words, 0.0, 0.0, s, r ? ev : nullptr);
+      if (e) return e;
+      if (!r) continue;
+      if ((e = cuda_status(cudaEventSynchronize(ev[kNSPasses]), "ns_tune_plan"))) return e;
+      float t = 0, t2 = 0;
+      cudaEventElapsedTime(&t, ev[pass], ev[pass + 1]);
+      if (y_pair) cudaEventElapsedTime(&t2, ev[3], ev[4]);
+      best = std::min(best, t + t2);
+    }
+    *out = best;
+    return OK;
+  };
+  auto pick = [&](std::vector<NSPlan>& cands, int pass, bool y_pair) -> int {
+    float best = 3.4e38f;
+    int bi = -1;
+    for (size_t i = 0; i < cands.size(); i++) {
+      float t = 0;
+      int e = measure(cands[i], pass, y_pair, &t);
+      if (e) return e;
+      if (t < best) {
+        best = t;
+        bi = (int)i;
+      }
+    }
+    if (bi >= 0) pl = cands[bi];
+    return OK;
+  };
+  std::vector<NSPlan> c;
+  // K1: tile of the z-inverse + curl pass
+  if (rc == OK) {
+    c.clear();
+    c.push_back(pl);
+    for (int W : {2, 4, 8, 16})
+      for (int G : {1, 2, 4})
+        if (k1_ok(pl, W, G) && !(pl.k1_fused && W == pl.k1W && G == pl.k1G)) {
+          NSPlan q = pl;
+          q.k1W = W;
+          q.k1G = G;
+          q.k1_fused = true;
+          c.push_back(q);
+        }
+    NSPlan split = pl;
+    split.k1_fused = false;
+    c.push_back(split);
+    rc = pick(c, 0, false);
+  }
+  // K2 + K4: run width and thread cap, then radix order, of the y line passes
+  if (rc == OK) {
+    c.clear();
+    for (int W : {4, 8, 16})
+      for (int T : {128, 256, 512}) {
+        NSPlan q = pl;
+        q.lineW = W;
+        q.lineT = T;
+        c.push_back(q);
+      }
+    rc = pick(c, 1, true);
+  }
+  if (rc == OK && pl.ny >= 64 && pl.ny <= 1024) {
+    c.clear();
+    for (int o = 0; o < kRadixOrders; o++) {
+      NSPlan q = pl;
+      q.lineOrd = o;
+      c.push_back(q);
+    }
+    rc = pick(c, 1, true);
+  }
+  // K3: rows per CTA of the x cross pass
+  if (rc == OK) {
+    c.clear();
+    for (int G : {1, 2, 4, 8, 16})
+      if (xg_ok(pl, G)) {
+        NSPlan q = pl;
+        q.xG = G;
+        c.push_back(q);
+      }
+    if (!c.empty()) rc = pick(c, 2, false);
+  }
+  // K5: adjacent z lines per CTA of the update pass
+  if (rc == OK) {
+    c.clear();
+    for (int W : {2, 4, 8, 16, 32})
+      if (zw_ok(pl, W, max_blocks)) {
+        NSPlan q = pl;
+        q.zW = W;
+        q.update_blocks = (pl.nx / W) * pl.ny;
+        c.push_back(q);
+      }
+    if (!c.empty()) rc = pick(c, 4, false);
+  }
+  for (int i = 0; i < made; i++) cudaEventDestroy(ev[i]);
+  if (rc == OK) pl.tuned = true;
+  return rc;
 }
 
 int ns_update(const NSPlan& pl, const UpdateArgs& a, bool sgs, cudaStream_t s) {

@@ -21,6 +21,9 @@ struct NSPlan {
   XYPlan xy;
   int xy_chunk;       // planes per slab of the separate xy passes (0 = all)
   int lineW;          // adjacent lines per tile of the y/z line passes (0 = default)
+  int lineT;          // threads per CTA up to which line groups are added (0 = default)
+  int lineOrd;        // radix order of the y line passes (RadixOrder)
+  bool tuned;         // the knobs above were chosen by measurement (ns_tune_plan)
   int passes;         // timed phases per step: z-inverse, xy, z-forward+update
   bool real;          // half-spectrum fields of a real velocity (R2C / C2R along x)
   int nx_phys;        // physical nx (= nx, or 2 nx for a real-field run)
@@ -46,6 +49,18 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
 // `a`; sgs adds the divergence of the Fourier eddy stress a.tau.
 struct UpdateArgs;
 int ns_update(const NSPlan& pl, const UpdateArgs& a, bool sgs, cudaStream_t s);
+// Autotuner of the plain complex or real step (the counterpart of the
+// reference's FFTW_MEASURE planning, src/FFT1D.cpp:18-22): times the passes
+// of candidate plans on the stepper's own fields -- which must hold no state
+// yet: the timing steps fill V and C0 with seeded data, and the caller clears
+// them after -- and keeps, pass by pass,
+// the fastest: K1 tile (W x G, or one output field per CTA), the y passes'
+// run width, thread cap and radix order, the x pass's rows per CTA and the
+// update pass's width.  `max_blocks` is the capacity of `stats` in update
+// blocks.  Plans of another pass structure (fused xy phases) are left as they
+// are.
+int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[6],
+                 double* stats, int max_blocks, int* sync_words, cudaStream_t s);
 // Reduce the per-block diagnostics into out4 (device): sum|div|, sum|V|^2,
 // sum|i k x V|^2, max|div|.
 int ns_stats_final(const double* partials, int blocks, double* out4, cudaStream_t s);

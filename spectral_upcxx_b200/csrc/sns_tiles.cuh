@@ -63,8 +63,9 @@ __device__ __forceinline__ C pro_load(const C* __restrict__ src, const C* __rest
   }
 }
 
-// One tile of a line pass: field `blk mod nf`, tile `blk / nf` of `geo`.
-template <typename T, int L, int PRO, typename Fields>
+// One tile of a line pass: field `blk mod nf`, tile `blk / nf` of `geo`;
+// ORD is the radix order of the line FFT (RadixOrder).
+template <typename T, int L, int PRO, typename Fields, int ORD = RADIX16_FIRST>
 __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields& f, int nf,
                                                const cx_t<T>* __restrict__ tw, T sg, T scale,
                                                int flags, int wshift, int64_t blk,
@@ -116,7 +117,7 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
       }
     }
   }
-  line_fft<L, true>(v, row, j, tw, sg);
+  line_fft<L, true, ORD>(v, row, j, tw, sg);
 
   C* __restrict__ dst = reinterpret_cast<C*>(f.out(field));
   const bool do_scale = flags & PASS_SCALE;

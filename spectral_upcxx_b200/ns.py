@@ -16,10 +16,12 @@ from .ops import _check_field, _stream
 
 class NSStepper:
     """real=True keeps the half spectrum of a real velocity field
-    (sns_ns_create_real); the interface is unchanged."""
+    (sns_ns_create_real); the interface is unchanged.  tune=True chooses the
+    plan's tile shapes by measurement before the first use (sns_ns_tune; cached
+    per device and shape)."""
 
     def __init__(self, shape, nu: float, dt: float, dtype=torch.complex128, device="cuda",
-                 real: bool = False):
+                 real: bool = False, tune: bool = False):
         nz, ny, nx = shape
         self.shape = tuple(shape)
         self.nu, self.dt = float(nu), float(dt)
@@ -33,6 +35,8 @@ class NSStepper:
         N.call("sns_ns_create_real" if real else "sns_ns_create", C.byref(h), nx, ny, nz, self.nu,
                self.dt, self.prec, C.c_void_p(self._stream.cuda_stream))
         self.h = h
+        if tune:
+            N.call("sns_ns_tune", self.h)
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

@@ -63,6 +63,18 @@ def fft3d(fields, direction: int, normalise: bool = False, zero_nyquist: bool = 
     return fields
 
 
+def fft3d_tune(shape, dtype=torch.complex64, nfields: int = 1, device=None):
+    """Choose the 3D transform plan of `nfields` fields of `shape` (nz, ny, nx)
+    by measurement on scratch fields (sns_fft3d_tune); cached per device and
+    shape, used by every later fft3d of that shape."""
+    nz, ny, nx = shape
+    prec = N.SNS_C128 if dtype == torch.complex128 else N.SNS_C64
+    dev = torch.device(device) if device is not None else torch.device(
+        "cuda", torch.cuda.current_device())
+    s = torch.cuda.current_stream(dev)
+    N.call("sns_fft3d_tune", nx, ny, nz, int(nfields), prec, C.c_void_p(s.cuda_stream))
+
+
 def forward(f: torch.Tensor, zero: bool = True):
     """Scalar::forward (src/Scalar.cpp:208-215): transform(-1) + Nyquist zeroing."""
     return fft3d(f, -1, normalise=False, zero_nyquist=zero)
