@@ -197,6 +197,14 @@ int sns_ns_get_state(sns_ns* handle, void* const V1[3], void* const omega1[3],
  * 0.5<|u|^2>, enstrophy 0.5<|omega|^2> and max |div u_hat|.  Synchronises. */
 int sns_ns_stats(sns_ns* handle, double* div_avg, double* energy, double* enstrophy,
                  double* max_div);
+/* The same four values (div_avg, energy, enstrophy, max_div) queued on the
+ * stepper's stream and copied to out4 (pinned host or device memory) without
+ * waiting: a run can read its monitor every step (ns.cpp:206-210) while the
+ * GPU keeps stepping, and look at the values once the stream has been
+ * synchronised.  No reference counterpart (the reference's div.average()
+ * returns synchronously, src/Scalar.cpp:15-22).  Unlike sns_ns_stats it does
+ * not check the stepper's error word; sns_ns_check does. */
+int sns_ns_stats_async(sns_ns* handle, double* out4);
 /* Synchronise and report whether any step since the last check hit a bounded
  * wait of the persistent xy pass that gave up (SNS_ERR_TIMEOUT: the results
  * of those steps are invalid).  sns_ns_stats performs this check too. */

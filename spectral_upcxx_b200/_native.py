@@ -79,6 +79,7 @@ SIGNATURES = {
     "sns_ns_launches_per_step": ([_vp], _int),
     "sns_ns_describe": ([_vp, C.c_char_p, _int], _int),
     "sns_ns_tune": ([_vp], _int),
+    "sns_ns_stats_async": ([_vp, _vp], _int),
     "sns_ns_profile": ([_vp, _int], _int),
     "sns_ns_pass_times": ([_vp, C.POINTER(_dbl), C.POINTER(_int), _int], _int),
     "sns_ns_set_closure": ([_vp, _int, _dbl, _vp, _dbl], _int),

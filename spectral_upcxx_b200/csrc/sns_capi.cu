@@ -924,6 +924,23 @@ int sns_ns_stats(sns_ns* h, double* div_avg, double* energy, double* enstrophy, 
   return OK;
 }
 
+int sns_ns_stats_async(sns_ns* h, double* out4) {
+  if (!nonnull(h, "sns_ns_stats_async") || !nonnull(out4, "sns_ns_stats_async")) return ERR_ARG;
+  if (!h->stepped) {
+    set_error("sns_ns_stats_async: no step has run since the state was set");
+    return ERR_ARG;
+  }
+  int rc = ns_stats_final(h->stats_part,
+                          h->cl.model != CLOSURE_NONE ? h->pl.sgs_blocks : h->pl.update_blocks,
+                          h->stats_out, h->s);
+  if (rc) return rc;
+  const double N = (double)h->pl.nx_phys * h->pl.ny * h->pl.nz;  // full grid
+  if ((rc = ns_stats_normalise(h->stats_out, N, h->s))) return rc;
+  return cuda_status(cudaMemcpyAsync(out4, h->stats_out, 4 * sizeof(double), cudaMemcpyDefault,
+                                     h->s),
+                     "sns_ns_stats_async");
+}
+
 int sns_ns_launches_per_step(sns_ns* h) {
   if (!nonnull(h, "sns_ns_launches_per_step")) return ERR_ARG;
   return h->cl.model != CLOSURE_NONE ? kLESLaunches : h->pl.passes;

@@ -802,6 +802,22 @@ int ns_update(const NSPlan& pl, const UpdateArgs& a, bool sgs, cudaStream_t s) {
   return sgs ? update<float, true>(pl, a, s) : update<float, false>(pl, a, s);
 }
 
+// The normalisation sns_ns_stats applies on the host (mean |div|, 1/2 <|u|^2>,
+// 1/2 <|omega|^2> of the unnormalised Fourier fields), with the same divisions.
+__global__ void k_stats_normalise(double* out4, double N) {
+  if (threadIdx.x == 0) {
+    out4[0] = out4[0] / N;
+    out4[1] = 0.5 * out4[1] / (N * N);
+    out4[2] = 0.5 * out4[2] / (N * N);
+  }
+}
+
+int ns_stats_normalise(double* out4, double N, cudaStream_t s) {
+  k_stats_normalise<<<1, 32, 0, s>>>(out4, N);
+  SNS_CHECK_LAUNCH("k_stats_normalise");
+  return OK;
+}
+
 int ns_stats_final(const double* partials, int blocks, double* out4, cudaStream_t s) {
   k_stats_final<<<1, 256, 0, s>>>(partials, blocks, out4);
   SNS_CHECK_LAUNCH("k_stats_final");

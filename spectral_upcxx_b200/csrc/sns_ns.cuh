@@ -64,5 +64,8 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
 // Reduce the per-block diagnostics into out4 (device): sum|div|, sum|V|^2,
 // sum|i k x V|^2, max|div|.
 int ns_stats_final(const double* partials, int blocks, double* out4, cudaStream_t s);
+// out4 (device, from ns_stats_final) -> div_avg, energy, enstrophy, max_div of
+// an N-point grid, as sns_ns_stats reports them.
+int ns_stats_normalise(double* out4, double N, cudaStream_t s);
 
 }  // namespace sns

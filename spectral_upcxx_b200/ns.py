@@ -99,6 +99,13 @@ class NSStepper:
         return {"div_avg": v[0].value, "energy": v[1].value, "enstrophy": v[2].value,
                 "max_div": v[3].value}
 
+    def stats_async(self, out: torch.Tensor):
+        """Queue the four diagnostics (div_avg, energy, enstrophy, max_div) into
+        `out` (4 float64, pinned host or device) without synchronising."""
+        assert out.dtype == torch.float64 and out.numel() >= 4 and out.is_contiguous()
+        N.call("sns_ns_stats_async", self.h, C.c_void_p(out.data_ptr()))
+        return out
+
     def launches_per_step(self) -> int:
         return N.lib().sns_ns_launches_per_step(self.h)
 

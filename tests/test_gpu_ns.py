@@ -219,3 +219,22 @@ def test_xy_cluster_pass_matches_separate_passes(sns, cuda, dtype, n, monkeypatc
         err = (torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)).item()
         assert err < tol, err
     torch.cuda.empty_cache()
+
+
+def test_stats_async_equals_stats(sns, cuda):
+    """sns_ns_stats_async queues the diagnostics to pinned host memory without a
+    stall; after a synchronise they equal sns_ns_stats bit for bit."""
+    from spectral_upcxx_b200 import ic
+    n = 64
+    V = [x.to(torch.complex128) for x in ic.solenoidal_spectrum_hat(n, 8, cuda)]
+    st = sns.NSStepper((n, n, n), 1 / 400, 5e-4, torch.complex128)
+    st.bootstrap(V, sns.curl(V))
+    buf = torch.zeros((3, 4), dtype=torch.float64).pin_memory()
+    for t in range(3):
+        st.step(1)
+        st.stats_async(buf[t])
+    torch.cuda.synchronize()
+    s = st.stats()
+    assert buf[2].tolist() == [s["div_avg"], s["energy"], s["enstrophy"], s["max_div"]]
+    assert buf[0, 1].item() != buf[2, 1].item()  # one reading per step
+    st.close()
