@@ -118,6 +118,7 @@ struct __align__(128) TcSmem {
   float w3[kMlpHidden];
   float b3, s_out;
   uint64_t mbar;
+  uint64_t never;  // a barrier nothing arrives at (the stall test's wait)
   uint32_t tmem;
   int abort;
 };
@@ -125,9 +126,14 @@ struct __align__(128) TcSmem {
 __device__ int g_mlp_tc_status;  // nonzero: a tensor-core wait ran out
 
 
+// stall_cycles > 0 (a test of the timeout path, SNS_TC_STALL_TEST): after the
+// first layer-1 MMA of its first tile each CTA also waits, for that many
+// cycles, on a barrier that nothing arrives at; the wait runs out, the CTA
+// records the timeout and stops after waiting (with the full budget) for the
+// MMA it issued, so tensor memory is freed only once the MMA is complete.
 __global__ void __launch_bounds__(kTcRows)
     k_mlp_infer_tc(const MlpPacked* __restrict__ P, const __nv_bfloat16* __restrict__ X,
-                   int64_t M, float* __restrict__ nut) {
+                   int64_t M, float* __restrict__ nut, long long stall_cycles) {
   extern __shared__ __align__(128) unsigned char tc_raw[];
   TcSmem& S = *reinterpret_cast<TcSmem*>(tc_raw);
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -138,6 +144,7 @@ __global__ void __launch_bounds__(kTcRows)
     S.s_out = P->s_out;
     S.abort = 0;
     tc::mbar_init(&S.mbar, 1);
+    tc::mbar_init(&S.never, 1);
   }
   if (warp == 0) {
     tc::tmem_alloc(&S.tmem, kTcCols);
@@ -176,6 +183,8 @@ __global__ void __launch_bounds__(kTcRows)
       tc::mma_bf16(tmem, tc::sdesc(sX, 128, 16 * kMlpK1), tc::sdesc(sW1, 128, 16 * kMlpK1), id, 0);
       tc::commit(&S.mbar);
     }
+    if (stall_cycles > 0 && tile == blockIdx.x && !tc::mbar_wait(&S.never, 0, stall_cycles))
+      S.abort = 1;
     if (!tc::mbar_wait(&S.mbar, phase, tc::kWaitCycles)) S.abort = 1;
     phase ^= 1;
     tc::fence_after_sync();
@@ -714,9 +723,13 @@ int sns_mlp_infer(const void* packed, const void* X, int64_t M, float* nut, void
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int64_t tiles = (M + kTcRows - 1) / kTcRows;
   const int blocks = (int)std::min<int64_t>(tiles, (int64_t)per_sm[dev & 63] * sms);
+  // SNS_TC_STALL_TEST=<cycles>: exercise the timeout path (see k_mlp_infer_tc)
+  long long stall = 0;
+  if (const char* e = getenv("SNS_TC_STALL_TEST")) stall = atoll(e);
+  if (stall < 0 || stall > tc::kWaitCycles) stall = 0;
   k_mlp_infer_tc<<<blocks, kTcRows, sizeof(TcSmem), reinterpret_cast<cudaStream_t>(stream)>>>(
       reinterpret_cast<const MlpPacked*>(packed), reinterpret_cast<const __nv_bfloat16*>(X), M,
-      nut);
+      nut, stall);
   SNS_CHECK_LAUNCH("k_mlp_infer_tc");
   return OK;
 }

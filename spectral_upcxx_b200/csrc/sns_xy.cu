@@ -347,6 +347,11 @@ int xy_run(const XYPlan& p, void* const U[6], int* sync_words, cudaStream_t s) {
   a.cntB = sync_words + 2 + p.nz;
   a.err = sync_words + 2 + 2 * p.nz;
   a.spin_limit = 4000000;  // a few hundred ms of 64 ns sleeps; producers take microseconds
+  // SNS_XY_SPIN=<polls>: a smaller budget (a test of the timeout path)
+  if (const char* e = getenv("SNS_XY_SPIN")) {
+    const long long v = atoll(e);
+    if (v >= 1 && v < a.spin_limit) a.spin_limit = v;
+  }
   XYPlan q = p;
   q.sync_words = sync_words;
   q.sync_bytes_to_clear = sizeof(int) * (2 + 2 * (size_t)p.nz);

@@ -1,11 +1,13 @@
 """Small, fixed workloads for profiling the kernels under ncu.
 
-    python -m spectral_upcxx_b200.profile_cases ns128|ns256|ns256r|ens|closure64|mlp|misc
+    python -m spectral_upcxx_b200.profile_cases ns128|ns256|ns256r|ns256d|ens|closure64|mlp|misc
 
 Each case builds its inputs on the device, runs a few steps of one path and
 exits; sizes keep every case to a few GB of device memory so that a full ncu
 capture of one launch ends in seconds.  SNS_GRAPH=0 in the environment keeps
-the stepper's launches direct (one kernel per launch in the profile).
+the stepper's launches direct (one kernel per launch in the profile).  The
+stepper cases tune their plan first and run the profiled steps inside the NVTX
+range "profiled" (ncu --nvtx --nvtx-include "profiled/").
 """
 from __future__ import annotations
 
@@ -24,13 +26,21 @@ from . import ic
 def run(case: str) -> None:
     dev = torch.device("cuda", 0)
     if case.startswith("ns"):
-        # a trailing r: the real-field stepper (half spectrum)
+        # a trailing r: the real-field stepper (half spectrum); d: complex128.
+        # The plan is tuned, as the benchmark's is.
         real = case.endswith("r")
-        n = int(case[2:].rstrip("r"))
-        V0 = [x.to(torch.complex64) for x in ic.solenoidal_spectrum_hat(n, 1, dev)]
-        st = NSStepper((n, n, n), 1 / 400, 5e-4, torch.complex64, device=dev, real=real)
+        dtype = torch.complex128 if case.endswith("d") else torch.complex64
+        n = int(case[2:].rstrip("rd"))
+        V0 = [x.to(dtype) for x in ic.solenoidal_spectrum_hat(n, 1, dev)]
+        st = NSStepper((n, n, n), 1 / 400, 5e-4, dtype, device=dev, real=real, tune=True)
         st.bootstrap(V0, curl(V0))
-        st.step(3)
+        st.step(1)
+        # the steps to profile, inside an NVTX range ("profiled/" for ncu --nvtx-include)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("profiled")
+        st.step(2)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
     elif case == "ens":
         # the ensemble benchmark's boxes, untuned tiles, eager stage launches
         shapes = [(32, 32, 32)] * 32 + [(64, 64, 64)] * 24 + [(128, 128, 128)] * 8

@@ -1,0 +1,76 @@
+"""Bounded waits that run out, in the safe form: no GPU fault, no hang.
+
+* The persistent dataflow xy pass (SNS_XY_PASSES=1) with a poll budget of one
+  (SNS_XY_SPIN=1) and a one-plane lag between producers and consumers: some
+  consumer finds its plane unfinished and gives up at once; the launch still
+  ends (every access stays in bounds), sns_ns_check reports SNS_ERR_TIMEOUT
+  and clears the record, and a stepper run afterwards with the normal budget
+  succeeds and matches the separate passes.
+* The tcgen05 MLP inference with a stall test (SNS_TC_STALL_TEST=<cycles>):
+  each CTA also waits on a barrier nothing arrives at; the wait runs out,
+  sns_mlp_status reports SNS_ERR_TIMEOUT, the MMA already issued is still
+  waited for before tensor memory is freed, and the next inference is normal.
+"""
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def test_dataflow_wait_runs_out_and_recovers(sns, cuda, monkeypatch):
+    from spectral_upcxx_b200 import ic
+    N = sns._native
+    n = 64
+    Vh = ic.solenoidal_spectrum_hat(n, 4, cuda)
+    V = [x.to(torch.complex64) for x in Vh]
+    monkeypatch.setenv("SNS_XY_PASSES", "1")
+    monkeypatch.setenv("SNS_GRAPH", "0")
+    monkeypatch.setenv("SNS_XY_LAG", "1")
+    monkeypatch.setenv("SNS_XY_SPIN", "1")
+    st = sns.NSStepper((n, n, n), 1 / 400, 5e-4, torch.complex64)
+    assert "xy=dataflow" in st.describe()
+    st.bootstrap(V, sns.curl(V))
+    codes = []
+    for _ in range(10):
+        st.step(1)
+        codes.append(N.lib().sns_ns_check(st.h))
+        if codes[-1] == N.SNS_ERR_TIMEOUT:
+            break
+    assert N.SNS_ERR_TIMEOUT in codes, codes
+    assert "gave up" in N.last_error()
+    assert N.lib().sns_ns_check(st.h) == N.SNS_OK  # the record was cleared
+    st.close()
+    # the normal budget: a fresh run matches the separate passes
+    monkeypatch.delenv("SNS_XY_SPIN")
+    monkeypatch.delenv("SNS_XY_LAG")
+    out = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("SNS_XY_PASSES", mode)
+        st = sns.NSStepper((n, n, n), 1 / 400, 5e-4, torch.complex64)
+        st.bootstrap(V, sns.curl(V))
+        st.step(3)
+        assert N.lib().sns_ns_check(st.h) == N.SNS_OK
+        out[mode] = [x.clone() for x in st.state()["V1"]]
+        st.close()
+    for a, b in zip(out["1"], out["0"]):
+        assert (torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)).item() < 1e-6
+
+
+def test_tensor_core_wait_runs_out_and_recovers(sns, cuda, monkeypatch):
+    from spectral_upcxx_b200 import closure as CL
+    N = sns._native
+    m = CL.MLPModel.init(0, s_in=1.0, s_out=1.0, device=cuda)
+    X = torch.randn((1 << 16, 16), device=cuda)
+    X[:, 9:] = 0
+    X = X.to(torch.bfloat16)
+    want = m.infer(X)
+    assert N.lib().sns_mlp_status() == N.SNS_OK
+    monkeypatch.setenv("SNS_TC_STALL_TEST", "20000")
+    m.infer(X)
+    assert N.lib().sns_mlp_status() == N.SNS_ERR_TIMEOUT
+    assert "gave up" in N.last_error()
+    assert N.lib().sns_mlp_status() == N.SNS_OK  # the record was cleared
+    monkeypatch.delenv("SNS_TC_STALL_TEST")
+    got = m.infer(X)
+    assert N.lib().sns_mlp_status() == N.SNS_OK
+    assert torch.equal(got, want)
