@@ -277,6 +277,7 @@ struct sns_ns {
   void* V[3];
   void* C0[3];
   void* U[6];
+  void* W[kNSLineWork] = {};  // z-inverted V and i kz V (K1 as a line pass)
   double* stats_part;
   double* stats_out;
   int* sync_words;  // dataflow xy pass: ticket, per-plane counters, error word
@@ -317,7 +318,7 @@ int step_on(sns_ns* h, cudaStream_t s, cudaEvent_t* ev) {
     return les_step_once(h->pl, h->V, h->C0, U, h->stats_part, h->nu, h->dt, h->cl, s);
   }
   return ns_step_once(h->pl, h->V, h->C0, h->U, h->stats_part, h->sync_words, h->nu, h->dt, s,
-                      ev);
+                      ev, h->W);
 }
 
 int capture_step(sns_ns* h) {
@@ -646,6 +647,13 @@ int sns::ns_create(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double n
   }
   for (int i = 0; i < 6; i++) all[6 + i] = &h->U[i];
   for (int i = 0; i < 12 && rc == OK; i++) rc = pool_malloc(all[i], bytes);
+  // K1 as a line pass of V and i kz V into five more work fields, the curl
+  // formed in K2 (SNS_K1_LINES=0: the fused K1 tile, no extra fields)
+  const char* kl = getenv("SNS_K1_LINES");
+  if (rc == OK && !(kl && kl[0] == '0')) {
+    for (int i = 0; i < kNSLineWork && rc == OK; i++) rc = pool_malloc(&h->W[i], bytes);
+    if (rc == OK) h->pl.k1_lines = true;
+  }
   if (rc == OK)
     rc = pool_malloc((void**)&h->stats_part,
                      sizeof(double) * 4 * std::max(h->pl.update_blocks, h->pl.sgs_blocks));
@@ -684,6 +692,7 @@ int sns_ns_destroy(sns_ns* h) {
     pool_free(h->C0[d]);
   }
   for (int i = 0; i < 6; i++) pool_free(h->U[i]);
+  for (int i = 0; i < kNSLineWork; i++) pool_free(h->W[i]);
   pool_free(h->stats_part);
   pool_free(h->stats_out);
   pool_free(h->sync_words);
@@ -790,7 +799,7 @@ int sns_ns_step(sns_ns* h, int nsteps) {
       ev = &h->events[(size_t)h->recorded * (kNSPasses + 1)];
     }
     int rc = ns_step_once(h->pl, h->V, h->C0, h->U, h->stats_part, h->sync_words, h->nu, h->dt,
-                          h->s, ev);
+                          h->s, ev, h->W);
     if (rc) return rc;
     if (ev) h->recorded++;
     h->stepped = true;
@@ -991,7 +1000,8 @@ int sns_ns_tune(sns_ns* h) {
   pool_free(h->stats_part);
   h->stats_part = static_cast<double*>(part);
   NSPlan q = h->pl;
-  rc = ns_tune_plan(q, h->V, h->C0, h->U, h->stats_part, max_blocks, h->sync_words, h->s);
+  rc = ns_tune_plan(q, h->V, h->C0, h->U, h->stats_part, max_blocks, h->sync_words, h->s,
+                    h->W[0] ? h->W : nullptr);
   if (rc) return rc;
   // the timing steps ran on seeded data: the stepper starts from zero fields
   for (int d = 0; d < 3; d++) {
@@ -1015,8 +1025,9 @@ int sns_ns_describe(sns_ns* h, char* buf, int len) {
   const char* ord[3] = {"16-first", "remainder-first", "radix-8"};
   const int n = snprintf(tmp, sizeof(tmp),
                          "passes=%d xy=%s k1=%dx%d%s y=W%d/T%d/%s zW=%d xG=%d%s%s",
-                         h->cl.model != CLOSURE_NONE ? kLESLaunches : p.passes, xy, p.k1W,
-                         p.k1G, p.k1_fused ? "" : "(split)", p.lineW, p.lineT,
+                         h->cl.model != CLOSURE_NONE ? kLESLaunches : p.passes, xy,
+                         p.k1_lines ? p.k1lW : p.k1W, p.k1_lines ? p.k1lT : p.k1G,
+                         p.k1_lines ? "(lines)" : p.k1_fused ? "" : "(split)", p.lineW, p.lineT,
                          ord[p.lineOrd % 3], p.zW, p.xG, p.real ? " real" : "",
                          p.tuned ? " tuned" : "");
   if (buf && len > 0) {

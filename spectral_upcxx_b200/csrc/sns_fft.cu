@@ -185,6 +185,20 @@ int run_line_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags, d
       return dispatch_pass<double, PRO_CURL6>(geo, f, sign, flags, scale, stream);
     return dispatch_pass<float, PRO_CURL6>(geo, f, sign, flags, scale, stream);
   }
+  if (prologue == PRO_OMEGA) {
+    if (f.n != 6) {
+      set_error("omega prologue needs six output fields");
+      return ERR_ARG;
+    }
+    for (int i = 0; i < 6; i++)
+      if (!f.out[i] || (i < 5 && !f.in[i])) {
+        set_error("line pass: null field pointer");
+        return ERR_ARG;
+      }
+    if (prec == PREC_C128)
+      return dispatch_pass<double, PRO_OMEGA>(geo, f, sign, flags, scale, stream);
+    return dispatch_pass<float, PRO_OMEGA>(geo, f, sign, flags, scale, stream);
+  }
   if (prologue != PRO_LOAD && prologue != PRO_IKAXIS) {
     set_error("line pass: unknown prologue");
     return ERR_ARG;

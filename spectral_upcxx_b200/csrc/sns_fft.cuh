@@ -57,6 +57,10 @@ enum PassPrologue : int {
   PRO_IKAXIS = 3,  // field f reads in[f], times i k (the wavenumber along the
                    // line) when bit f of ikmask is set: a derivative along the
                    // pass axis taken on the way in
+  PRO_OMEGA = 4,   // y lines after a z pass: in[0..2] = the z-inverted V,
+                   // in[3..4] = the z-inverted i kz Vx, i kz Vy; fields 0..2
+                   // read V, fields 3..5 form omega = i k x V from them
+                   // (i ky Vz - dzVy, dzVx - i kx Vz, i kx Vy - i ky Vx)
 };
 
 // Geometry of a batch of lines: element p of line (w, g) of tile t sits at

@@ -514,6 +514,9 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
   pl.lineT = 0;
   pl.lineOrd = 0;
   pl.tuned = false;
+  pl.k1_lines = false;  // enabled by a caller that provides the work fields W
+  pl.k1lW = 0;
+  pl.k1lT = 0;
   pl.kc2 = 1e300;
   pl.sgs_klo = 0;
   pl.sgs_kinv = 1e30;
@@ -522,7 +525,7 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
 
 int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* const U[6],
                  double* stats, int* sync_words, double nu, double dt, cudaStream_t s,
-                 cudaEvent_t* ev) {
+                 cudaEvent_t* ev, void* const* W) {
   const int nx = pl.nx, ny = pl.ny, nz = pl.nz, prec = pl.prec;
   int rc;
   int pass = 0;
@@ -531,8 +534,24 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     pass++;
   };
   mark();
+  const bool lines = pl.k1_lines && W && !pl.use_xy && !pl.use_xyc;
   // K1: z-inverse of (V, i k x V)
-  {
+  if (lines) {
+    // V and the z derivatives i kz Vx, i kz Vy (taken on the way in), each
+    // field z-inverse-transformed on its own; K2 forms omega from them
+    FieldPtrs f{};
+    f.n = kNSLineWork;
+    for (int d = 0; d < 3; d++) f.in[d] = V[d];
+    f.in[3] = V[0];
+    f.in[4] = V[1];
+    for (int i = 0; i < kNSLineWork; i++) f.out[i] = W[i];
+    f.ikmask = 0x18u;
+    LineGeo g = axis_geo(2, nx, ny, nz, prec, pl.k1lW, pl.k1lT);
+    g.kx_half = pl.real;
+    rc = run_line_pass(g, f, +1, 0, 1.0, prec, s, PRO_IKAXIS);
+    if (rc) return rc;
+    mark();
+  } else {
     FieldPtrs f{};
     f.n = 6;
     for (int d = 0; d < 3; d++) f.in[d] = V[d];
@@ -563,7 +582,18 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     const size_t off = esz * (size_t)z0 * nx * ny;
     void* Uc[6];
     for (int i = 0; i < 6; i++) Uc[i] = static_cast<char*>(U[i]) + off;
-    {  // K2: y-inverse of the six fields
+    if (lines) {  // K2: y-inverse of V and of omega formed from the five z-inverted fields
+      FieldPtrs f{};
+      f.n = 6;
+      for (int i = 0; i < kNSLineWork; i++) f.in[i] = static_cast<char*>(W[i]) + off;
+      f.in[5] = f.in[0];
+      for (int i = 0; i < 6; i++) f.out[i] = Uc[i];
+      LineGeo g = axis_geo(1, nx, ny, pz, prec, pl.lineW, pl.lineT, pl.lineOrd);
+      g.kx_half = pl.real;
+      int r = run_line_pass(g, f, +1, 0, 1.0, prec, s, PRO_OMEGA);
+      if (r) return r;
+      if (marks) mark();
+    } else {  // K2: y-inverse of the six fields
       FieldPtrs f{};
       f.n = 6;
       for (int i = 0; i < 6; i++) f.in[i] = f.out[i] = Uc[i];
@@ -683,7 +713,8 @@ bool zw_ok(const NSPlan& p, int W, int max_blocks) {
 }  // namespace
 
 int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[6],
-                 double* stats, int max_blocks, int* sync_words, cudaStream_t s) {
+                 double* stats, int max_blocks, int* sync_words, cudaStream_t s,
+                 void* const* W) {
   if (pl.passes != kNSPasses) return OK;
   cudaEvent_t ev[kNSPasses + 1];
   int rc = OK;
@@ -697,29 +728,33 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
   int made = 0;
   for (; made < kNSPasses + 1 && rc == OK; made++)
     rc = cuda_status(cudaEventCreate(&ev[made]), "ns_tune_plan(events)");
-  // time of pass `pass` (or of passes 1 + 3) of a candidate plan: one step to
-  // set the kernels up, then the least of five timed steps
-  auto measure = [&](const NSPlan& c, int pass, bool y_pair, float* out) -> int {
+  // time of the passes in the bit mask `passes` of a candidate plan: one step
+  // to set the kernels up, then the least of five timed steps
+  auto measure = [&](const NSPlan& c, unsigned passes, float* out) -> int {
     float best = 3.4e38f;
     for (int r = 0; r < 6; r++) {
-      int e = ns_step_once(c, V, C0, U, stats, sync_words, 0.0, 0.0, s, r ? ev : nullptr);
+      int e = ns_step_once(c, V, C0, U, stats, sync_words, 0.0, 0.0, s, r ? ev : nullptr, W);
       if (e) return e;
       if (!r) continue;
       if ((e = cuda_status(cudaEventSynchronize(ev[kNSPasses]), "ns_tune_plan"))) return e;
-      float t = 0, t2 = 0;
-      cudaEventElapsedTime(&t, ev[pass], ev[pass + 1]);
-      if (y_pair) cudaEventElapsedTime(&t2, ev[3], ev[4]);
-      best = std::min(best, t + t2);
+      float sum = 0;
+      for (int p = 0; p < kNSPasses; p++)
+        if ((passes >> p) & 1u) {
+          float t = 0;
+          cudaEventElapsedTime(&t, ev[p], ev[p + 1]);
+          sum += t;
+        }
+      best = std::min(best, sum);
     }
     *out = best;
     return OK;
   };
-  auto pick = [&](std::vector<NSPlan>& cands, int pass, bool y_pair) -> int {
+  auto pick = [&](std::vector<NSPlan>& cands, unsigned passes) -> int {
     float best = 3.4e38f;
     int bi = -1;
     for (size_t i = 0; i < cands.size(); i++) {
       float t = 0;
-      int e = measure(cands[i], pass, y_pair, &t);
+      int e = measure(cands[i], passes, &t);
       if (e) return e;
       if (t < best) {
         best = t;
@@ -730,23 +765,36 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
     return OK;
   };
   std::vector<NSPlan> c;
-  // K1: tile of the z-inverse + curl pass
+  // K1: the z-inverse + curl pass as a fused tile (its shape), one output
+  // field per CTA, or the five-field line pass with the curl formed in K2
+  // (its run width and thread cap); timed with K2, whose input it sets
   if (rc == OK) {
     c.clear();
     c.push_back(pl);
-    for (int W : {2, 4, 8, 16})
+    for (int Wd : {2, 4, 8, 16})
       for (int G : {1, 2, 4})
-        if (k1_ok(pl, W, G) && !(pl.k1_fused && W == pl.k1W && G == pl.k1G)) {
+        if (k1_ok(pl, Wd, G)) {
           NSPlan q = pl;
-          q.k1W = W;
+          q.k1W = Wd;
           q.k1G = G;
           q.k1_fused = true;
+          q.k1_lines = false;
           c.push_back(q);
         }
     NSPlan split = pl;
     split.k1_fused = false;
+    split.k1_lines = false;
     c.push_back(split);
-    rc = pick(c, 0, false);
+    if (W)
+      for (int Wd : {8, 16})
+        for (int T : {256, 512}) {
+          NSPlan q = pl;
+          q.k1_lines = true;
+          q.k1lW = Wd;
+          q.k1lT = T;
+          c.push_back(q);
+        }
+    rc = pick(c, 0x3u);
   }
   // K2 + K4: run width and thread cap, then radix order, of the y line passes
   if (rc == OK) {
@@ -758,7 +806,7 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
         q.lineT = T;
         c.push_back(q);
       }
-    rc = pick(c, 1, true);
+    rc = pick(c, 0xAu);
   }
   if (rc == OK && pl.ny >= 64 && pl.ny <= 1024) {
     c.clear();
@@ -767,7 +815,7 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
       q.lineOrd = o;
       c.push_back(q);
     }
-    rc = pick(c, 1, true);
+    rc = pick(c, 0xAu);
   }
   // K3: rows per CTA of the x cross pass
   if (rc == OK) {
@@ -778,7 +826,7 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
         q.xG = G;
         c.push_back(q);
       }
-    if (!c.empty()) rc = pick(c, 2, false);
+    if (!c.empty()) rc = pick(c, 0x4u);
   }
   // K5: adjacent z lines per CTA of the update pass
   if (rc == OK) {
@@ -790,7 +838,7 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
         q.update_blocks = (pl.nx / W) * pl.ny;
         c.push_back(q);
       }
-    if (!c.empty()) rc = pick(c, 4, false);
+    if (!c.empty()) rc = pick(c, 0x10u);
   }
   for (int i = 0; i < made; i++) cudaEventDestroy(ev[i]);
   if (rc == OK) pl.tuned = true;

@@ -12,6 +12,9 @@ struct NSPlan {
   int xG;             // rows per CTA of the x cross pass
   int k1W, k1G;       // K1 tile: adjacent z lines x groups (all six outputs per CTA)
   bool k1_fused;      // K1 loads V once per tile (else one output field per CTA)
+  bool k1_lines;      // K1 as a line pass of V and i kz V (5 fields into the work
+                      // fields W), the curl formed in K2's prologue (PRO_OMEGA)
+  int k1lW, k1lT;     // tile knobs of that z line pass (axis_geo wmax, tmax)
   int zW;             // adjacent z lines per CTA of the update pass
   int update_blocks;  // CTAs of the update pass (= diagnostics partials)
   int sgs_W;          // adjacent z lines per CTA of the closure update (9 fields)
@@ -40,11 +43,13 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW = 0, int lineW 
 // with six work fields U; per-block diagnostics go to `stats`
 // (4 doubles x update_blocks).
 // `ev`, when not null, holds kNSPasses + 1 events recorded around the passes.
-// `sync_words` (xy_sync_words(nz) ints) serves the dataflow xy pass.
+// `sync_words` (xy_sync_words(nz) ints) serves the dataflow xy pass.  W: five
+// more work fields, needed when pl.k1_lines (else may be null).
 constexpr int kNSPasses = 5;
+constexpr int kNSLineWork = 5;
 int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* const U[6],
                  double* stats, int* sync_words, double nu, double dt, cudaStream_t s,
-                 cudaEvent_t* ev = nullptr);
+                 cudaEvent_t* ev = nullptr, void* const* W = nullptr);
 // The update pass (z-forward + AB2 / projection / CN update) on the fields of
 // `a`; sgs adds the divergence of the Fourier eddy stress a.tau.
 struct UpdateArgs;
@@ -60,7 +65,8 @@ int ns_update(const NSPlan& pl, const UpdateArgs& a, bool sgs, cudaStream_t s);
 // blocks.  Plans of another pass structure (fused xy phases) are left as they
 // are.
 int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[6],
-                 double* stats, int max_blocks, int* sync_words, cudaStream_t s);
+                 double* stats, int max_blocks, int* sync_words, cudaStream_t s,
+                 void* const* W = nullptr);
 // Reduce the per-block diagnostics into out4 (device): sum|div|, sum|V|^2,
 // sum|i k x V|^2, max|div|.
 int ns_stats_final(const double* partials, int blocks, double* out4, cudaStream_t s);

@@ -49,14 +49,22 @@ __device__ __forceinline__ LineCoord line_coord(const LineGeo& geo, int64_t base
 }
 
 // Element of the thread's line as the prologue forms it.
+// PRO_OMEGA: v0..v2 are the z-inverted components of V and d0, d1 the
+// z-inverted i kz Vx, i kz Vy (the z derivative taken before the z pass).
 template <int PRO, typename C, typename T>
 __device__ __forceinline__ C pro_load(const C* __restrict__ src, const C* __restrict__ v0,
                                       const C* __restrict__ v1, const C* __restrict__ v2,
+                                      const C* __restrict__ d0, const C* __restrict__ d1,
                                       int field, int64_t idx, T kx, T ky, T kz) {
   if constexpr (PRO == PRO_CURL6) {
     if (field < 3) return src[idx];
     if (field == 3) return csub(ikmul(ky, v2[idx]), ikmul(kz, v1[idx]));
     if (field == 4) return csub(ikmul(kz, v0[idx]), ikmul(kx, v2[idx]));
+    return csub(ikmul(kx, v1[idx]), ikmul(ky, v0[idx]));
+  } else if constexpr (PRO == PRO_OMEGA) {
+    if (field < 3) return src[idx];
+    if (field == 3) return csub(ikmul(ky, v2[idx]), d1[idx]);
+    if (field == 4) return csub(d0[idx], ikmul(kx, v2[idx]));
     return csub(ikmul(kx, v1[idx]), ikmul(ky, v0[idx]));
   } else {
     return src[idx];
@@ -92,10 +100,16 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
     const C* __restrict__ v0 = nullptr;
     const C* __restrict__ v1 = nullptr;
     const C* __restrict__ v2 = nullptr;
-    if constexpr (PRO == PRO_CURL6) {
+    const C* __restrict__ d0 = nullptr;
+    const C* __restrict__ d1 = nullptr;
+    if constexpr (PRO == PRO_CURL6 || PRO == PRO_OMEGA) {
       v0 = reinterpret_cast<const C*>(f.in(0));
       v1 = reinterpret_cast<const C*>(f.in(1));
       v2 = reinterpret_cast<const C*>(f.in(2));
+    }
+    if constexpr (PRO == PRO_OMEGA) {
+      d0 = reinterpret_cast<const C*>(f.in(3));
+      d1 = reinterpret_cast<const C*>(f.in(4));
     }
     // wavenumbers of the line: two are fixed, the one along the axis varies
     const T kx0 = geo.kx_half ? (T)lc.x : (T)freq_i(lc.x, geo.nx),
@@ -111,7 +125,7 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
         const C x = src[lc.idx0 + e * lc.step];
         v[e] = ik ? ikmul(kp, x) : x;
       } else {
-        v[e] = pro_load<PRO, C>(src, v0, v1, v2, field, lc.idx0 + e * lc.step,
+        v[e] = pro_load<PRO, C>(src, v0, v1, v2, d0, d1, field, lc.idx0 + e * lc.step,
                                 geo.axis == 0 ? kp : kx0, geo.axis == 1 ? kp : ky0,
                                 geo.axis == 2 ? kp : kz0);
       }
