@@ -50,8 +50,12 @@ SHAPES = [(32, 32, 32), (64, 64, 64), (32, 32, 32), (16, 32, 64), (128, 128, 128
 
 
 def _build(sns, cuda, dtype, shapes, nus, dt, tune):
+    import os
     ens = sns.NSEnsemble(shapes, nus, dt, dtype, tune=tune)
     singles = []
+    # the ensemble steps its boxes with the fused K1 tile: single steppers of
+    # the same plan (without the K1 line-pass variant)
+    os.environ["SNS_K1_LINES"] = "0"
     for b, shape in enumerate(shapes):
         Vd = [dev(x, dtype, cuda) for x in random_velocity_hat(shape, seed=100 + b)]
         wd = sns.curl(Vd)
@@ -59,6 +63,7 @@ def _build(sns, cuda, dtype, shapes, nus, dt, tune):
         st = sns.NSStepper(shape, nus[b], dt, dtype)
         st.bootstrap(Vd, wd)
         singles.append(st)
+    del os.environ["SNS_K1_LINES"]
     return ens, singles
 
 
