@@ -647,10 +647,13 @@ int sns::ns_create(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double n
   }
   for (int i = 0; i < 6; i++) all[6 + i] = &h->U[i];
   for (int i = 0; i < 12 && rc == OK; i++) rc = pool_malloc(all[i], bytes);
-  // K1 as a line pass of V and i kz V into five more work fields, the curl
-  // formed in K2 (SNS_K1_LINES=0: the fused K1 tile, no extra fields)
+  // SNS_K1_LINES=1: K1 as a line pass of V and i kz V into five more work
+  // fields, the curl formed in K2 (and a candidate of the tuner).  Measured on
+  // B200 at 256^3 complex64 it loses: the z line pass runs at 3.1 TB/s like
+  // the fused K1 tile (0.351 vs 0.394 ms) while the omega prologue's extra
+  // loads slow K2 from 0.297 to 0.522 ms.
   const char* kl = getenv("SNS_K1_LINES");
-  if (rc == OK && !(kl && kl[0] == '0')) {
+  if (rc == OK && kl && kl[0] == '1') {
     for (int i = 0; i < kNSLineWork && rc == OK; i++) rc = pool_malloc(&h->W[i], bytes);
     if (rc == OK) h->pl.k1_lines = true;
   }

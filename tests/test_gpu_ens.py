@@ -54,7 +54,7 @@ def _build(sns, cuda, dtype, shapes, nus, dt, tune):
     ens = sns.NSEnsemble(shapes, nus, dt, dtype, tune=tune)
     singles = []
     # the ensemble steps its boxes with the fused K1 tile: single steppers of
-    # the same plan (without the K1 line-pass variant)
+    # the same plan (not the opt-in K1 line-pass variant)
     os.environ["SNS_K1_LINES"] = "0"
     for b, shape in enumerate(shapes):
         Vd = [dev(x, dtype, cuda) for x in random_velocity_hat(shape, seed=100 + b)]

@@ -238,3 +238,25 @@ def test_stats_async_equals_stats(sns, cuda):
     assert buf[2].tolist() == [s["div_avg"], s["energy"], s["enstrophy"], s["max_div"]]
     assert buf[0, 1].item() != buf[2, 1].item()  # one reading per step
     st.close()
+
+
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+def test_k1_line_pass_variant_matches(sns, cuda, dtype, monkeypatch):
+    """The opt-in K1 variant (SNS_K1_LINES=1: z line pass of V and i kz V, the
+    curl formed in the y pass) gives the step of the fused K1 tile."""
+    from spectral_upcxx_b200 import ic
+    n = 64
+    Vh = ic.solenoidal_spectrum_hat(n, 13, cuda)
+    out = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("SNS_K1_LINES", mode)
+        V = [x.to(dtype) for x in Vh]
+        st = sns.NSStepper((n, n, n), 1 / 400, 5e-4, dtype)
+        assert ("(lines)" in st.describe()) == (mode == "1")
+        st.bootstrap(V, sns.curl(V))
+        st.step(3)
+        out[mode] = [x.to(torch.complex128) for x in st.state()["V1"]]
+        st.close()
+    tol = 1e-13 if dtype == torch.complex128 else 2e-6
+    for a, b in zip(out["1"], out["0"]):
+        assert (torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)).item() < tol
