@@ -1030,7 +1030,8 @@ int sns_ns_describe(sns_ns* h, char* buf, int len) {
                          "passes=%d xy=%s k1=%dx%d%s y=W%d/T%d/%s zW=%d xG=%d%s%s",
                          h->cl.model != CLOSURE_NONE ? kLESLaunches : p.passes, xy,
                          p.k1_lines ? p.k1lW : p.k1W, p.k1_lines ? p.k1lT : p.k1G,
-                         p.k1_lines ? "(lines)" : p.k1_fused ? "" : "(split)", p.lineW, p.lineT,
+                         p.k1_lines ? "(lines)" : !p.k1_fused ? "(split)" : p.k1_reload ? "(reload)" : "",
+                         p.lineW, p.lineT,
                          ord[p.lineOrd % 3], p.zW, p.xG, p.real ? " real" : "",
                          p.tuned ? " tuned" : "");
   if (buf && len > 0) {

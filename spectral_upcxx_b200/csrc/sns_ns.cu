@@ -157,14 +157,18 @@ __global__ void __launch_bounds__(384, sizeof(T) == 4 ? 2 : 1)
 
 // ---------------------------------------------------------------------------
 // K1: z lines -- inverse of V and of omega = i k x V from one load of V.
-template <typename T, int L>
+template <typename T, int L, bool RELOAD>
 __global__ void __launch_bounds__(MaxThreads<T>::value)
     k_zcurl(const LineGeo geo, const FieldPtrs f, const cx_t<T>* __restrict__ tw, int wshift) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   pdl_trigger();
   pdl_wait();
-  curl_zpass_tile<T, L>(geo, ParamFields{f}, tw, wshift, (int64_t)blockIdx.x,
-                        reinterpret_cast<cx_t<T>*>(smem_raw));
+  if constexpr (RELOAD)
+    curl_zpass_tile_reload<T, L>(geo, ParamFields{f}, tw, wshift, (int64_t)blockIdx.x,
+                                 reinterpret_cast<cx_t<T>*>(smem_raw));
+  else
+    curl_zpass_tile<T, L>(geo, ParamFields{f}, tw, wshift, (int64_t)blockIdx.x,
+                          reinterpret_cast<cx_t<T>*>(smem_raw));
 }
 
 // ---------------------------------------------------------------------------
@@ -237,8 +241,8 @@ int launch_xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream
   return OK;
 }
 
-template <typename T, int L>
-int launch_zcurl(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
+template <typename T, int L, bool RELOAD>
+int launch_zcurl_as(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
   using C = cx_t<T>;
   constexpr int TPL = LinePlan<L>::TPL;
   LineGeo g{};
@@ -257,12 +261,12 @@ int launch_zcurl(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
   g.sa = g.W;
   g.sb = (int64_t)g.G * pl.nx;
   const int threads = 3 * g.W * g.G * TPL;
-  const size_t smem = (size_t)6 * g.W * g.G * tile_stride(L, g.W) * sizeof(C);
+  const size_t smem = (size_t)(RELOAD ? 3 : 6) * g.W * g.G * tile_stride(L, g.W) * sizeof(C);
   static bool attr[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr[dev & 63]) {
-    cudaError_t e = allow_max_dynamic_smem(k_zcurl<T, L>);
+    cudaError_t e = allow_max_dynamic_smem(k_zcurl<T, L, RELOAD>);
     if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_zcurl)");
     attr[dev & 63] = true;
   }
@@ -273,10 +277,16 @@ int launch_zcurl(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
   }
   int wshift = 0;
   while ((1 << wshift) < g.W) wshift++;
-  cudaError_t e = launch_pdl(k_zcurl<T, L>, dim3((unsigned)(g.TA * g.TB)), dim3(threads), smem, s,
-                             g, f, tw, wshift);
+  cudaError_t e = launch_pdl(k_zcurl<T, L, RELOAD>, dim3((unsigned)(g.TA * g.TB)), dim3(threads),
+                             smem, s, g, f, tw, wshift);
   if (e != cudaSuccess) return cuda_status(e, "k_zcurl");
   return OK;
+}
+
+template <typename T, int L>
+int launch_zcurl(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
+  return pl.k1_reload ? launch_zcurl_as<T, L, true>(pl, f, s)
+                      : launch_zcurl_as<T, L, false>(pl, f, s);
 }
 
 template <typename T, int M>
@@ -515,6 +525,10 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
   pl.lineOrd = 0;
   pl.tuned = false;
   pl.k1_lines = false;  // enabled by a caller that provides the work fields W
+  {
+    const char* e = getenv("SNS_K1_RELOAD");
+    pl.k1_reload = e && e[0] == '1';
+  }
   pl.k1lW = 0;
   pl.k1lT = 0;
   pl.kc2 = 1e300;
@@ -689,11 +703,11 @@ int fill_tune(void* p, int64_t n, int prec, uint32_t seed, cudaStream_t s) {
   return OK;
 }
 
-bool k1_ok(const NSPlan& p, int W, int G) {
+bool k1_ok(const NSPlan& p, int W, int G, bool reload) {
   const int TPL = p.nz / elems(p.nz);
   const size_t esz = p.prec == PREC_C128 ? 16 : 8;
   return p.nx % W == 0 && p.ny % G == 0 && 3 * W * G * TPL <= max_threads(p.prec) &&
-         (size_t)6 * W * G * tile_stride(p.nz, W) * esz <= kTuneSmemCap;
+         (size_t)(reload ? 3 : 6) * W * G * tile_stride(p.nz, W) * esz <= kTuneSmemCap;
 }
 bool xg_ok(const NSPlan& p, int G) {
   const int TPL = p.nx / elems(p.nx);
@@ -771,16 +785,18 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
   if (rc == OK) {
     c.clear();
     c.push_back(pl);
-    for (int Wd : {2, 4, 8, 16})
-      for (int G : {1, 2, 4})
-        if (k1_ok(pl, Wd, G)) {
-          NSPlan q = pl;
-          q.k1W = Wd;
-          q.k1G = G;
-          q.k1_fused = true;
-          q.k1_lines = false;
-          c.push_back(q);
-        }
+    for (int reload = 0; reload < 2; reload++)
+      for (int Wd : {2, 4, 8, 16})
+        for (int G : {1, 2, 4})
+          if (k1_ok(pl, Wd, G, reload)) {
+            NSPlan q = pl;
+            q.k1W = Wd;
+            q.k1G = G;
+            q.k1_fused = true;
+            q.k1_reload = reload;
+            q.k1_lines = false;
+            c.push_back(q);
+          }
     NSPlan split = pl;
     split.k1_fused = false;
     split.k1_lines = false;

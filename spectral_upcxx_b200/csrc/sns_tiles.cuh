@@ -227,6 +227,75 @@ __device__ __forceinline__ void curl_zpass_tile(const LineGeo& geo, const Fields
 }
 
 // ---------------------------------------------------------------------------
+// K1 with omega formed in registers: each thread z-inverse-transforms its
+// component V_d and stores it, then loads the two other components at its
+// positions again -- lines the CTA has just read, so the loads are served from
+// L1 -- forms omega_d = (i k x V)_d and transforms that.  Shared memory holds
+// one set of 3 W G padded rows (the line FFTs' exchanges) and carries no
+// component data, so the tile issues 64 shared-memory accesses per thread
+// instead of 144.
+template <typename T, int L, typename Fields>
+__device__ __forceinline__ void curl_zpass_tile_reload(const LineGeo& geo, const Fields& f,
+                                                       const cx_t<T>* __restrict__ tw,
+                                                       int wshift, int64_t blk, cx_t<T>* sm) {
+  using C = cx_t<T>;
+  using P = LinePlan<L>;
+  constexpr int E = P::E, TPL = P::TPL;
+  const int W = geo.W, G = geo.G, lines = W * G;
+  const int RS = tile_stride(L, W);
+  const int64_t base = (blk % geo.TA) * geo.sa + (blk / geo.TA) * geo.sb;
+  const int w = threadIdx.x & (W - 1);
+  const int s = threadIdx.x >> wshift;
+  const int j = s & (TPL - 1);
+  const int s2 = s / TPL;
+  const int g = s2 % G, d = s2 / G;  // line (w, g) of component d
+  C* row = sm + (d * lines + w + W * g) * RS;
+  const LineCoord lc = line_coord(geo, base, w, g, j, TPL);
+  const C* __restrict__ v0 = reinterpret_cast<const C*>(f.in(0));
+  const C* __restrict__ v1 = reinterpret_cast<const C*>(f.in(1));
+  const C* __restrict__ v2 = reinterpret_cast<const C*>(f.in(2));
+  C v[E];
+  {
+    const C* __restrict__ src = d == 0 ? v0 : d == 1 ? v1 : v2;
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = src[lc.idx0 + e * lc.step];
+  }
+  line_fft<L, true>(v, row, j, tw, (T)1);
+  {
+    C* __restrict__ dst = reinterpret_cast<C*>(d == 0 ? f.out(0) : d == 1 ? f.out(1) : f.out(2));
+#pragma unroll
+    for (int e = 0; e < E; e++) dst[lc.idx0 + e * lc.step] = v[e];
+  }
+  {
+    // (ky Vz - kz Vy, kz Vx - kx Vz, kx Vy - ky Vx) times i, as curl_zpass_tile forms it
+    const C* __restrict__ pa = d == 0 ? v2 : d == 1 ? v0 : v1;
+    const C* __restrict__ pb = d == 0 ? v1 : d == 1 ? v2 : v0;
+    const T kx = geo.kx_half ? (T)lc.x : (T)freq_i(lc.x, geo.nx);
+    const T ky = (T)freq_i(lc.y, geo.ny);
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int64_t q = lc.idx0 + e * lc.step;
+      const T kz = (T)freq_i(j + TPL * e, geo.nz);
+      const C a = pa[q], b = pb[q];
+      if (d == 0)
+        v[e] = csub(ikmul(ky, a), ikmul(kz, b));
+      else if (d == 1)
+        v[e] = csub(ikmul(kz, a), ikmul(kx, b));
+      else
+        v[e] = csub(ikmul(kx, a), ikmul(ky, b));
+    }
+  }
+  // the last stage of the first transform read the row before a block barrier,
+  // so the second may write it at once
+  line_fft<L, true>(v, row, j, tw, (T)1);
+  {
+    C* __restrict__ dst = reinterpret_cast<C*>(d == 0 ? f.out(3) : d == 1 ? f.out(4) : f.out(5));
+#pragma unroll
+    for (int e = 0; e < E; e++) dst[lc.idx0 + e * lc.step] = v[e];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // K3 of the NS step: x lines -- inverse 6 fields, 1/N^2-scaled complex cross
 // product u x omega, forward 3 fields (src/Vector.cpp:79-89).  A tile is G
 // rows of all six fields; f.in(0..5) = (u, omega), f.out(0..2) = the product.

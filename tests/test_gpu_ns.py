@@ -241,18 +241,21 @@ def test_stats_async_equals_stats(sns, cuda):
 
 
 @pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
-def test_k1_line_pass_variant_matches(sns, cuda, dtype, monkeypatch):
-    """The opt-in K1 variant (SNS_K1_LINES=1: z line pass of V and i kz V, the
-    curl formed in the y pass) gives the step of the fused K1 tile."""
+@pytest.mark.parametrize("variant,tag", [("SNS_K1_LINES", "(lines)"),
+                                         ("SNS_K1_RELOAD", "(reload)")])
+def test_k1_variants_match(sns, cuda, dtype, variant, tag, monkeypatch):
+    """The K1 variants -- SNS_K1_LINES=1: z line pass of V and i kz V, the curl
+    formed in the y pass; SNS_K1_RELOAD=1: the fused tile forming omega from
+    reloads of V -- give the step of the default fused K1 tile."""
     from spectral_upcxx_b200 import ic
     n = 64
     Vh = ic.solenoidal_spectrum_hat(n, 13, cuda)
     out = {}
     for mode in ("1", "0"):
-        monkeypatch.setenv("SNS_K1_LINES", mode)
+        monkeypatch.setenv(variant, mode)
         V = [x.to(dtype) for x in Vh]
         st = sns.NSStepper((n, n, n), 1 / 400, 5e-4, dtype)
-        assert ("(lines)" in st.describe()) == (mode == "1")
+        assert (tag in st.describe()) == (mode == "1")
         st.bootstrap(V, sns.curl(V))
         st.step(3)
         out[mode] = [x.to(torch.complex128) for x in st.state()["V1"]]
