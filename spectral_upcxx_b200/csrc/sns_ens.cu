@@ -328,7 +328,7 @@ bool make_class(const sns_ens* e, int s, int c, const StageCfg& cfg, EnsClass& k
     k.wshift = log2i(W);
     k.nf = s == 3 ? 3 : 6;
     k.tiles = g.TA * g.TB * k.nf;
-    smem = (size_t)lines * tile_stride(L, W) * esz;
+    smem = (size_t)lines * tile_stride(L, W, (int)esz) * esz;
   } else if (s == 2) {
     const int tpl = tpl_of(nx);
     if (T % (6 * tpl)) return false;
@@ -338,7 +338,7 @@ bool make_class(const sns_ens* e, int s, int c, const StageCfg& cfg, EnsClass& k
     k.L = nx;
     k.G = G;
     k.tiles = rows / G;
-    smem = (size_t)6 * G * xrow_stride(nx) * esz;
+    smem = (size_t)6 * G * xrow_stride(nx, (int)esz) * esz;
   } else {
     const int tpl = tpl_of(nz);
     if (T % (3 * tpl)) return false;
@@ -348,7 +348,7 @@ bool make_class(const sns_ens* e, int s, int c, const StageCfg& cfg, EnsClass& k
     k.L = nz;
     k.W = W;
     k.tiles = cols / W;
-    smem = (size_t)3 * W * tile_stride(nz, W) * esz;
+    smem = (size_t)3 * W * tile_stride(nz, W, (int)esz) * esz;
   }
   k.tw = twiddles(k.L, e->prec);
   return k.tw != nullptr && smem <= 200 * 1024;

@@ -104,7 +104,7 @@ static int launch_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int fla
   constexpr int TPL = LinePlan<L>::TPL;
   const int lines = geo.W * geo.G;
   const int threads = lines * TPL;
-  const size_t smem = (size_t)lines * tile_stride(L, geo.W) * sizeof(C);
+  const size_t smem = (size_t)lines * tile_stride(L, geo.W, (int)sizeof(C)) * sizeof(C);
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -234,13 +234,13 @@ static void choose_tile(LineGeo& g, int64_t adjacent, int64_t groups, int prec, 
     if (v >= 1 && (v & (v - 1)) == 0) Wmax = v;
   }
   while (W * 2 <= Wmax && adjacent % (W * 2) == 0 && W * 2 * TPL <= max_threads(prec) &&
-         (size_t)(W * 2) * tile_stride(g.L, W * 2) * esz <= smem_cap)
+         (size_t)(W * 2) * tile_stride(g.L, W * 2, (int)esz) * esz <= smem_cap)
     W *= 2;
   int G = 1;
   const int tcap = tmax > 0 ? tmax : 256;  // threads per CTA up to which groups are added
   while (W * G * 2 * TPL <= tcap && W * G * 2 * TPL <= max_threads(prec) &&
          groups % (G * 2) == 0 &&
-         (size_t)(W * G * 2) * tile_stride(g.L, W) * esz <= smem_cap / 2)
+         (size_t)(W * G * 2) * tile_stride(g.L, W, (int)esz) * esz <= smem_cap / 2)
     G *= 2;
   g.W = W;
   g.G = G;

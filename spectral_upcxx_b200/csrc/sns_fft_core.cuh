@@ -26,22 +26,23 @@ __host__ __device__ constexpr int pad_pos(int p) { return p + (p >> 4); }
 __host__ __device__ constexpr int row_stride(int L) {
   return (pad_pos(L) & 1) ? pad_pos(L) : pad_pos(L) + 1;
 }
-// Row stride of a tile whose half-warps hold 16 / J lines of J consecutive
-// positions each: J = min(TPL, 16 / W) for runs of W adjacent lines (thread
-// index w fastest; W = 1 for single x lines).  An 8-byte access is served per
-// half-warp, so its 16 lanes must fall on distinct 8-byte slots (modulo 16): a
-// stride of J times an odd number does that.  J = 1 is the odd stride of
-// row_stride.
-__host__ __device__ constexpr int tile_stride(int L, int W) {
+// Row stride of a tile whose accesses are served per group of P = 128 / esz
+// lanes (a half-warp for 8-byte elements, a quarter-warp for 16-byte ones):
+// such a group holds P / J lines of J = min(TPL, P / W) consecutive positions
+// for runs of W adjacent lines (thread index w fastest; W = 1 for single x
+// lines), so its P lanes fall on distinct element slots (modulo P) when the
+// stride is J times an odd number.  J = 1 is an odd stride.
+__host__ __device__ constexpr int tile_stride(int L, int W, int esz = 8) {
+  const int P = 128 / esz;
   const int tpl = L >= 16 ? L / 16 : 1;
-  const int J = W >= 16 ? 1 : (16 / W < tpl ? 16 / W : tpl);
+  const int J = W >= P ? 1 : (P / W < tpl ? P / W : tpl);
   int rs = pad_pos(L);
-  if (J >= 16) return rs;
+  if (J >= P) return rs;
   while (rs % J != 0 || ((rs / J) & 1) == 0) rs++;
   return rs;
 }
-// Tiles of x lines: pad_pos(L) = 17 TPL for L >= 16.
-__host__ __device__ constexpr int xrow_stride(int L) { return tile_stride(L, 1); }
+// Tiles of x lines.
+__host__ __device__ constexpr int xrow_stride(int L, int esz = 8) { return tile_stride(L, 1, esz); }
 
 // Radix orders of a line (all give the same transform to rounding; the
 // autotuner picks one per line length):

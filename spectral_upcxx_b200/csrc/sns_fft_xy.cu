@@ -43,7 +43,8 @@ __host__ __device__ constexpr int xy_threads() {
 template <typename T, int L>
 constexpr size_t xy_smem_bytes() {
   constexpr int R = L / xy_cluster<L>();
-  constexpr int a = R * xrow_stride(L), b = R * tile_stride(L, R);
+  constexpr int es = (int)sizeof(cx_t<T>);
+  constexpr int a = R * xrow_stride(L, es), b = R * tile_stride(L, R, es);
   return (size_t)(a > b ? a : b) * sizeof(cx_t<T>);
 }
 
@@ -55,7 +56,7 @@ __global__ void __launch_bounds__(xy_threads<L>(), 2)
   using C = cx_t<T>;
   using P = LinePlan<L>;
   constexpr int E = P::E, TPL = P::TPL, R = L / xy_cluster<L>();
-  constexpr int RSX = xrow_stride(L), RSY = tile_stride(L, R);
+  constexpr int RSX = xrow_stride(L, (int)sizeof(C)), RSY = tile_stride(L, R, (int)sizeof(C));
   static_assert(TPL <= 32, "row lines stay within a warp");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* sm = reinterpret_cast<C*>(smem_raw);

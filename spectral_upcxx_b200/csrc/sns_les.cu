@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kXlesThreads)
     k_xles(const XlesArgs a, const cx_t<T>* __restrict__ tw) {
   using C = cx_t<T>;
   using P = LinePlan<L>;
-  constexpr int E = P::E, TPL = P::TPL, RS = xrow_stride(L);
+  constexpr int E = P::E, TPL = P::TPL, RS = xrow_stride(L, (int)sizeof(C));
   constexpr int G = 32 / TPL;
   constexpr int PTS = G * L;
   static_assert(TPL <= 32 && 12 * G * TPL == kXlesThreads, "tile shape");
@@ -297,7 +297,7 @@ int launch_xles_l(const XlesArgs& a, int64_t rows, cudaStream_t s) {
     set_error("closure step: ny * nz must be a multiple of the x-pass rows per CTA");
     return ERR_UNSUPPORTED;
   }
-  const size_t smem = (size_t)12 * G * xrow_stride(L) * sizeof(C);
+  const size_t smem = (size_t)12 * G * xrow_stride(L, (int)sizeof(C)) * sizeof(C);
   static bool attr[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);

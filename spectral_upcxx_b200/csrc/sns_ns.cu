@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(384, sizeof(T) == 4 ? 2 : 1)
                  int G, T scale2) {
   using C = cx_t<T>;
   using P = LinePlan<M>;
-  constexpr int E = P::E, TPL = P::TPL, RS = xrow_stride(M);
+  constexpr int E = P::E, TPL = P::TPL, RS = xrow_stride(M, (int)sizeof(C));
   static_assert(TPL <= 32, "a line's threads share a warp");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   pdl_trigger();
@@ -223,7 +223,7 @@ int launch_xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream
   constexpr int TPL = LinePlan<L>::TPL;
   const int G = pl.xG;
   const int threads = 6 * G * TPL;
-  const size_t smem = (size_t)6 * G * xrow_stride(L) * sizeof(C);
+  const size_t smem = (size_t)6 * G * xrow_stride(L, (int)sizeof(C)) * sizeof(C);
   static bool attr[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -261,7 +261,8 @@ int launch_zcurl_as(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
   g.sa = g.W;
   g.sb = (int64_t)g.G * pl.nx;
   const int threads = 3 * g.W * g.G * TPL;
-  const size_t smem = (size_t)(RELOAD ? 3 : 6) * g.W * g.G * tile_stride(L, g.W) * sizeof(C);
+  const size_t smem =
+      (size_t)(RELOAD ? 3 : 6) * g.W * g.G * tile_stride(L, g.W, (int)sizeof(C)) * sizeof(C);
   static bool attr[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -295,7 +296,7 @@ int launch_xcross_r2c(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaSt
   constexpr int TPL = LinePlan<M>::TPL;
   const int G = pl.xG;
   const int threads = 6 * G * TPL;
-  const size_t smem = (size_t)6 * G * xrow_stride(M) * sizeof(C);
+  const size_t smem = (size_t)6 * G * xrow_stride(M, (int)sizeof(C)) * sizeof(C);
   static bool attr[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -353,7 +354,7 @@ int launch_update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
   constexpr int TPL = LinePlan<L>::TPL;
   constexpr int NF = SGS ? 9 : 3;
   const int threads = NF * a.W * TPL;
-  const size_t smem = (size_t)NF * a.W * tile_stride(L, a.W) * sizeof(C);
+  const size_t smem = (size_t)NF * a.W * tile_stride(L, a.W, (int)sizeof(C)) * sizeof(C);
   const int blocks = (int)(((int64_t)pl.nx * pl.ny) / a.W);
   static bool attr[64] = {false};
   int dev = 0;
@@ -441,7 +442,7 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
     const int TPL = nx / elems(nx);
     int G = 1;
     while (6 * (G * 2) * TPL <= 384 && ((int64_t)ny * nz) % (G * 2) == 0 &&
-           (size_t)6 * G * 2 * xrow_stride(nx) * esz <= 110 * 1024)
+           (size_t)6 * G * 2 * xrow_stride(nx, (int)esz) * esz <= 110 * 1024)
       G *= 2;
     if (6 * G * TPL > max_threads(prec)) {
       set_error("fused NS step: nx too large for the x-pass tile");
@@ -467,17 +468,17 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
     int W = 1;
     const int Wmax = prec == PREC_C128 ? 8 : 16;
     while (W * 2 <= Wmax && nx % (W * 2) == 0 && 3 * (W * 2) * TPL <= cap &&
-           (size_t)6 * (W * 2) * tile_stride(nz, W * 2) * esz <= smem_cap)
+           (size_t)6 * (W * 2) * tile_stride(nz, W * 2, (int)esz) * esz <= smem_cap)
       W *= 2;
     int G = 1;
     while (ny % (G * 2) == 0 && 3 * W * (G * 2) * TPL <= 384 &&
-           (size_t)6 * W * (G * 2) * tile_stride(nz, W) * esz <= smem_cap)
+           (size_t)6 * W * (G * 2) * tile_stride(nz, W, (int)esz) * esz <= smem_cap)
       G *= 2;
     pl.k1W = W;
     pl.k1G = G;
     const char* e = getenv("SNS_K1_SPLIT");
     pl.k1_fused = !(e && e[0] == '1') && 3 * W * G * TPL <= cap &&
-                  (size_t)6 * W * G * tile_stride(nz, W) * esz <= smem_cap;
+                  (size_t)6 * W * G * tile_stride(nz, W, (int)esz) * esz <= smem_cap;
   }
   // K5 tile: W adjacent z lines of three fields
   {
@@ -491,7 +492,7 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
       if (v >= 1 && (v & (v - 1)) == 0) Wmax = v;
     }
     while (W * 2 <= Wmax && nx % (W * 2) == 0 && 3 * (W * 2) * TPL <= max_threads(prec) &&
-           (size_t)3 * W * 2 * tile_stride(nz, W * 2) * esz <= 110 * 1024)
+           (size_t)3 * W * 2 * tile_stride(nz, W * 2, (int)esz) * esz <= 110 * 1024)
       W *= 2;
     pl.zW = W;
     pl.update_blocks = (nx / W) * ny;
@@ -499,7 +500,7 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
     const int cap = std::min(576, max_threads(prec));
     int Ws = 1;
     while (Ws * 2 <= Wmax && ((int64_t)nx * ny) % (Ws * 2) == 0 && 9 * (Ws * 2) * TPL <= cap &&
-           (size_t)9 * Ws * 2 * tile_stride(nz, Ws * 2) * esz <= 110 * 1024)
+           (size_t)9 * Ws * 2 * tile_stride(nz, Ws * 2, (int)esz) * esz <= 110 * 1024)
       Ws *= 2;
     pl.sgs_W = Ws;
     pl.sgs_blocks = (int)(((int64_t)nx * ny) / Ws);
@@ -707,20 +708,20 @@ bool k1_ok(const NSPlan& p, int W, int G, bool reload) {
   const int TPL = p.nz / elems(p.nz);
   const size_t esz = p.prec == PREC_C128 ? 16 : 8;
   return p.nx % W == 0 && p.ny % G == 0 && 3 * W * G * TPL <= max_threads(p.prec) &&
-         (size_t)(reload ? 3 : 6) * W * G * tile_stride(p.nz, W) * esz <= kTuneSmemCap;
+         (size_t)(reload ? 3 : 6) * W * G * tile_stride(p.nz, W, (int)esz) * esz <= kTuneSmemCap;
 }
 bool xg_ok(const NSPlan& p, int G) {
   const int TPL = p.nx / elems(p.nx);
   const size_t esz = p.prec == PREC_C128 ? 16 : 8;
   const int cap = p.real ? 384 : max_threads(p.prec);  // k_xcross_r2c launch bound
   return ((int64_t)p.ny * p.nz) % G == 0 && 6 * G * TPL <= cap &&
-         (size_t)6 * G * xrow_stride(p.nx) * esz <= kTuneSmemCap;
+         (size_t)6 * G * xrow_stride(p.nx, (int)esz) * esz <= kTuneSmemCap;
 }
 bool zw_ok(const NSPlan& p, int W, int max_blocks) {
   const int TPL = p.nz / elems(p.nz);
   const size_t esz = p.prec == PREC_C128 ? 16 : 8;
   return p.nx % W == 0 && 3 * W * TPL <= max_threads(p.prec) &&
-         (size_t)3 * W * tile_stride(p.nz, W) * esz <= kTuneSmemCap &&
+         (size_t)3 * W * tile_stride(p.nz, W, (int)esz) * esz <= kTuneSmemCap &&
          ((int64_t)p.nx * p.ny) / W <= max_blocks;
 }
 

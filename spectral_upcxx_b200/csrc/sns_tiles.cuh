@@ -90,7 +90,7 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
   const int s = threadIdx.x >> wshift;
   const int j = s & (TPL - 1);
   const int g = s / TPL;
-  const int RS = tile_stride(L, W);
+  const int RS = tile_stride(L, W, (int)sizeof(C));
   C* row = sm + (w + W * g) * RS;
   const LineCoord lc = line_coord(geo, base, w, g, j, TPL);
 
@@ -165,7 +165,7 @@ __device__ __forceinline__ void curl_zpass_tile(const LineGeo& geo, const Fields
   using P = LinePlan<L>;
   constexpr int E = P::E, TPL = P::TPL;
   const int W = geo.W, G = geo.G, lines = W * G;
-  const int RS = tile_stride(L, W);
+  const int RS = tile_stride(L, W, (int)sizeof(C));
   const int64_t base = (blk % geo.TA) * geo.sa + (blk / geo.TA) * geo.sb;
   const int w = threadIdx.x & (W - 1);
   const int s = threadIdx.x >> wshift;
@@ -242,7 +242,7 @@ __device__ __forceinline__ void curl_zpass_tile_reload(const LineGeo& geo, const
   using P = LinePlan<L>;
   constexpr int E = P::E, TPL = P::TPL;
   const int W = geo.W, G = geo.G, lines = W * G;
-  const int RS = tile_stride(L, W);
+  const int RS = tile_stride(L, W, (int)sizeof(C));
   const int64_t base = (blk % geo.TA) * geo.sa + (blk / geo.TA) * geo.sb;
   const int w = threadIdx.x & (W - 1);
   const int s = threadIdx.x >> wshift;
@@ -304,7 +304,7 @@ __device__ __forceinline__ void xcross_tile(const Fields& f, const cx_t<T>* __re
                                             T scale2, int64_t blk, int nthr, cx_t<T>* sm) {
   using C = cx_t<T>;
   using P = LinePlan<L>;
-  constexpr int E = P::E, TPL = P::TPL, RS = xrow_stride(L);
+  constexpr int E = P::E, TPL = P::TPL, RS = xrow_stride(L, (int)sizeof(C));
   const int64_t row0 = blk * G;
   const int per = G * L;
 
@@ -412,7 +412,7 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
   constexpr int E = P::E, TPL = P::TPL;
 
   const int W = a.W;
-  const int RS = tile_stride(L, W);
+  const int RS = tile_stride(L, W, (int)sizeof(C));
   const int64_t nxy = (int64_t)a.nx * a.ny;
   const int64_t base = blk * W;
   const int per = W * L;

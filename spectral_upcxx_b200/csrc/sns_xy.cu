@@ -104,7 +104,7 @@ __device__ __forceinline__ void item_ylines(const XYArgs& a, cx_t<T>* sm, int f0
   using P = LinePlan<LY>;
   constexpr int E = P::E, TPL = P::TPL;
   const int W = a.W;
-  const int RS = tile_stride(LY, W);
+  const int RS = tile_stride(LY, W, (int)sizeof(C));
   const int t = threadIdx.x;
   const int fi = t / (W * TPL), rest = t - fi * (W * TPL);
   const int w = rest % W, j = rest / W;
@@ -126,7 +126,7 @@ __device__ __forceinline__ void item_xcross(const XYArgs& a, cx_t<T>* sm, int z,
                                             const cx_t<T>* tw) {
   using C = cx_t<T>;
   using P = LinePlan<LX>;
-  constexpr int E = P::E, TPL = P::TPL, RS = xrow_stride(LX);
+  constexpr int E = P::E, TPL = P::TPL, RS = xrow_stride(LX, (int)sizeof(C));
   const int G = a.G;
   const int t = threadIdx.x;
   const int line = t / TPL, j = t % TPL;
@@ -311,9 +311,9 @@ int xy_plan(XYPlan& p, int nx, int ny, int nz, int prec) {
   p.W = W;
   p.G = G;
   p.threads = 3 * W * tply;
-  p.smem_bytes = (size_t)(3 * W) * tile_stride(ny, W) * esz;
-  if ((size_t)(6 * G) * xrow_stride(nx) * esz > p.smem_bytes)
-    p.smem_bytes = (size_t)(6 * G) * xrow_stride(nx) * esz;
+  p.smem_bytes = (size_t)(3 * W) * tile_stride(ny, W, (int)esz) * esz;
+  if ((size_t)(6 * G) * xrow_stride(nx, (int)esz) * esz > p.smem_bytes)
+    p.smem_bytes = (size_t)(6 * G) * xrow_stride(nx, (int)esz) * esz;
   p.nA = 2 * (nx / W);
   p.nB = ny / G;
   p.nC = nx / W;
