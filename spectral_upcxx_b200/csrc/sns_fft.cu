@@ -492,6 +492,50 @@ int fft3d_tune(int nx, int ny, int nz, int nf, int prec, cudaStream_t stream) {
                  &t_plane);
     c.plane = rc == OK && t_plane < t_lines;
   }
+  // keep the tuned plan only if the whole transform pair beats the default
+  // plan's (pass-by-pass timings of L2-resident fields can mislead)
+  if (rc == OK) {
+    auto whole = [&](const FftChoice* ch, float* t) {
+      return timed([&](int sg) -> int {
+        const int axes_fwd[3] = {0, 1, 2}, axes_inv[3] = {2, 1, 0};
+        const int* order = sg < 0 ? axes_fwd : axes_inv;
+        const bool plane = ch ? ch->plane : true;
+        if (plane && fft_xy_supported(nx, ny, nz, nf, prec)) {
+          LineGeo gz = ch ? axis_geo(2, nx, ny, nz, prec, ch->wmax[2], ch->tmax[2], ch->ord[2])
+                          : axis_geo(2, nx, ny, nz, prec);
+          int e = 0;
+          if (sg < 0) {
+            e = fft_xy_pass(f, nx, nz, sg, 0, 1.0, prec, stream);
+            if (!e && nz > 1) e = run_line_pass(gz, f, sg, 0, 1.0, prec, stream);
+          } else {
+            if (nz > 1) e = run_line_pass(gz, f, sg, 0, 1.0, prec, stream);
+            if (!e) e = fft_xy_pass(f, nx, nz, sg, 0, 1.0, prec, stream);
+          }
+          return e;
+        }
+        for (int i = 0; i < 3; i++) {
+          const int a = order[i];
+          if (dims[a] < 2) continue;
+          LineGeo g = ch ? axis_geo(a, nx, ny, nz, prec, ch->wmax[a], ch->tmax[a], ch->ord[a])
+                         : axis_geo(a, nx, ny, nz, prec);
+          int e = run_line_pass(g, f, sg, 0, 1.0, prec, stream);
+          if (e) return e;
+        }
+        return OK;
+      }, t);
+    };
+    float t_default = 0, t_tuned = 0;
+    rc = whole(nullptr, &t_default);
+    if (rc == OK) rc = whole(&c, &t_tuned);
+    if (rc == OK && t_default <= t_tuned) {
+      for (int a = 0; a < 3; a++) {
+        c.wmax[a] = 0;
+        c.tmax[a] = 0;
+        c.ord[a] = 0;
+      }
+      c.plane = true;
+    }
+  }
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
   for (int i = 0; i < nf; i++) pool_free(fld[i]);
