@@ -85,6 +85,13 @@ int sns_fft3d_many(void* const* fields, int nfields, int64_t nx, int64_t ny, int
  * shape and used by every later transform of that shape (results agree with
  * the default plan to rounding).  SNS_TUNE=1 tunes each new shape on first use. */
 int sns_fft3d_tune(int64_t nx, int64_t ny, int64_t nz, int nfields, int prec, void* stream);
+/* The line passes of selected axes only (bit 0: x, bit 1: y, bit 2: z), in that
+ * order, the last one multiplied by `scale` (1: none).  The local phases of the
+ * slab-distributed transform of Scalar::transform (src/Scalar.cpp:419-566: the
+ * y and x lines of the rank's own z planes, then the z lines of the planes
+ * gathered by the transpose). */
+int sns_fft3d_axes(void* field, int64_t nx, int64_t ny, int64_t nz, int axes, int dir,
+                   double scale, int prec, void* stream);
 /* Scalar::forward(): transform(-1) + zeroHighModes (src/Scalar.cpp:208-215). */
 int sns_forward(void* field, int64_t nx, int64_t ny, int64_t nz, int prec, void* stream);
 /* Scalar::inverse(): transform(+1) then divide by N (src/Scalar.cpp:217-229). */

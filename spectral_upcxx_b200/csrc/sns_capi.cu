@@ -428,6 +428,36 @@ int sns_fft3d(void* field, int64_t nx, int64_t ny, int64_t nz, int dir, int flag
   return sns_fft3d_many(f, 1, nx, ny, nz, dir, flags, prec, stream);
 }
 
+int sns_fft3d_axes(void* field, int64_t nx, int64_t ny, int64_t nz, int axes, int dir,
+                   double scale, int prec, void* stream) {
+  if (!check_prec(prec) || !check_dims(nx, ny, nz) || !nonnull(field, "sns_fft3d_axes"))
+    return ERR_ARG;
+  if ((dir != 1 && dir != -1) || axes < 0 || axes > 7) {
+    set_error("sns_fft3d_axes: dir must be -1 or +1 and axes a mask of bits 0 (x), 1 (y), 2 (z)");
+    return ERR_ARG;
+  }
+  if (!line_supported(nx) || !line_supported(ny) || !line_supported(nz)) {
+    set_error("sns_fft3d_axes: dimensions must be powers of two up to 4096");
+    return ERR_UNSUPPORTED;
+  }
+  const int dims[3] = {(int)nx, (int)ny, (int)nz};
+  int todo[3], na = 0;
+  for (int a = 0; a < 3; a++)
+    if (((axes >> a) & 1) && dims[a] > 1) todo[na++] = a;
+  FieldPtrs f{};
+  f.n = 1;
+  f.in[0] = f.out[0] = field;
+  for (int i = 0; i < na; i++) {
+    const int fl = (i == na - 1 && scale != 1.0) ? PASS_SCALE : 0;
+    int rc = run_line_pass(axis_geo(todo[i], dims[0], dims[1], dims[2], prec), f, dir, fl, scale,
+                           prec, S(stream));
+    if (rc) return rc;
+  }
+  if (na == 0 && scale != 1.0)
+    return sns_axpby(scale, field, 0.0, nullptr, field, (int64_t)nx * ny * nz, prec, stream);
+  return OK;
+}
+
 int sns_forward(void* field, int64_t nx, int64_t ny, int64_t nz, int prec, void* stream) {
   return sns_fft3d(field, nx, ny, nz, -1, SNS_FFT_ZERO_NYQUIST, prec, stream);
 }
