@@ -55,14 +55,15 @@ def pass_names(npasses, plan):
     return [nm % mode if "%s" in nm else nm for nm in names], fields
 STEP_FIELDS = 30  # 9 FFTs x 2 + 12 for the spectral update: 30 N^3 S per step
 
-# DRAM bytes (read + write) per launch of each pass at 256^3 complex64, from the
-# one-pass ncu capture summarised in profiles/ns_step_256_c64_launches.md.
+# DRAM bytes (read + write) per launch of each pass at 256^3 complex64 with the
+# tuned plan, from the one-kernel ncu captures summarised in
+# profiles/ns_step_256_c64_launches.md.
 NCU_TRAFFIC = {
-    ("ns256_fp32", "K1 z-inverse+curl"): (403 + 790) * 1e6,
-    ("ns256_fp32", "K2 y-inverse x6"): (806 + 809) * 1e6,
-    ("ns256_fp32", "K3 x-inv+cross+x-fwd"): (805 + 365) * 1e6,
-    ("ns256_fp32", "K4 y-forward x3"): (403 + 374) * 1e6,
-    ("ns256_fp32", "K5 z-forward+update"): (1208 + 851) * 1e6,
+    ("ns256_fp32", "K1 z-inverse+curl"): (403 + 761) * 1e6,
+    ("ns256_fp32", "K2 y-inverse x6"): (806 + 746) * 1e6,
+    ("ns256_fp32", "K3 x-inv+cross+x-fwd"): (805 + 359) * 1e6,
+    ("ns256_fp32", "K4 y-forward x3"): (403 + 341) * 1e6,
+    ("ns256_fp32", "K5 z-forward+update"): (1208 + 752) * 1e6,
 }
 
 WORKLOADS = {

@@ -161,15 +161,25 @@ __global__ void __launch_bounds__(kTcRows)
   const uint32_t one2 = bf16_bits(1.f) * 0x10001u;
   uint32_t phase = 0;
   const int64_t tiles = (M + kTcRows - 1) / kTcRows;
+  // this thread's input row of a tile (zeros past the end)
+  auto load_row = [&](int64_t tile, uint4& x0, uint4& x1) {
+    const int64_t r = tile * kTcRows + tid;
+    x0 = make_uint4(0, 0, 0, 0);
+    x1 = x0;
+    if (tile < tiles && r < M) {
+      const uint4* src = reinterpret_cast<const uint4*>(X + r * kMlpK1);
+      x0 = src[0];
+      x1 = src[1];
+    }
+  };
+  // the next tile's row is loaded while this tile's MMAs and epilogues run
+  uint4 nx0, nx1;
+  load_row(blockIdx.x, nx0, nx1);
   for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     const int64_t row = tile * kTcRows + tid;
     {
-      uint4 x0 = make_uint4(0, 0, 0, 0), x1 = x0;
-      if (row < M) {
-        const uint4* src = reinterpret_cast<const uint4*>(X + row * kMlpK1);
-        x0 = src[0];
-        x1 = src[1];
-      }
+      uint4 x0 = nx0, x1 = nx1;
+      load_row(tile + gridDim.x, nx0, nx1);
       // columns 9, 10: the constant 1 of the b1 terms
       x1.x = (x1.x & 0xFFFFu) | (one2 & 0xFFFF0000u);
       x1.y = (x1.y & 0xFFFF0000u) | (one2 & 0xFFFFu);
@@ -381,20 +391,33 @@ __global__ void __launch_bounds__(kGtRows)
   float acc_db3 = 0.f, acc_loss = 0.f;
   bool first = true;
   const int64_t tiles = (B + kGtRows - 1) / kGtRows;
+  // this thread's sample of a tile: input row, target and weight (zeros past
+  // the end); the next tile's is loaded while this tile's MMAs run
+  auto load_sample = [&](int64_t tile, uint4& x0, uint4& x1, float& tgt, float& wt) {
+    const int64_t b = tile * kGtRows + tid;
+    x0 = make_uint4(0, 0, 0, 0);
+    x1 = x0;
+    tgt = 0.f;
+    wt = 0.f;
+    if (tile < tiles && b < B) {
+      const int64_t row = idx ? (int64_t)idx[b] : b;
+      const uint4* src = reinterpret_cast<const uint4*>(X + row * kMlpK1);
+      x0 = src[0];
+      x1 = src[1];
+      tgt = target[row];
+      wt = weight ? weight[row] : 1.f;
+    }
+  };
+  uint4 nx0, nx1;
+  float ntgt, nwt;
+  load_sample(blockIdx.x, nx0, nx1, ntgt, nwt);
   for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     const int64_t b = tile * kGtRows + tid;
     const bool valid = b < B;
-    const int64_t row = valid ? (idx ? (int64_t)idx[b] : b) : 0;
-    float tgt = 0.f, wt = 0.f;
+    float tgt = ntgt, wt = nwt;
     {
-      uint4 x0 = make_uint4(0, 0, 0, 0), x1 = x0;
-      if (valid) {
-        const uint4* src = reinterpret_cast<const uint4*>(X + row * kMlpK1);
-        x0 = src[0];
-        x1 = src[1];
-        tgt = target[row];
-        wt = weight ? weight[row] : 1.f;
-      }
+      uint4 x0 = nx0, x1 = nx1;
+      load_sample(tile + gridDim.x, nx0, nx1, ntgt, nwt);
       x1.x = (x1.x & 0xFFFFu) | (one2 & 0xFFFF0000u);
       x1.y = (x1.y & 0xFFFF0000u) | (one2 & 0xFFFFu);
       *reinterpret_cast<uint4*>(S.X + tc::kmajor_off(tid, 0, kMlpK1)) = x0;
