@@ -118,6 +118,7 @@ __device__ __forceinline__ void ens_item(const EnsClass* __restrict__ k,
       a.stats = box->stats;
       a.kc2 = 1e300;
       a.kx_half = 0;
+      a.pf = 0;
     }
     __syncthreads();
     zfwd_update_tile<T, L>(a, tw, blk, (int)blockDim.x, sm, red);

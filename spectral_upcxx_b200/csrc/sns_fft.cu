@@ -126,8 +126,10 @@ static int launch_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int fla
     set_error("line pass: grid too large");
     return ERR_UNSUPPORTED;
   }
+  LineGeo g = geo;
+  g.pf = tiles_in_waves(k_line_pass<T, L, PRO, ORD>, threads, smem, geo.pfw);
   cudaError_t e = launch_pdl(k_line_pass<T, L, PRO, ORD>, dim3((unsigned)blocks), dim3(threads),
-                             smem, stream, geo, f, tw, (T)sign, (T)scale, flags, wshift);
+                             smem, stream, g, f, tw, (T)sign, (T)scale, flags, wshift);
   if (e != cudaSuccess) return cuda_status(e, "k_line_pass");
   return OK;
 }

@@ -82,7 +82,23 @@ struct LineGeo {
   int kx_half;
   // radix order of the line FFT (RadixOrder; plain-load passes of 64..1024)
   int ord;
+  // L2 prefetch: each CTA asks L2 for the inputs of the tile pf launches
+  // ahead (0: none); the launcher sets pf to pfw waves of resident CTAs
+  int64_t pf;
+  int pfw;
 };
+
+// Tiles in `waves` waves of a kernel's resident CTAs on this device.
+template <typename K>
+inline int64_t tiles_in_waves(K* kernel, int threads, size_t smem, int waves) {
+  if (waves <= 0) return 0;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return (int64_t)waves * per_sm * sm_count();
+}
 
 struct FieldPtrs {
   void* in[kMaxFields];

@@ -34,12 +34,12 @@ namespace sns {
 // K3: x lines -- inverse 6 fields, cross product, forward 3 fields.
 template <typename T, int L>
 __global__ void __launch_bounds__(MaxThreads<T>::value)
-    k_xcross(FieldPtrs f, const cx_t<T>* __restrict__ tw, int G, T scale2) {
+    k_xcross(FieldPtrs f, const cx_t<T>* __restrict__ tw, int G, T scale2, int64_t pf) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   pdl_trigger();
   pdl_wait();
   xcross_tile<T, L>(ParamFields{f}, tw, G, scale2, (int64_t)blockIdx.x, (int)blockDim.x,
-                    reinterpret_cast<cx_t<T>*>(smem_raw));
+                    reinterpret_cast<cx_t<T>*>(smem_raw), pf, (int64_t)gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -235,8 +235,9 @@ int launch_xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream
   const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
   const double N = (double)pl.nx * pl.ny * pl.nz;
   const int blocks = (int)(rows / G);
+  const int64_t pf = tiles_in_waves(k_xcross<T, L>, threads, smem, pl.pf_waves);
   cudaError_t e = launch_pdl(k_xcross<T, L>, dim3(blocks), dim3(threads), smem, s, f, tw, G,
-                             (T)(1.0 / (N * N)));
+                             (T)(1.0 / (N * N)), pf);
   if (e != cudaSuccess) return cuda_status(e, "k_xcross");
   return OK;
 }
@@ -278,6 +279,7 @@ int launch_zcurl_as(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
   }
   int wshift = 0;
   while ((1 << wshift) < g.W) wshift++;
+  g.pf = tiles_in_waves(k_zcurl<T, L, RELOAD>, threads, smem, pl.pf_waves);
   cudaError_t e = launch_pdl(k_zcurl<T, L, RELOAD>, dim3((unsigned)(g.TA * g.TB)), dim3(threads),
                              smem, s, g, f, tw, wshift);
   if (e != cudaSuccess) return cuda_status(e, "k_zcurl");
@@ -365,7 +367,9 @@ int launch_update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
     attr[dev & 63] = true;
   }
   const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
-  cudaError_t e = launch_pdl(k_zfwd_update<T, L, SGS>, dim3(blocks), dim3(threads), smem, s, a,
+  UpdateArgs ap = a;
+  ap.pf = SGS ? 0 : tiles_in_waves(k_zfwd_update<T, L, SGS>, threads, smem, pl.pf_waves);
+  cudaError_t e = launch_pdl(k_zfwd_update<T, L, SGS>, dim3(blocks), dim3(threads), smem, s, ap,
                              tw);
   if (e != cudaSuccess) return cuda_status(e, "k_zfwd_update");
   return OK;
@@ -527,6 +531,11 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
   pl.tuned = false;
   pl.k1_lines = false;  // enabled by a caller that provides the work fields W
   {
+    // L2 prefetch of the tile a wave or two ahead (SNS_PF = 0, 1, 2 waves)
+    const char* e = getenv("SNS_PF");
+    pl.pf_waves = e ? std::max(0, std::min(4, atoi(e))) : 0;
+  }
+  {
     const char* e = getenv("SNS_K1_RELOAD");
     pl.k1_reload = e && e[0] == '1';
   }
@@ -605,6 +614,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
       for (int i = 0; i < 6; i++) f.out[i] = Uc[i];
       LineGeo g = axis_geo(1, nx, ny, pz, prec, pl.lineW, pl.lineT, pl.lineOrd);
       g.kx_half = pl.real;
+      g.pfw = pl.pf_waves;
       int r = run_line_pass(g, f, +1, 0, 1.0, prec, s, PRO_OMEGA);
       if (r) return r;
       if (marks) mark();
@@ -613,6 +623,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
       f.n = 6;
       for (int i = 0; i < 6; i++) f.in[i] = f.out[i] = Uc[i];
       LineGeo g = axis_geo(1, nx, ny, pz, prec, pl.lineW, pl.lineT, pl.lineOrd);
+      g.pfw = pl.pf_waves;
       int r = run_line_pass(g, f, +1, 0, 1.0, prec, s);
       if (r) return r;
       if (marks) mark();
@@ -632,6 +643,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
       f.n = 3;
       for (int i = 0; i < 3; i++) f.in[i] = f.out[i] = Uc[i];
       LineGeo g = axis_geo(1, nx, ny, pz, prec, pl.lineW, pl.lineT, pl.lineOrd);
+      g.pfw = pl.pf_waves;
       int r = run_line_pass(g, f, -1, 0, 1.0, prec, s);
       if (r) return r;
     }

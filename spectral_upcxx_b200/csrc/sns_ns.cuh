@@ -28,6 +28,7 @@ struct NSPlan {
   int lineT;          // threads per CTA up to which line groups are added (0 = default)
   int lineOrd;        // radix order of the y line passes (RadixOrder)
   bool tuned;         // the knobs above were chosen by measurement (ns_tune_plan)
+  int pf_waves;       // L2 prefetch of each pass's tile this many waves ahead (0: none)
   int passes;         // timed phases per step: z-inverse, xy, z-forward+update
   bool real;          // half-spectrum fields of a real velocity (R2C / C2R along x)
   int nx_phys;        // physical nx (= nx, or 2 nx for a real-field run)

@@ -48,6 +48,47 @@ __device__ __forceinline__ LineCoord line_coord(const LineGeo& geo, int64_t base
   return c;
 }
 
+// Ask L2 for the 128-byte line holding p (a hint: no register, no wait).
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// Prefetch into L2, spread over the CTA's threads, the tile of a line pass
+// that starts at element `base` of `src`: G groups (gs apart) of L positions
+// (ps apart) of W adjacent elements each; for x lines (ps = 1) the G runs of
+// L + W - 1 contiguous elements.  Every address asked for lies inside the
+// tile's elements.
+template <int L>
+__device__ __forceinline__ void prefetch_lines(const char* src, int64_t base, int W, int G,
+                                               int64_t gs, int64_t ps, int esz, int nthr) {
+  if (ps == 1) {
+    const int per_row = ((L - 1 + W) * esz + 127) / 128;
+    for (int q = threadIdx.x; q < G * per_row; q += nthr) {
+      const int g = q / per_row, c = q - g * per_row;
+      prefetch_l2(src + (base + g * gs) * esz + 128 * c);
+    }
+    return;
+  }
+  const int per_run = (W * esz + 127) / 128;
+  for (int q = threadIdx.x; q < G * L * per_run; q += nthr) {
+    const int c = q % per_run, r = q / per_run;
+    const int g = r / L, p = r - g * L;
+    prefetch_l2(src + (base + g * gs + p * ps) * esz + 128 * c);
+  }
+}
+
+// K1's tile `bp` (the three components of V) into L2, when it exists.
+template <int L, typename C, typename Fields>
+__device__ __forceinline__ void prefetch_curl_tile(const LineGeo& geo, const Fields& f,
+                                                   int64_t bp) {
+  if (geo.pf <= 0 || bp >= geo.TA * geo.TB) return;
+  const int64_t basep = (bp % geo.TA) * geo.sa + (bp / geo.TA) * geo.sb;
+#pragma unroll
+  for (int d = 0; d < 3; d++)
+    prefetch_lines<L>(reinterpret_cast<const char*>(f.in(d)), basep, geo.W, geo.G, geo.gs, geo.ps,
+                      (int)sizeof(C), (int)blockDim.x);
+}
+
 // Element of the thread's line as the prologue forms it.
 // PRO_OMEGA: v0..v2 are the z-inverted components of V and d0, d1 the
 // z-inverted i kz Vx, i kz Vy (the z derivative taken before the z pass).
@@ -86,6 +127,15 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
   const int64_t t = blk / nf;
   const int64_t base = (t % geo.TA) * geo.sa + (t / geo.TA) * geo.sb;
   const int W = geo.W;
+  if constexpr (PRO == PRO_LOAD || PRO == PRO_IKAXIS) {
+    const int64_t bp = blk + geo.pf;
+    if (geo.pf > 0 && bp < geo.TA * geo.TB * nf) {
+      const int64_t tp = bp / nf;
+      prefetch_lines<L>(reinterpret_cast<const char*>(f.in((int)(bp % nf))),
+                        (tp % geo.TA) * geo.sa + (tp / geo.TA) * geo.sb, W, geo.G, geo.gs,
+                        geo.ps, (int)sizeof(C), (int)blockDim.x);
+    }
+  }
   const int w = threadIdx.x & (W - 1);
   const int s = threadIdx.x >> wshift;
   const int j = s & (TPL - 1);
@@ -167,6 +217,7 @@ __device__ __forceinline__ void curl_zpass_tile(const LineGeo& geo, const Fields
   const int W = geo.W, G = geo.G, lines = W * G;
   const int RS = tile_stride(L, W, (int)sizeof(C));
   const int64_t base = (blk % geo.TA) * geo.sa + (blk / geo.TA) * geo.sb;
+  prefetch_curl_tile<L, C>(geo, f, blk + geo.pf);
   const int w = threadIdx.x & (W - 1);
   const int s = threadIdx.x >> wshift;
   const int j = s & (TPL - 1);
@@ -244,6 +295,7 @@ __device__ __forceinline__ void curl_zpass_tile_reload(const LineGeo& geo, const
   const int W = geo.W, G = geo.G, lines = W * G;
   const int RS = tile_stride(L, W, (int)sizeof(C));
   const int64_t base = (blk % geo.TA) * geo.sa + (blk / geo.TA) * geo.sb;
+  prefetch_curl_tile<L, C>(geo, f, blk + geo.pf);
   const int w = threadIdx.x & (W - 1);
   const int s = threadIdx.x >> wshift;
   const int j = s & (TPL - 1);
@@ -301,12 +353,20 @@ __device__ __forceinline__ void curl_zpass_tile_reload(const LineGeo& geo, const
 // rows of all six fields; f.in(0..5) = (u, omega), f.out(0..2) = the product.
 template <typename T, int L, typename Fields>
 __device__ __forceinline__ void xcross_tile(const Fields& f, const cx_t<T>* __restrict__ tw, int G,
-                                            T scale2, int64_t blk, int nthr, cx_t<T>* sm) {
+                                            T scale2, int64_t blk, int nthr, cx_t<T>* sm,
+                                            int64_t pf = 0, int64_t nblk = 0) {
   using C = cx_t<T>;
   using P = LinePlan<L>;
   constexpr int E = P::E, TPL = P::TPL, RS = xrow_stride(L, (int)sizeof(C));
   const int64_t row0 = blk * G;
   const int per = G * L;
+  if (pf > 0 && blk + pf < nblk) {
+    // the six input rows of tile blk + pf into L2
+#pragma unroll
+    for (int fl = 0; fl < 6; fl++)
+      prefetch_lines<L>(reinterpret_cast<const char*>(f.in(fl)), (blk + pf) * G * L, 1, G, L, 1,
+                        (int)sizeof(C), nthr);
+  }
 
   // thread t owns line t / TPL (field-major: field = line / G, row = line % G)
   // at positions j + e*TPL; loads go straight to registers, E per thread
@@ -386,6 +446,8 @@ struct UpdateArgs {
   int kx_half;  // half-spectrum fields (see LineGeo::kx_half)
   // SGS: the stress divergence is weighted by clamp((|k| - sgs_klo) sgs_kinv, 0, 1)
   double sgs_klo, sgs_kinv;
+  // L2 prefetch distance in tiles (0: none)
+  int64_t pf;
 };
 
 // Field f of the update's z-forward: the cross product (f < 3) or, with the
@@ -416,6 +478,19 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
   const int64_t nxy = (int64_t)a.nx * a.ny;
   const int64_t base = blk * W;
   const int per = W * L;
+  if (!SGS && a.pf > 0 && (blk + a.pf) * W < nxy) {
+    // tile blk + pf's cross product, V and C0 into L2
+    const int64_t bp = (blk + a.pf) * W;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      prefetch_lines<L>(reinterpret_cast<const char*>(a.U[d]), bp, W, 1, 0, nxy, (int)sizeof(C),
+                        nthr);
+      prefetch_lines<L>(reinterpret_cast<const char*>(a.V[d]), bp, W, 1, 0, nxy, (int)sizeof(C),
+                        nthr);
+      prefetch_lines<L>(reinterpret_cast<const char*>(a.C0[d]), bp, W, 1, 0, nxy, (int)sizeof(C),
+                        nthr);
+    }
+  }
 
   // thread t owns z line (field, base + w) at positions j + e*TPL with
   // w = t mod W, j = (t / W) mod TPL, field = t / (W*TPL): consecutive threads

@@ -1,6 +1,6 @@
 """Parity at the benchmark sizes against the reference's own code.
 
-The 3D transforms of the standalone FFT workload (128^3, 256^3, and a
+The 3D transforms of the standalone FFT workload (128^3, 256^3, 512^3, and a
 non-cubic 16 x 256 x 512 box whose y and z lines are long and strided) and the
 first two steps of the 256^3 NS workload are compared with the reference's
 src/Scalar.cpp / exec/ns.cpp compiled in place (oracle/_ref).  The 128^3
@@ -41,7 +41,8 @@ def ref(oracle):
 
 
 @pytest.mark.parametrize("dtype", DT)
-@pytest.mark.parametrize("shape", [(128, 128, 128), (256, 256, 256), (512, 256, 16)])
+@pytest.mark.parametrize("shape", [(128, 128, 128), (256, 256, 256), (512, 512, 512),
+                                   (512, 256, 16)])
 def test_fft3d_matches_reference_full_size(sns, ref, cuda, dtype, shape):
     """Raw forward (Scalar::transform(-1) without ZERO), Scalar::forward with
     Nyquist zeroing, and Scalar::inverse against the reference build, on the

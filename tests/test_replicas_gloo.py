@@ -38,7 +38,8 @@ def _worker(rank, world, port, out):
 def test_two_gloo_ranks_max_time_and_whole_job_rate():
     world = 2
     port = _free_port()
-    with mp.Manager() as m:
+    # the manager process is spawned too: a fork of this (threaded) process is unsafe
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)
