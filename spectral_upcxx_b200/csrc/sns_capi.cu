@@ -935,7 +935,10 @@ int sns_ns_check(sns_ns* h) {
   if ((rc = cuda_status(cudaStreamSynchronize(h->s), "sns_ns_check"))) return rc;
   if (err) {
     cudaMemsetAsync(h->sync_words + err_index, 0, sizeof(int), h->s);
-    set_error("sns_ns_step: a wait of the xy dataflow pass gave up; results are invalid");
+    set_error(err == 2 ? "sns_ns_step: the TMA-staged z pass refused a tile box (alignment or "
+                         "range); results are invalid"
+                       : "sns_ns_step: a bounded wait of a step pass (the xy dataflow pass or the "
+                         "TMA-staged z pass) gave up; results are invalid");
     return ERR_TIMEOUT;
   }
   return OK;
@@ -1057,12 +1060,14 @@ int sns_ns_describe(sns_ns* h, char* buf, int len) {
   char tmp[256];
   const char* ord[3] = {"16-first", "remainder-first", "radix-8"};
   const int n = snprintf(tmp, sizeof(tmp),
-                         "passes=%d xy=%s k1=%dx%d%s y=W%d/T%d/%s zW=%d xG=%d%s%s",
+                         "passes=%d xy=%s k1=%dx%d%s y=W%d/T%d/%s zW=%d xG=%d pf=%d%s%s",
                          h->cl.model != CLOSURE_NONE ? kLESLaunches : p.passes, xy,
                          p.k1_lines ? p.k1lW : p.k1W, p.k1_lines ? p.k1lT : p.k1G,
-                         p.k1_lines ? "(lines)" : !p.k1_fused ? "(split)" : p.k1_reload ? "(reload)" : "",
+                         p.k1_lines ? "(lines)" : !p.k1_fused ? "(split)"
+                         : p.k1_tma ? (p.k1_stages == 1 ? "(tma1)" : "(tma2)")
+                         : p.k1_reload ? "(reload)" : "",
                          p.lineW, p.lineT,
-                         ord[p.lineOrd % 3], p.zW, p.xG, p.real ? " real" : "",
+                         ord[p.lineOrd % 3], p.zW, p.xG, p.pf_waves, p.real ? " real" : "",
                          p.tuned ? " tuned" : "");
   if (buf && len > 0) {
     strncpy(buf, tmp, (size_t)len - 1);

@@ -27,6 +27,7 @@
 #include "sns_ns.cuh"
 #include "sns_ops.cuh"
 #include "sns_tiles.cuh"
+#include "sns_tma.cuh"
 
 namespace sns {
 
@@ -171,6 +172,108 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
                           reinterpret_cast<cx_t<T>*>(smem_raw));
 }
 
+// K1 with TMA-staged tiles.  A persistent CTA walks the tiles blockIdx.x,
+// blockIdx.x + gridDim.x, ...; the three components of V of a tile come into
+// shared memory as TMA boxes (W x G x L elements each, one box per component
+// and 256 z planes) while the CTA transforms the tile before it, so the
+// HBM reads overlap the line FFTs instead of preceding them.  S = 2: two
+// stages, the next tile's load is issued as the current tile starts; S = 1:
+// one stage, refilled as soon as the current tile's last read of it is done
+// (before its omega transforms).  Every wait on a stage is bounded: a wait
+// that runs out sets *err, waits (with the full budget again) for the CTA's
+// copies still in flight and ends the CTA.  stall_cycles > 0 is the test of
+// that path: the first tile's wait also waits that long on a barrier that
+// nothing arrives at.
+template <typename T, int L, int S>
+__global__ void __launch_bounds__(MaxThreads<T>::value)
+    k_zcurl_tma(const __grid_constant__ CUtensorMap m0, const __grid_constant__ CUtensorMap m1,
+                const __grid_constant__ CUtensorMap m2, const LineGeo geo, const FieldPtrs f,
+                const cx_t<T>* __restrict__ tw, int wshift, int* err, long long stall_cycles) {
+  using C = cx_t<T>;
+  constexpr int ZB = L < 256 ? L : 256;  // z planes per box
+  // the TMA writes to 128-byte aligned shared memory: the stages start at the
+  // first 128-byte boundary of the dynamic block (the launch adds the slack),
+  // then the rows, then the mbarriers (the stages', then the stall test's)
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lines = geo.W * geo.G;
+  const int comp = lines * L;  // elements of one component's tile
+  const uint32_t raw = tc::smem_u32(smem_raw);
+  C* stage0 = reinterpret_cast<C*>(smem_raw + (((raw + 127u) & ~127u) - raw));
+  C* rows = stage0 + S * 3 * comp;
+  uint64_t* full = reinterpret_cast<uint64_t*>(rows + 3 * lines * tile_stride(L, geo.W, (int)sizeof(C)));
+  const int64_t ntiles = geo.TA * geo.TB;
+  const int64_t stride = gridDim.x;
+  pdl_trigger();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k <= S; k++) tc::mbar_init(&full[k], 1);
+    tma::prefetch_map(&m0);
+    tma::prefetch_map(&m1);
+    tma::prefetch_map(&m2);
+  }
+  __syncthreads();
+  // V is written by the step before (its update pass)
+  pdl_wait();
+  auto issue = [&](int64_t blk, int k) {  // thread 0
+    const int u = (int)(sizeof(C) / 8);
+    const int x0 = (int)((blk % geo.TA) * geo.W) * u, y0 = (int)((blk / geo.TA) * geo.G);
+    C* st = stage0 + k * 3 * comp;
+    // self-check of the box (16-byte aligned x, inside the field, 128-byte
+    // aligned destination): a bad one is recorded and not loaded, and the
+    // stage's barrier is released without it
+    if ((x0 & 1) || x0 + geo.W * u > geo.nx * u || y0 + geo.G > geo.ny ||
+        (tc::smem_u32(st) & 127u)) {
+      atomicExch(err, 2);
+      tma::arrive(&full[k]);
+      return;
+    }
+    tma::expect_tx(&full[k], (uint32_t)(3 * comp * sizeof(C)));
+#pragma unroll 1
+    for (int z0 = 0; z0 < L; z0 += ZB) {
+      tma::load_3d(st + z0 * lines, &m0, x0, y0, z0, &full[k]);
+      tma::load_3d(st + comp + z0 * lines, &m1, x0, y0, z0, &full[k]);
+      tma::load_3d(st + 2 * comp + z0 * lines, &m2, x0, y0, z0, &full[k]);
+    }
+  };
+  const int64_t first = blockIdx.x;
+  if (threadIdx.x == 0 && first < ntiles) issue(first, 0);
+  int it = 0;
+#pragma unroll 1
+  for (int64_t blk = first; blk < ntiles; blk += stride, it++) {
+    const int k = S == 1 ? 0 : (it & 1);
+    const uint32_t par = S == 1 ? (uint32_t)(it & 1) : (uint32_t)((it >> 1) & 1);
+    const bool more = blk + stride < ntiles;
+    if (S == 2 && threadIdx.x == 0 && more) {
+      // stage k ^ 1 was last read by the previous tile, before the barrier
+      // that closed it
+      tma::fence_proxy_async();
+      issue(blk + stride, k ^ 1);
+    }
+    bool ok = tc::mbar_wait(&full[k], par, tc::kWaitCycles);
+    if (stall_cycles > 0 && it == 0) ok = ok && tc::mbar_wait(&full[S], 0, stall_cycles);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+        tc::mbar_wait(&full[k], par, tc::kWaitCycles);
+        if (S == 2 && more) tc::mbar_wait(&full[k ^ 1], (uint32_t)(((it + 1) >> 1) & 1), tc::kWaitCycles);
+      }
+      __syncthreads();
+      return;
+    }
+    curl_zpass_tile_staged<T, L>(geo, ParamFields{f}, tw, wshift, blk, stage0 + k * 3 * comp, rows,
+                                 [&] {
+                                   if (S == 1) {
+                                     __syncthreads();
+                                     if (threadIdx.x == 0 && more) {
+                                       tma::fence_proxy_async();
+                                       issue(blk + stride, 0);
+                                     }
+                                   }
+                                 });
+    // the stage and the rows are free for the next tile
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // K5: z lines -- forward 3 fields + Nyquist zeroing, then the AB2 /
 // projection / CN update per mode.
@@ -286,8 +389,96 @@ int launch_zcurl_as(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
   return OK;
 }
 
+// Shared memory of the TMA-staged K1: S stages of the three components'
+// W x G x L tiles, then the 3 W G padded rows of the line FFTs' exchanges,
+// 128 bytes of alignment slack and the S + 1 mbarriers.
+inline size_t zcurl_tma_smem(int L, int W, int G, int S, size_t esz) {
+  return ((size_t)S * 3 * W * G * L + (size_t)3 * W * G * tile_stride(L, W, (int)esz)) * esz +
+         128 + 8 * (size_t)(S + 1);
+}
+
+// Whether the TMA-staged K1 can run W x G tiles with S stages on the box.
+bool k1_tma_ok(const NSPlan& p, int W, int G, int S) {
+  if (p.nz < 16 || p.nz > 1024) return false;
+  const int TPL = p.nz / 16;
+  const int esz = p.prec == PREC_C128 ? 16 : 8;
+  const int zb = p.nz < 256 ? p.nz : 256;
+  return p.nx % W == 0 && p.ny % G == 0 && 3 * W * G * TPL <= max_threads(p.prec) &&
+         zcurl_tma_smem(p.nz, W, G, S, esz) <= 220 * 1024 &&
+         field_box_ok(p.nx, p.ny, p.nz, esz, W, G, zb);
+}
+
+// Stall test of the TMA-staged K1 (SNS_K1_STALL_TEST=<cycles>; 0: none).
+inline long long zcurl_stall_cycles() {
+  const char* e = getenv("SNS_K1_STALL_TEST");
+  const long long v = e ? atoll(e) : 0;
+  return v > 0 ? v : 0;
+}
+
+template <typename T, int L, int S>
+int launch_zcurl_tma(const NSPlan& pl, const FieldPtrs& f, int* err, cudaStream_t s) {
+  using C = cx_t<T>;
+  constexpr int TPL = LinePlan<L>::TPL;
+  constexpr int ZB = L < 256 ? L : 256;
+  LineGeo g{};
+  g.L = L;
+  g.W = pl.k1W;
+  g.G = pl.k1G;
+  g.axis = 2;
+  g.nx = pl.nx;
+  g.ny = pl.ny;
+  g.nz = pl.nz;
+  g.kx_half = pl.real;
+  g.ps = (int64_t)pl.nx * pl.ny;
+  g.gs = pl.nx;
+  g.TA = pl.nx / g.W;
+  g.TB = pl.ny / g.G;
+  g.sa = g.W;
+  g.sb = (int64_t)g.G * pl.nx;
+  const int threads = 3 * g.W * g.G * TPL;
+  const size_t smem = zcurl_tma_smem(L, g.W, g.G, S, sizeof(C));
+  CUtensorMap m[3];
+  for (int d = 0; d < 3; d++) {
+    const int rc = field_tensor_map(&m[d], f.in[d], pl.nx, pl.ny, pl.nz, (int)sizeof(C), g.W,
+                                    g.G, ZB);
+    if (rc) return rc;
+  }
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr[dev & 63]) {
+    cudaError_t e = allow_max_dynamic_smem(k_zcurl_tma<T, L, S>);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_zcurl_tma)");
+    attr[dev & 63] = true;
+  }
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_zcurl_tma<T, L, S>,
+                                                                threads, smem);
+  if (e != cudaSuccess) return cuda_status(e, "occupancy(k_zcurl_tma)");
+  if (per_sm < 1) {
+    set_error("K1 TMA tile: does not fit on an SM");
+    return ERR_UNSUPPORTED;
+  }
+  const int64_t ntiles = g.TA * g.TB;
+  const int blocks = (int)std::min<int64_t>(ntiles, (int64_t)per_sm * sm_count());
+  const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
+  if (!tw) {
+    set_error("twiddle table allocation failed");
+    return ERR_ALLOC;
+  }
+  int wshift = 0;
+  while ((1 << wshift) < g.W) wshift++;
+  e = launch_pdl(k_zcurl_tma<T, L, S>, dim3((unsigned)blocks), dim3(threads), smem, s, m[0], m[1],
+                 m[2], g, f, tw, wshift, err, zcurl_stall_cycles());
+  if (e != cudaSuccess) return cuda_status(e, "k_zcurl_tma");
+  return OK;
+}
+
 template <typename T, int L>
-int launch_zcurl(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
+int launch_zcurl(const NSPlan& pl, const FieldPtrs& f, int* err, cudaStream_t s) {
+  if (pl.k1_tma && err)
+    return pl.k1_stages == 1 ? launch_zcurl_tma<T, L, 1>(pl, f, err, s)
+                             : launch_zcurl_tma<T, L, 2>(pl, f, err, s);
   return pl.k1_reload ? launch_zcurl_as<T, L, true>(pl, f, s)
                       : launch_zcurl_as<T, L, false>(pl, f, s);
 }
@@ -335,17 +526,17 @@ int xcross_r2c(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream_t 
 }
 
 template <typename T>
-int zcurl(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
+int zcurl(const NSPlan& pl, const FieldPtrs& f, int* err, cudaStream_t s) {
   switch (pl.nz) {
-    case 4: return launch_zcurl<T, 4>(pl, f, s);
-    case 8: return launch_zcurl<T, 8>(pl, f, s);
-    case 16: return launch_zcurl<T, 16>(pl, f, s);
-    case 32: return launch_zcurl<T, 32>(pl, f, s);
-    case 64: return launch_zcurl<T, 64>(pl, f, s);
-    case 128: return launch_zcurl<T, 128>(pl, f, s);
-    case 256: return launch_zcurl<T, 256>(pl, f, s);
-    case 512: return launch_zcurl<T, 512>(pl, f, s);
-    case 1024: return launch_zcurl<T, 1024>(pl, f, s);
+    case 4: return launch_zcurl<T, 4>(pl, f, err, s);
+    case 8: return launch_zcurl<T, 8>(pl, f, err, s);
+    case 16: return launch_zcurl<T, 16>(pl, f, err, s);
+    case 32: return launch_zcurl<T, 32>(pl, f, err, s);
+    case 64: return launch_zcurl<T, 64>(pl, f, err, s);
+    case 128: return launch_zcurl<T, 128>(pl, f, err, s);
+    case 256: return launch_zcurl<T, 256>(pl, f, err, s);
+    case 512: return launch_zcurl<T, 512>(pl, f, err, s);
+    case 1024: return launch_zcurl<T, 1024>(pl, f, err, s);
     default: set_error("fused NS step: nz must be a power of two in [4, 1024]"); return ERR_UNSUPPORTED;
   }
 }
@@ -539,6 +730,29 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
     const char* e = getenv("SNS_K1_RELOAD");
     pl.k1_reload = e && e[0] == '1';
   }
+  {
+    // K1 over TMA-staged tiles, one stage by default (SNS_K1_TMA = 0: off,
+    // 2: two stages); an explicit SNS_K1_RELOAD=1 or SNS_K1_SPLIT=1 keeps
+    // that form.  Measured on B200 at 256^3: complex64 0.28 ms against 0.37
+    // (reload tile), complex128 0.58 against 0.79 (split).
+    const char* e = getenv("SNS_K1_TMA");
+    const char* es = getenv("SNS_K1_SPLIT");
+    const int v = e ? atoi(e) : ((pl.k1_reload || (es && es[0] == '1')) ? 0 : 1);
+    pl.k1_stages = v == 2 ? 2 : 1;
+    pl.k1_tma = false;
+    if (v == 1 || v == 2) {
+      // the widest tile of at most 384 threads that fits the stages
+      const int TPL = nz / elems(nz);
+      for (int W = 16; W >= 1 && !pl.k1_tma; W /= 2)
+        for (int G = 4; G >= 1 && !pl.k1_tma; G /= 2)
+          if (3 * W * G * TPL <= 384 && k1_tma_ok(pl, W, G, pl.k1_stages)) {
+            pl.k1_tma = true;
+            pl.k1_fused = true;
+            pl.k1W = W;
+            pl.k1G = G;
+          }
+    }
+  }
   pl.k1lW = 0;
   pl.k1lT = 0;
   pl.kc2 = 1e300;
@@ -581,7 +795,9 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     for (int d = 0; d < 3; d++) f.in[d] = V[d];
     for (int i = 0; i < 6; i++) f.out[i] = U[i];
     if (pl.k1_fused) {
-      rc = prec == PREC_C128 ? zcurl<double>(pl, f, s) : zcurl<float>(pl, f, s);
+      // the error word of the step's bounded waits
+      int* err = sync_words ? sync_words + xy_sync_words(nz) - 1 : nullptr;
+      rc = prec == PREC_C128 ? zcurl<double>(pl, f, err, s) : zcurl<float>(pl, f, err, s);
     } else {
       LineGeo g = axis_geo(2, nx, ny, nz, prec, pl.lineW);
       g.kx_half = pl.real;
@@ -808,17 +1024,35 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
             q.k1_fused = true;
             q.k1_reload = reload;
             q.k1_lines = false;
+            q.k1_tma = false;
             c.push_back(q);
           }
+    // the persistent pass over TMA-staged tiles (one or two stages)
+    if (sync_words)
+      for (int S = 1; S <= 2; S++)
+        for (int Wd : {2, 4, 8, 16})
+          for (int G : {1, 2, 4})
+            if (k1_tma_ok(pl, Wd, G, S)) {
+              NSPlan q = pl;
+              q.k1W = Wd;
+              q.k1G = G;
+              q.k1_fused = true;
+              q.k1_tma = true;
+              q.k1_stages = S;
+              q.k1_lines = false;
+              c.push_back(q);
+            }
     NSPlan split = pl;
     split.k1_fused = false;
     split.k1_lines = false;
+    split.k1_tma = false;
     c.push_back(split);
     if (W)
       for (int Wd : {8, 16})
         for (int T : {256, 512}) {
           NSPlan q = pl;
           q.k1_lines = true;
+          q.k1_tma = false;
           q.k1lW = Wd;
           q.k1lT = T;
           c.push_back(q);
@@ -868,6 +1102,17 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
         c.push_back(q);
       }
     if (!c.empty()) rc = pick(c, 0x10u);
+  }
+  // L2 prefetch distance of all five passes, timed over the whole step
+  // (unless SNS_PF fixes it)
+  if (rc == OK && !getenv("SNS_PF")) {
+    c.clear();
+    for (int pw : {0, 1, 2}) {
+      NSPlan q = pl;
+      q.pf_waves = pw;
+      c.push_back(q);
+    }
+    rc = pick(c, 0x1Fu);
   }
   for (int i = 0; i < made; i++) cudaEventDestroy(ev[i]);
   if (rc == OK) pl.tuned = true;

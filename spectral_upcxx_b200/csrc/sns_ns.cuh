@@ -13,6 +13,8 @@ struct NSPlan {
   int k1W, k1G;       // K1 tile: adjacent z lines x groups (all six outputs per CTA)
   bool k1_fused;      // K1 loads V once per tile (else one output field per CTA)
   bool k1_reload;     // the fused K1 forms omega from reloads of V (L1), not shared memory
+  bool k1_tma;        // the fused K1 as a persistent pass over TMA-staged tiles
+  int k1_stages;      // its stages (1 or 2)
   bool k1_lines;      // K1 as a line pass of V and i kz V (5 fields into the work
                       // fields W), the curl formed in K2's prologue (PRO_OMEGA)
   int k1lW, k1lT;     // tile knobs of that z line pass (axis_geo wmax, tmax)

@@ -347,6 +347,73 @@ __device__ __forceinline__ void curl_zpass_tile_reload(const LineGeo& geo, const
   }
 }
 
+// K1 from a staged tile: the three components of V for the tile are already
+// in shared memory (`stage`, put there by the TMA): component c, position p
+// of line (w, g) at c L W G + (p G + g) W + w, the [z][y][x] order of the
+// TMA box.  The arithmetic is curl_zpass_tile_reload's with its loads of V
+// read from the stage, so both give the same bits.  after_reads() is called
+// by every thread once the tile's last read of the stage is issued (the CTA
+// may then refill the stage).
+template <typename T, int L, typename Fields, typename AfterReads>
+__device__ __forceinline__ void curl_zpass_tile_staged(const LineGeo& geo, const Fields& f,
+                                                       const cx_t<T>* __restrict__ tw,
+                                                       int wshift, int64_t blk,
+                                                       const cx_t<T>* stage, cx_t<T>* sm,
+                                                       AfterReads after_reads) {
+  using C = cx_t<T>;
+  using P = LinePlan<L>;
+  constexpr int E = P::E, TPL = P::TPL;
+  const int W = geo.W, G = geo.G, lines = W * G;
+  const int RS = tile_stride(L, W, (int)sizeof(C));
+  const int64_t base = (blk % geo.TA) * geo.sa + (blk / geo.TA) * geo.sb;
+  const int w = threadIdx.x & (W - 1);
+  const int s = threadIdx.x >> wshift;
+  const int j = s & (TPL - 1);
+  const int s2 = s / TPL;
+  const int g = s2 % G, d = s2 / G;  // line (w, g) of component d
+  C* row = sm + (d * lines + w + W * g) * RS;
+  const LineCoord lc = line_coord(geo, base, w, g, j, TPL);
+  const int q0 = j * lines + g * W + w, qs = TPL * lines, comp = L * lines;
+  C v[E];
+  {
+    const C* sv = stage + d * comp;
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = sv[q0 + e * qs];
+  }
+  line_fft<L, true>(v, row, j, tw, (T)1);
+  {
+    C* __restrict__ dst = reinterpret_cast<C*>(d == 0 ? f.out(0) : d == 1 ? f.out(1) : f.out(2));
+#pragma unroll
+    for (int e = 0; e < E; e++) dst[lc.idx0 + e * lc.step] = v[e];
+  }
+  {
+    // (ky Vz - kz Vy, kz Vx - kx Vz, kx Vy - ky Vx) times i, as curl_zpass_tile forms it
+    const C* pa = stage + (d == 0 ? 2 : d == 1 ? 0 : 1) * comp;
+    const C* pb = stage + (d == 0 ? 1 : d == 1 ? 2 : 0) * comp;
+    const T kx = geo.kx_half ? (T)lc.x : (T)freq_i(lc.x, geo.nx);
+    const T ky = (T)freq_i(lc.y, geo.ny);
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int q = q0 + e * qs;
+      const T kz = (T)freq_i(j + TPL * e, geo.nz);
+      const C a = pa[q], b = pb[q];
+      if (d == 0)
+        v[e] = csub(ikmul(ky, a), ikmul(kz, b));
+      else if (d == 1)
+        v[e] = csub(ikmul(kz, a), ikmul(kx, b));
+      else
+        v[e] = csub(ikmul(kx, a), ikmul(ky, b));
+    }
+  }
+  after_reads();
+  line_fft<L, true>(v, row, j, tw, (T)1);
+  {
+    C* __restrict__ dst = reinterpret_cast<C*>(d == 0 ? f.out(3) : d == 1 ? f.out(4) : f.out(5));
+#pragma unroll
+    for (int e = 0; e < E; e++) dst[lc.idx0 + e * lc.step] = v[e];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // K3 of the NS step: x lines -- inverse 6 fields, 1/N^2-scaled complex cross
 // product u x omega, forward 3 fields (src/Vector.cpp:79-89).  A tile is G

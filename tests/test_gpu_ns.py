@@ -263,3 +263,43 @@ def test_k1_variants_match(sns, cuda, dtype, variant, tag, monkeypatch):
     tol = 1e-13 if dtype == torch.complex128 else 2e-6
     for a, b in zip(out["1"], out["0"]):
         assert (torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)).item() < tol
+
+
+def _random_fourier(shape, dtype, device, seed):
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    return [torch.complex(torch.randn(shape, generator=g, dtype=torch.float64),
+                          torch.randn(shape, generator=g, dtype=torch.float64)).to(device, dtype)
+            for _ in range(3)]
+
+
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (32, 64, 128), (512, 16, 32)])
+def test_k1_tma_stages_match_reload_bit_for_bit(sns, cuda, dtype, shape, monkeypatch):
+    """K1 as a persistent pass over TMA-staged tiles (SNS_K1_TMA=1: one stage,
+    2: two) does the arithmetic of the reload tile with V read from shared
+    memory instead of HBM, so three steps are identical bit for bit.  The
+    non-cubic boxes give tiles of other widths, and nz = 512 loads each
+    component of a tile as two boxes of 256 planes."""
+    N = sns._native
+    V = _random_fourier(shape, dtype, cuda, 5)
+    out = {}
+    monkeypatch.setenv("SNS_GRAPH", "0")
+    for mode in ("reload", "1", "2"):
+        monkeypatch.delenv("SNS_K1_TMA", raising=False)
+        monkeypatch.delenv("SNS_K1_RELOAD", raising=False)
+        if mode == "reload":
+            monkeypatch.setenv("SNS_K1_RELOAD", "1")
+        else:
+            monkeypatch.setenv("SNS_K1_TMA", mode)
+        st = sns.NSStepper(shape, 1 / 400, 5e-4, dtype)
+        if mode != "reload":
+            assert f"(tma{mode})" in st.describe(), st.describe()
+        st.bootstrap(V, sns.curl(V))
+        st.step(3)
+        rc = N.lib().sns_ns_check(st.h)
+        assert rc == N.SNS_OK, (mode, rc, N.last_error(), st.describe())
+        out[mode] = [x.clone() for x in st.state()["V1"]] + [x.clone() for x in st.state()["cross0"]]
+        st.close()
+    for mode in ("1", "2"):
+        for a, b in zip(out[mode], out["reload"]):
+            assert torch.equal(a, b), mode

@@ -6,6 +6,9 @@
   ends (every access stays in bounds), sns_ns_check reports SNS_ERR_TIMEOUT
   and clears the record, and a stepper run afterwards with the normal budget
   succeeds and matches the separate passes.
+* The TMA-staged z pass of the step (SNS_K1_TMA) with a stall test
+  (SNS_K1_STALL_TEST=<cycles>): the first tile waits on a barrier nothing
+  arrives at; sns_ns_check reports SNS_ERR_TIMEOUT, and the next run is normal.
 * The tcgen05 MLP inference with a stall test (SNS_TC_STALL_TEST=<cycles>):
   each CTA also waits on a barrier nothing arrives at; the wait runs out,
   sns_mlp_status reports SNS_ERR_TIMEOUT, the MMA already issued is still
@@ -74,3 +77,39 @@ def test_tensor_core_wait_runs_out_and_recovers(sns, cuda, monkeypatch):
     got = m.infer(X)
     assert N.lib().sns_mlp_status() == N.SNS_OK
     assert torch.equal(got, want)
+
+
+def test_tma_stage_wait_runs_out_and_recovers(sns, cuda, monkeypatch):
+    """The TMA-staged K1 with a stall test (SNS_K1_STALL_TEST=<cycles>): the
+    first tile's wait also waits on a barrier that nothing arrives at, runs
+    out, and the CTA records the timeout, waits for its copies in flight and
+    ends; sns_ns_check reports SNS_ERR_TIMEOUT and clears the record, and a
+    stepper run afterwards without the stall matches the reload tile."""
+    from spectral_upcxx_b200 import ic
+    N = sns._native
+    n = 64
+    V = [x.to(torch.complex64) for x in ic.solenoidal_spectrum_hat(n, 4, cuda)]
+    monkeypatch.setenv("SNS_GRAPH", "0")
+    monkeypatch.setenv("SNS_K1_TMA", "2")
+    monkeypatch.setenv("SNS_K1_STALL_TEST", "20000")
+    st = sns.NSStepper((n, n, n), 1 / 400, 5e-4, torch.complex64)
+    assert "(tma2)" in st.describe()
+    st.bootstrap(V, sns.curl(V))
+    st.step(1)
+    assert N.lib().sns_ns_check(st.h) == N.SNS_ERR_TIMEOUT
+    assert "gave up" in N.last_error()
+    assert N.lib().sns_ns_check(st.h) == N.SNS_OK  # the record was cleared
+    st.close()
+    monkeypatch.delenv("SNS_K1_STALL_TEST")
+    out = {}
+    for env in ("SNS_K1_TMA", "SNS_K1_RELOAD"):
+        monkeypatch.delenv("SNS_K1_TMA", raising=False)
+        monkeypatch.setenv(env, "2" if env == "SNS_K1_TMA" else "1")
+        st = sns.NSStepper((n, n, n), 1 / 400, 5e-4, torch.complex64)
+        st.bootstrap(V, sns.curl(V))
+        st.step(2)
+        assert N.lib().sns_ns_check(st.h) == N.SNS_OK
+        out[env] = [x.clone() for x in st.state()["V1"]]
+        st.close()
+    for a, b in zip(out["SNS_K1_TMA"], out["SNS_K1_RELOAD"]):
+        assert torch.equal(a, b)
