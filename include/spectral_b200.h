@@ -221,9 +221,11 @@ int sns_ns_check(sns_ns* handle);
 int sns_ns_launches_per_step(sns_ns* handle);
 /* Tune the stepper's plan by measurement (no reference counterpart; the
  * reference's planning is FFTW_MEASURE per line plan, src/FFT1D.cpp:18-22):
- * times candidate tile shapes of each pass -- K1 z-inverse + curl tile, the
+ * times candidate tile shapes of each pass -- K1 z-inverse + curl tile (direct
+ * loads, or TMA-staged with one or two stages), the
  * y passes' run width, thread count and radix order, the x pass's rows per
- * CTA, the update pass's width, then the L2 prefetch distance of all passes
+ * CTA (direct or TMA-staged), the update pass's width, then the L2 prefetch
+ * distance of all passes
  * (SNS_PF=0..4 in the environment fixes it) -- on the stepper's own fields (seeded data
  * for the timing, zero again after) and keeps the fastest per pass.  Call it after create and before the first
  * bootstrap, set_state or step (SNS_ERR_ARG otherwise); the choice is cached
@@ -234,7 +236,7 @@ int sns_ns_tune(sns_ns* handle);
 /* The stepper's plan as text (no reference counterpart; the reference's
  * planning is FFTW_MEASURE per line plan, src/FFT1D.cpp:18-22): the pass
  * structure and tile shapes chosen for this box, e.g.
- * "passes=5 xy=separate k1=8x1 y=W16/T256/16-first zW=16 xG=4 pf=0 tuned".  Writes at most len bytes
+ * "passes=5 xy=separate k1=8x1(tma1) y=W16/T256/16-first zW=16 xG=4(tma) pf=0 tuned".  Writes at most len bytes
  * (NUL-terminated) to buf; returns the full length. */
 int sns_ns_describe(sns_ns* handle, char* buf, int len);
 /* Per-pass timing (no reference counterpart; the reference times phases with

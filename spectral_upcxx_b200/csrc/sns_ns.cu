@@ -43,6 +43,78 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
                     reinterpret_cast<cx_t<T>*>(smem_raw), pf, (int64_t)gridDim.x);
 }
 
+// K3 with TMA-staged tiles: a persistent CTA walks the tiles blockIdx.x,
+// + gridDim.x, ...; the G rows of each of the six fields of its next tile (G L
+// contiguous elements per field) come into a shared-memory stage as six bulk
+// copies on an mbarrier, issued as soon as the current tile's threads have
+// read the stage into registers, so the loads overlap the transforms and the
+// cross product.  Bounded waits and the stall test as in k_zcurl_tma.
+template <typename T, int L>
+__global__ void __launch_bounds__(MaxThreads<T>::value)
+    k_xcross_tma(FieldPtrs f, const cx_t<T>* __restrict__ tw, int G, T scale2, int64_t ntiles,
+                 int* err, long long stall_cycles) {
+  using C = cx_t<T>;
+  constexpr int E = LinePlan<L>::E, TPL = LinePlan<L>::TPL;
+  constexpr int RS = xrow_stride(L, (int)sizeof(C));
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int per = G * L;  // elements of one field's rows of a tile
+  const uint32_t raw = tc::smem_u32(smem_raw);
+  C* stage = reinterpret_cast<C*>(smem_raw + (((raw + 127u) & ~127u) - raw));
+  C* rows = stage + 6 * per;
+  uint64_t* full = reinterpret_cast<uint64_t*>(rows + 6 * G * RS);  // stage, stall test
+  const int64_t stride = gridDim.x;
+  pdl_trigger();
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&full[0], 1);
+    tc::mbar_init(&full[1], 1);
+  }
+  __syncthreads();
+  pdl_wait();  // the rows are written by the y pass before
+  auto issue = [&](int64_t blk) {  // thread 0
+    const int64_t e0 = blk * per;
+    if ((tc::smem_u32(stage) & 127u) || ((e0 * (int64_t)sizeof(C)) & 15)) {
+      atomicExch(err, 2);
+      tma::arrive(&full[0]);
+      return;
+    }
+    tma::expect_tx(&full[0], (uint32_t)(6 * per * sizeof(C)));
+#pragma unroll 1
+    for (int fl = 0; fl < 6; fl++)
+      tma::load_bulk(stage + fl * per, reinterpret_cast<const C*>(select_ptr(f.in, fl)) + e0,
+                     (uint32_t)(per * sizeof(C)), &full[0]);
+  };
+  if (threadIdx.x == 0 && (int64_t)blockIdx.x < ntiles) issue(blockIdx.x);
+  int it = 0;
+#pragma unroll 1
+  for (int64_t blk = blockIdx.x; blk < ntiles; blk += stride, it++) {
+    const bool more = blk + stride < ntiles;
+    bool ok = tc::mbar_wait(&full[0], (uint32_t)(it & 1), tc::kWaitCycles);
+    if (stall_cycles > 0 && it == 0) ok = ok && tc::mbar_wait(&full[1], 0, stall_cycles);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+        tc::mbar_wait(&full[0], (uint32_t)(it & 1), tc::kWaitCycles);
+      }
+      __syncthreads();
+      return;
+    }
+    xcross_tile_from<T, L>(ParamFields{f}, tw, G, scale2, blk, (int)blockDim.x, rows,
+                           [&](int fld, int gl, int j, C (&v)[E]) {
+                             const C* src = stage + fld * per + gl * L + j;
+#pragma unroll
+                             for (int e = 0; e < E; e++) v[e] = src[TPL * e];
+                             // every thread has read the stage: refill it
+                             __syncthreads();
+                             if (threadIdx.x == 0 && more) {
+                               tma::fence_proxy_async();
+                               issue(blk + stride);
+                             }
+                           });
+    // the rows are free for the next tile
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // K3 of a real-field run: rows of the half spectrum, M = nx/2 values
 // (kx = 0 .. M-1; kx = M is a Nyquist mode, zero).  Inverse: the real line u of
@@ -345,6 +417,70 @@ int launch_xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream
   return OK;
 }
 
+// Stall test of the TMA-staged passes (SNS_TMA_STALL_TEST=<cycles>; 0: none).
+inline long long tma_stall_cycles() {
+  const char* e = getenv("SNS_TMA_STALL_TEST");
+  const long long v = e ? atoll(e) : 0;
+  return v > 0 ? v : 0;
+}
+
+// Shared memory of the TMA-staged K3: the stage (6 G rows), 128 bytes of
+// alignment slack, the 6 G padded rows of the exchanges and two mbarriers.
+inline size_t xcross_tma_smem(int L, int G, size_t esz) {
+  return ((size_t)6 * G * L + (size_t)6 * G * xrow_stride(L, (int)esz)) * esz + 128 + 16;
+}
+
+// Whether the TMA-staged K3 can run G rows per tile on the (complex) box.
+bool x_tma_ok(const NSPlan& p, int G) {
+  const int TPL = p.nx >= 16 ? p.nx / 16 : 1;
+  const size_t esz = p.prec == PREC_C128 ? 16 : 8;
+  return !p.real && ((int64_t)p.ny * p.nz) % G == 0 && 6 * G * TPL <= max_threads(p.prec) &&
+         xcross_tma_smem(p.nx, G, esz) <= 220 * 1024 && ((size_t)G * p.nx * esz) % 16 == 0;
+}
+
+template <typename T, int L>
+int launch_xcross_tma(const NSPlan& pl, const FieldPtrs& f, int64_t rows, int* err,
+                      cudaStream_t s) {
+  using C = cx_t<T>;
+  constexpr int TPL = LinePlan<L>::TPL;
+  const int G = pl.xG;
+  const int threads = 6 * G * TPL;
+  const size_t smem = xcross_tma_smem(L, G, sizeof(C));
+  for (int i = 0; i < 6; i++)
+    if (reinterpret_cast<uintptr_t>(f.in[i]) & 15) {
+      set_error("K3 TMA tile: a field is not 16-byte aligned");
+      return ERR_UNSUPPORTED;
+    }
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr[dev & 63]) {
+    cudaError_t e = allow_max_dynamic_smem(k_xcross_tma<T, L>);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_xcross_tma)");
+    attr[dev & 63] = true;
+  }
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_xcross_tma<T, L>,
+                                                                threads, smem);
+  if (e != cudaSuccess) return cuda_status(e, "occupancy(k_xcross_tma)");
+  if (per_sm < 1) {
+    set_error("K3 TMA tile: does not fit on an SM");
+    return ERR_UNSUPPORTED;
+  }
+  const int64_t ntiles = rows / G;
+  const int blocks = (int)std::min<int64_t>(ntiles, (int64_t)per_sm * sm_count());
+  const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
+  if (!tw) {
+    set_error("twiddle table allocation failed");
+    return ERR_ALLOC;
+  }
+  const double N = (double)pl.nx * pl.ny * pl.nz;
+  e = launch_pdl(k_xcross_tma<T, L>, dim3((unsigned)blocks), dim3(threads), smem, s, f, tw, G,
+                 (T)(1.0 / (N * N)), ntiles, err, tma_stall_cycles());
+  if (e != cudaSuccess) return cuda_status(e, "k_xcross_tma");
+  return OK;
+}
+
 template <typename T, int L, bool RELOAD>
 int launch_zcurl_as(const NSPlan& pl, const FieldPtrs& f, cudaStream_t s) {
   using C = cx_t<T>;
@@ -408,12 +544,6 @@ bool k1_tma_ok(const NSPlan& p, int W, int G, int S) {
          field_box_ok(p.nx, p.ny, p.nz, esz, W, G, zb);
 }
 
-// Stall test of the TMA-staged K1 (SNS_K1_STALL_TEST=<cycles>; 0: none).
-inline long long zcurl_stall_cycles() {
-  const char* e = getenv("SNS_K1_STALL_TEST");
-  const long long v = e ? atoll(e) : 0;
-  return v > 0 ? v : 0;
-}
 
 template <typename T, int L, int S>
 int launch_zcurl_tma(const NSPlan& pl, const FieldPtrs& f, int* err, cudaStream_t s) {
@@ -469,7 +599,7 @@ int launch_zcurl_tma(const NSPlan& pl, const FieldPtrs& f, int* err, cudaStream_
   int wshift = 0;
   while ((1 << wshift) < g.W) wshift++;
   e = launch_pdl(k_zcurl_tma<T, L, S>, dim3((unsigned)blocks), dim3(threads), smem, s, m[0], m[1],
-                 m[2], g, f, tw, wshift, err, zcurl_stall_cycles());
+                 m[2], g, f, tw, wshift, err, tma_stall_cycles());
   if (e != cudaSuccess) return cuda_status(e, "k_zcurl_tma");
   return OK;
 }
@@ -567,17 +697,22 @@ int launch_update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
 }
 
 template <typename T>
-int xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream_t s) {
+int xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, int* err, cudaStream_t s) {
+  const bool tma = pl.x_tma && err;
   switch (pl.nx) {
-    case 4: return launch_xcross<T, 4>(pl, f, rows, s);
-    case 8: return launch_xcross<T, 8>(pl, f, rows, s);
-    case 16: return launch_xcross<T, 16>(pl, f, rows, s);
-    case 32: return launch_xcross<T, 32>(pl, f, rows, s);
-    case 64: return launch_xcross<T, 64>(pl, f, rows, s);
-    case 128: return launch_xcross<T, 128>(pl, f, rows, s);
-    case 256: return launch_xcross<T, 256>(pl, f, rows, s);
-    case 512: return launch_xcross<T, 512>(pl, f, rows, s);
-    case 1024: return launch_xcross<T, 1024>(pl, f, rows, s);
+#define SNS_XCROSS_CASE(L)                                                                   \
+  case L:                                                                                    \
+    return tma ? launch_xcross_tma<T, L>(pl, f, rows, err, s) : launch_xcross<T, L>(pl, f, rows, s);
+    SNS_XCROSS_CASE(4)
+    SNS_XCROSS_CASE(8)
+    SNS_XCROSS_CASE(16)
+    SNS_XCROSS_CASE(32)
+    SNS_XCROSS_CASE(64)
+    SNS_XCROSS_CASE(128)
+    SNS_XCROSS_CASE(256)
+    SNS_XCROSS_CASE(512)
+    SNS_XCROSS_CASE(1024)
+#undef SNS_XCROSS_CASE
     default: set_error("fused NS step: nx must be a power of two in [4, 1024]"); return ERR_UNSUPPORTED;
   }
 }
@@ -599,11 +734,12 @@ int update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
 }
 
 // K3 of the plan: complex rows, or half-spectrum rows of a real-field run
-int xpass(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream_t s) {
+int xpass(const NSPlan& pl, const FieldPtrs& f, int64_t rows, int* err, cudaStream_t s) {
   if (pl.real)
     return pl.prec == PREC_C128 ? xcross_r2c<double>(pl, f, rows, s)
                                 : xcross_r2c<float>(pl, f, rows, s);
-  return pl.prec == PREC_C128 ? xcross<double>(pl, f, rows, s) : xcross<float>(pl, f, rows, s);
+  return pl.prec == PREC_C128 ? xcross<double>(pl, f, rows, err, s)
+                              : xcross<float>(pl, f, rows, err, s);
 }
 
 int elems(int L) { return L >= 16 ? 16 : L; }
@@ -644,6 +780,20 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
       return ERR_UNSUPPORTED;
     }
     pl.xG = G;
+    // the TMA-staged form on request (SNS_X_TMA=1), with the widest tile up
+    // to G that fits its stage.  Measured on B200 at 256^3 it does not pay:
+    // complex64 0.315 ms against 0.284 (G = 4) and 0.262 (G = 2, direct);
+    // complex128 0.700 against 0.756 (G = 4) and 0.599 (G = 1, direct): the
+    // rows are contiguous, so direct loads already stream, and the stage
+    // halves the CTAs an SM holds.  The tuner still tries it.
+    const char* e = getenv("SNS_X_TMA");
+    pl.x_tma = false;
+    if (e && e[0] == '1')
+      for (int g = G; g >= 1 && !pl.x_tma; g /= 2)
+        if (x_tma_ok(pl, g)) {
+          pl.x_tma = true;
+          pl.xG = g;
+        }
   }
   // K1 tile: W adjacent z lines x G groups of the three components, one
   // CTA for all six outputs (SNS_K1_SPLIT=1: one output field per CTA)
@@ -765,6 +915,8 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
                  double* stats, int* sync_words, double nu, double dt, cudaStream_t s,
                  cudaEvent_t* ev, void* const* W) {
   const int nx = pl.nx, ny = pl.ny, nz = pl.nz, prec = pl.prec;
+  // the error word of the step's bounded waits
+  int* err_word = sync_words ? sync_words + xy_sync_words(nz) - 1 : nullptr;
   int rc;
   int pass = 0;
   auto mark = [&]() {
@@ -795,9 +947,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     for (int d = 0; d < 3; d++) f.in[d] = V[d];
     for (int i = 0; i < 6; i++) f.out[i] = U[i];
     if (pl.k1_fused) {
-      // the error word of the step's bounded waits
-      int* err = sync_words ? sync_words + xy_sync_words(nz) - 1 : nullptr;
-      rc = prec == PREC_C128 ? zcurl<double>(pl, f, err, s) : zcurl<float>(pl, f, err, s);
+      rc = prec == PREC_C128 ? zcurl<double>(pl, f, err_word, s) : zcurl<float>(pl, f, err_word, s);
     } else {
       LineGeo g = axis_geo(2, nx, ny, nz, prec, pl.lineW);
       g.kx_half = pl.real;
@@ -850,7 +1000,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
       for (int i = 0; i < 6; i++) f.in[i] = Uc[i];
       for (int i = 0; i < 3; i++) f.out[i] = Uc[i];
       const int64_t rows = (int64_t)ny * pz;
-      int r = xpass(pl, f, rows, s);
+      int r = xpass(pl, f, rows, err_word, s);
       if (r) return r;
       if (marks) mark();
     }
@@ -1083,12 +1233,20 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
   // K3: rows per CTA of the x cross pass
   if (rc == OK) {
     c.clear();
-    for (int G : {1, 2, 4, 8, 16})
+    for (int G : {1, 2, 4, 8, 16}) {
       if (xg_ok(pl, G)) {
         NSPlan q = pl;
         q.xG = G;
+        q.x_tma = false;
         c.push_back(q);
       }
+      if (sync_words && x_tma_ok(pl, G)) {
+        NSPlan q = pl;
+        q.xG = G;
+        q.x_tma = true;
+        c.push_back(q);
+      }
+    }
     if (!c.empty()) rc = pick(c, 0x4u);
   }
   // K5: adjacent z lines per CTA of the update pass

@@ -10,6 +10,7 @@ namespace sns {
 struct NSPlan {
   int nx, ny, nz, prec;
   int xG;             // rows per CTA of the x cross pass
+  bool x_tma;         // the x cross pass as a persistent pass over TMA-staged rows
   int k1W, k1G;       // K1 tile: adjacent z lines x groups (all six outputs per CTA)
   bool k1_fused;      // K1 loads V once per tile (else one output field per CTA)
   bool k1_reload;     // the fused K1 forms omega from reloads of V (L1), not shared memory

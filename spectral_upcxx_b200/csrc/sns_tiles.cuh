@@ -418,35 +418,27 @@ __device__ __forceinline__ void curl_zpass_tile_staged(const LineGeo& geo, const
 // K3 of the NS step: x lines -- inverse 6 fields, 1/N^2-scaled complex cross
 // product u x omega, forward 3 fields (src/Vector.cpp:79-89).  A tile is G
 // rows of all six fields; f.in(0..5) = (u, omega), f.out(0..2) = the product.
-template <typename T, int L, typename Fields>
-__device__ __forceinline__ void xcross_tile(const Fields& f, const cx_t<T>* __restrict__ tw, int G,
-                                            T scale2, int64_t blk, int nthr, cx_t<T>* sm,
-                                            int64_t pf = 0, int64_t nblk = 0) {
+//
+// The tile's input comes through load(fld, gl, j, v): the E elements j + e*TPL
+// of row gl of field fld (xcross_tile reads them from HBM; the TMA-staged pass
+// from the shared-memory stage).
+template <typename T, int L, typename Fields, typename Load>
+__device__ __forceinline__ void xcross_tile_from(const Fields& f, const cx_t<T>* __restrict__ tw,
+                                                 int G, T scale2, int64_t blk, int nthr,
+                                                 cx_t<T>* sm, Load load) {
   using C = cx_t<T>;
   using P = LinePlan<L>;
   constexpr int E = P::E, TPL = P::TPL, RS = xrow_stride(L, (int)sizeof(C));
   const int64_t row0 = blk * G;
   const int per = G * L;
-  if (pf > 0 && blk + pf < nblk) {
-    // the six input rows of tile blk + pf into L2
-#pragma unroll
-    for (int fl = 0; fl < 6; fl++)
-      prefetch_lines<L>(reinterpret_cast<const char*>(f.in(fl)), (blk + pf) * G * L, 1, G, L, 1,
-                        (int)sizeof(C), nthr);
-  }
 
   // thread t owns line t / TPL (field-major: field = line / G, row = line % G)
-  // at positions j + e*TPL; loads go straight to registers, E per thread
+  // at positions j + e*TPL, E elements in registers
   const int j = threadIdx.x % TPL, line = threadIdx.x / TPL;
   const int fld = line / G, gl = line - fld * G;
   C* row = sm + line * RS;
   C v[E];
-  {
-    const C* __restrict__ src = reinterpret_cast<const C*>(f.in(fld));
-    const int64_t i0 = (row0 + gl) * L + j;
-#pragma unroll
-    for (int e = 0; e < E; e++) v[e] = src[i0 + TPL * e];
-  }
+  load(fld, gl, j, v);
   line_fft<L>(v, row, j, tw, (T)1);
 #pragma unroll
   for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
@@ -489,6 +481,29 @@ __device__ __forceinline__ void xcross_tile(const Fields& f, const cx_t<T>* __re
 #pragma unroll
     for (int e = 0; e < E; e++) dst[i0 + TPL * e] = v[e];
   }
+}
+
+// K3 tile with its loads from HBM straight into registers (E per thread in
+// flight), optionally asking L2 for the rows of tile blk + pf first.
+template <typename T, int L, typename Fields>
+__device__ __forceinline__ void xcross_tile(const Fields& f, const cx_t<T>* __restrict__ tw, int G,
+                                            T scale2, int64_t blk, int nthr, cx_t<T>* sm,
+                                            int64_t pf = 0, int64_t nblk = 0) {
+  using C = cx_t<T>;
+  constexpr int E = LinePlan<L>::E, TPL = LinePlan<L>::TPL;
+  if (pf > 0 && blk + pf < nblk) {
+    // the six input rows of tile blk + pf into L2
+#pragma unroll
+    for (int fl = 0; fl < 6; fl++)
+      prefetch_lines<L>(reinterpret_cast<const char*>(f.in(fl)), (blk + pf) * G * L, 1, G, L, 1,
+                        (int)sizeof(C), nthr);
+  }
+  xcross_tile_from<T, L>(f, tw, G, scale2, blk, nthr, sm, [&](int fld, int gl, int j, C (&v)[E]) {
+    const C* __restrict__ src = reinterpret_cast<const C*>(f.in(fld));
+    const int64_t i0 = (blk * G + gl) * L + j;
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = src[i0 + TPL * e];
+  });
 }
 
 // ---------------------------------------------------------------------------

@@ -56,6 +56,17 @@ __device__ __forceinline__ void load_3d(void* dst, const CUtensorMap* map, int c
       : "memory");
 }
 
+// Contiguous bytes [src, src + bytes) of global memory into shared memory at
+// dst (both 16-byte aligned, bytes a multiple of 16); completes on mbar.
+__device__ __forceinline__ void load_bulk(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          tc::smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(tc::smem_u32(mbar))
+      : "memory");
+}
+
 // Order this thread's earlier generic-proxy accesses of shared memory before
 // its later async-proxy ones (a TMA load into a buffer the CTA has read).
 __device__ __forceinline__ void fence_proxy_async() {

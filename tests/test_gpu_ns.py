@@ -303,3 +303,27 @@ def test_k1_tma_stages_match_reload_bit_for_bit(sns, cuda, dtype, shape, monkeyp
     for mode in ("1", "2"):
         for a, b in zip(out[mode], out["reload"]):
             assert torch.equal(a, b), mode
+
+
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (32, 64, 128), (16, 32, 512)])
+def test_x_tma_matches_direct_bit_for_bit(sns, cuda, dtype, shape, monkeypatch):
+    """The x cross pass over TMA-staged rows (SNS_X_TMA=1; by default the rows
+    load straight from HBM) does the same arithmetic on the same values:
+    three steps are identical bit for bit, for row lengths 64, 128 and 512."""
+    N = sns._native
+    V = _random_fourier(shape, dtype, cuda, 7)
+    out = {}
+    monkeypatch.setenv("SNS_GRAPH", "0")
+    for mode in ("0", "1"):
+        monkeypatch.setenv("SNS_X_TMA", mode)
+        st = sns.NSStepper(shape, 1 / 400, 5e-4, dtype)
+        assert ("(tma) pf" in st.describe()) == (mode == "1"), st.describe()
+        st.bootstrap(V, sns.curl(V))
+        st.step(3)
+        rc = N.lib().sns_ns_check(st.h)
+        assert rc == N.SNS_OK, (mode, rc, N.last_error())
+        out[mode] = [x.clone() for x in st.state()["V1"]] + [x.clone() for x in st.state()["cross0"]]
+        st.close()
+    for a, b in zip(out["1"], out["0"]):
+        assert torch.equal(a, b)

@@ -7,7 +7,7 @@
   and clears the record, and a stepper run afterwards with the normal budget
   succeeds and matches the separate passes.
 * The TMA-staged z pass of the step (SNS_K1_TMA) with a stall test
-  (SNS_K1_STALL_TEST=<cycles>): the first tile waits on a barrier nothing
+  (SNS_TMA_STALL_TEST=<cycles>): the first tile waits on a barrier nothing
   arrives at; sns_ns_check reports SNS_ERR_TIMEOUT, and the next run is normal.
 * The tcgen05 MLP inference with a stall test (SNS_TC_STALL_TEST=<cycles>):
   each CTA also waits on a barrier nothing arrives at; the wait runs out,
@@ -80,7 +80,7 @@ def test_tensor_core_wait_runs_out_and_recovers(sns, cuda, monkeypatch):
 
 
 def test_tma_stage_wait_runs_out_and_recovers(sns, cuda, monkeypatch):
-    """The TMA-staged K1 with a stall test (SNS_K1_STALL_TEST=<cycles>): the
+    """The TMA-staged K1 with a stall test (SNS_TMA_STALL_TEST=<cycles>): the
     first tile's wait also waits on a barrier that nothing arrives at, runs
     out, and the CTA records the timeout, waits for its copies in flight and
     ends; sns_ns_check reports SNS_ERR_TIMEOUT and clears the record, and a
@@ -91,7 +91,7 @@ def test_tma_stage_wait_runs_out_and_recovers(sns, cuda, monkeypatch):
     V = [x.to(torch.complex64) for x in ic.solenoidal_spectrum_hat(n, 4, cuda)]
     monkeypatch.setenv("SNS_GRAPH", "0")
     monkeypatch.setenv("SNS_K1_TMA", "2")
-    monkeypatch.setenv("SNS_K1_STALL_TEST", "20000")
+    monkeypatch.setenv("SNS_TMA_STALL_TEST", "20000")
     st = sns.NSStepper((n, n, n), 1 / 400, 5e-4, torch.complex64)
     assert "(tma2)" in st.describe()
     st.bootstrap(V, sns.curl(V))
@@ -100,7 +100,7 @@ def test_tma_stage_wait_runs_out_and_recovers(sns, cuda, monkeypatch):
     assert "gave up" in N.last_error()
     assert N.lib().sns_ns_check(st.h) == N.SNS_OK  # the record was cleared
     st.close()
-    monkeypatch.delenv("SNS_K1_STALL_TEST")
+    monkeypatch.delenv("SNS_TMA_STALL_TEST")
     out = {}
     for env in ("SNS_K1_TMA", "SNS_K1_RELOAD"):
         monkeypatch.delenv("SNS_K1_TMA", raising=False)
