@@ -1060,14 +1060,14 @@ int sns_ns_describe(sns_ns* h, char* buf, int len) {
   char tmp[256];
   const char* ord[3] = {"16-first", "remainder-first", "radix-8"};
   const int n = snprintf(tmp, sizeof(tmp),
-                         "passes=%d xy=%s k1=%dx%d%s y=W%d/T%d/%s zW=%d xG=%d%s pf=%d%s%s",
+                         "passes=%d xy=%s k1=%dx%d%s y=W%d/T%d/%s zW=%d%s xG=%d%s pf=%d%s%s",
                          h->cl.model != CLOSURE_NONE ? kLESLaunches : p.passes, xy,
                          p.k1_lines ? p.k1lW : p.k1W, p.k1_lines ? p.k1lT : p.k1G,
                          p.k1_lines ? "(lines)" : !p.k1_fused ? "(split)"
                          : p.k1_tma ? (p.k1_stages == 1 ? "(tma1)" : "(tma2)")
                          : p.k1_reload ? "(reload)" : "",
                          p.lineW, p.lineT,
-                         ord[p.lineOrd % 3], p.zW, p.xG, p.x_tma ? "(tma)" : "", p.pf_waves, p.real ? " real" : "",
+                         ord[p.lineOrd % 3], p.zW, p.z_tma ? "(tma)" : "", p.xG, p.x_tma ? "(tma)" : "", p.pf_waves, p.real ? " real" : "",
                          p.tuned ? " tuned" : "");
   if (buf && len > 0) {
     strncpy(buf, tmp, (size_t)len - 1);

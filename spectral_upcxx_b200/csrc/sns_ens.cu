@@ -605,6 +605,7 @@ int sns_ens_create(sns_ens** handle, int nboxes, const int64_t* dims, const doub
     ch.seq.k1_lines = false;
     ch.seq.k1_tma = false;
     ch.seq.x_tma = false;
+    ch.seq.z_tma = false;
     ch.seq.xy_chunk = 0;
     ch.seq.passes = kNSPasses;
     for (int user : it->second) {

@@ -360,6 +360,92 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
                               reinterpret_cast<cx_t<T>*>(smem_raw), red);
 }
 
+// K5 with TMA-staged tiles (plain step, no closure).  A persistent CTA walks
+// the tiles blockIdx.x, + gridDim.x, ...; the three components of the cross
+// product for a tile (W x L boxes) come into a shared-memory stage by TMA, and
+// the next tile's boxes are issued as soon as the current tile's threads have
+// read the stage into registers, so they load under the current tile's
+// transforms and update.  V and C0 are read in the update as before.  The
+// diagnostics of each tile go to its own slot of a.stats, as in k_zfwd_update.
+// Bounded waits and the stall test as in k_zcurl_tma.
+template <typename T, int L>
+__global__ void __launch_bounds__(MaxThreads<T>::value)
+    k_zfwd_update_tma(const __grid_constant__ CUtensorMap m0, const __grid_constant__ CUtensorMap m1,
+                      const __grid_constant__ CUtensorMap m2, const UpdateArgs a,
+                      const cx_t<T>* __restrict__ tw, int64_t ntiles, int* err,
+                      long long stall_cycles) {
+  using C = cx_t<T>;
+  constexpr int E = LinePlan<L>::E, TPL = LinePlan<L>::TPL;
+  constexpr int ZB = L < 256 ? L : 256;  // z planes per box
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[4][32];
+  const int W = a.W;
+  const int comp = W * L;  // elements of one component's tile
+  const uint32_t raw = tc::smem_u32(smem_raw);
+  C* stage = reinterpret_cast<C*>(smem_raw + (((raw + 127u) & ~127u) - raw));
+  C* rows = stage + 3 * comp;
+  uint64_t* full =
+      reinterpret_cast<uint64_t*>(rows + 3 * W * tile_stride(L, W, (int)sizeof(C)));
+  const int64_t stride = gridDim.x;
+  pdl_trigger();
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&full[0], 1);
+    tc::mbar_init(&full[1], 1);
+    tma::prefetch_map(&m0);
+    tma::prefetch_map(&m1);
+    tma::prefetch_map(&m2);
+  }
+  __syncthreads();
+  pdl_wait();  // the cross product comes from the y pass before
+  auto issue = [&](int64_t blk) {  // thread 0
+    const int u = (int)(sizeof(C) / 8);
+    const int64_t base = blk * W;
+    const int x0 = (int)(base & (a.nx - 1)) * u, y0 = (int)(base >> a.lx);
+    if ((x0 & 1) || x0 + W * u > a.nx * u || y0 >= a.ny || (tc::smem_u32(stage) & 127u)) {
+      atomicExch(err, 2);
+      tma::arrive(&full[0]);
+      return;
+    }
+    tma::expect_tx(&full[0], (uint32_t)(3 * comp * sizeof(C)));
+#pragma unroll 1
+    for (int z0 = 0; z0 < L; z0 += ZB) {
+      tma::load_3d(stage + z0 * W, &m0, x0, y0, z0, &full[0]);
+      tma::load_3d(stage + comp + z0 * W, &m1, x0, y0, z0, &full[0]);
+      tma::load_3d(stage + 2 * comp + z0 * W, &m2, x0, y0, z0, &full[0]);
+    }
+  };
+  if (threadIdx.x == 0 && (int64_t)blockIdx.x < ntiles) issue(blockIdx.x);
+  int it = 0;
+#pragma unroll 1
+  for (int64_t blk = blockIdx.x; blk < ntiles; blk += stride, it++) {
+    const bool more = blk + stride < ntiles;
+    bool ok = tc::mbar_wait(&full[0], (uint32_t)(it & 1), tc::kWaitCycles);
+    if (stall_cycles > 0 && it == 0) ok = ok && tc::mbar_wait(&full[1], 0, stall_cycles);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+        tc::mbar_wait(&full[0], (uint32_t)(it & 1), tc::kWaitCycles);
+      }
+      __syncthreads();
+      return;
+    }
+    zfwd_update_tile_from<T, L, false>(a, tw, blk, (int)blockDim.x, rows, red,
+                                       [&](int fld, int w, int j, C (&v)[E]) {
+                                         const C* src = stage + fld * comp + j * W + w;
+#pragma unroll
+                                         for (int e = 0; e < E; e++) v[e] = src[TPL * e * W];
+                                         // every thread has read the stage: refill it
+                                         __syncthreads();
+                                         if (threadIdx.x == 0 && more) {
+                                           tma::fence_proxy_async();
+                                           issue(blk + stride);
+                                         }
+                                       });
+    // the rows and the reduction slots are free for the next tile
+    __syncthreads();
+  }
+}
+
 __global__ void k_stats_final(const double* part, int blocks, double* out) {
   __shared__ double sm[4][256];
   double a = 0, b = 0, c = 0, m = 0;
@@ -696,6 +782,62 @@ int launch_update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
   return OK;
 }
 
+// Shared memory of the TMA-staged K5: the stage (3 W x L boxes), 128 bytes of
+// alignment slack, the 3 W padded rows and two mbarriers.
+inline size_t update_tma_smem(int L, int W, size_t esz) {
+  return ((size_t)3 * W * L + (size_t)3 * W * tile_stride(L, W, (int)esz)) * esz + 128 + 16;
+}
+
+// Whether the TMA-staged K5 can run W-line tiles on the box.
+bool z_tma_ok(const NSPlan& p, int W) {
+  if (p.nz < 16 || p.nz > 1024 || W > p.nx || p.nx % W) return false;
+  const int TPL = p.nz / 16;
+  const int esz = p.prec == PREC_C128 ? 16 : 8;
+  return 3 * W * TPL <= max_threads(p.prec) && update_tma_smem(p.nz, W, esz) <= 220 * 1024 &&
+         field_box_ok(p.nx, p.ny, p.nz, esz, W, 1, p.nz < 256 ? p.nz : 256);
+}
+
+template <typename T, int L>
+int launch_update_tma(const NSPlan& pl, const UpdateArgs& a, int* err, cudaStream_t s) {
+  using C = cx_t<T>;
+  constexpr int TPL = LinePlan<L>::TPL;
+  constexpr int ZB = L < 256 ? L : 256;
+  const int threads = 3 * a.W * TPL;
+  const size_t smem = update_tma_smem(L, a.W, sizeof(C));
+  CUtensorMap m[3];
+  for (int d = 0; d < 3; d++) {
+    const int rc = field_tensor_map(&m[d], a.U[d], pl.nx, pl.ny, pl.nz, (int)sizeof(C), a.W, 1, ZB);
+    if (rc) return rc;
+  }
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr[dev & 63]) {
+    cudaError_t e = allow_max_dynamic_smem(k_zfwd_update_tma<T, L>);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_zfwd_update_tma)");
+    attr[dev & 63] = true;
+  }
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_zfwd_update_tma<T, L>,
+                                                                threads, smem);
+  if (e != cudaSuccess) return cuda_status(e, "occupancy(k_zfwd_update_tma)");
+  if (per_sm < 1) {
+    set_error("K5 TMA tile: does not fit on an SM");
+    return ERR_UNSUPPORTED;
+  }
+  const int64_t ntiles = ((int64_t)pl.nx * pl.ny) / a.W;
+  const int blocks = (int)std::min<int64_t>(ntiles, (int64_t)per_sm * sm_count());
+  const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
+  if (!tw) {
+    set_error("twiddle table allocation failed");
+    return ERR_ALLOC;
+  }
+  e = launch_pdl(k_zfwd_update_tma<T, L>, dim3((unsigned)blocks), dim3(threads), smem, s, m[0],
+                 m[1], m[2], a, tw, ntiles, err, tma_stall_cycles());
+  if (e != cudaSuccess) return cuda_status(e, "k_zfwd_update_tma");
+  return OK;
+}
+
 template <typename T>
 int xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, int* err, cudaStream_t s) {
   const bool tma = pl.x_tma && err;
@@ -718,17 +860,25 @@ int xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, int* err, cudaStr
 }
 
 template <typename T, bool SGS>
-int update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
+int update(const NSPlan& pl, const UpdateArgs& a, int* err, cudaStream_t s) {
+  const bool tma = !SGS && pl.z_tma && err;
   switch (pl.nz) {
-    case 4: return launch_update<T, 4, SGS>(pl, a, s);
-    case 8: return launch_update<T, 8, SGS>(pl, a, s);
-    case 16: return launch_update<T, 16, SGS>(pl, a, s);
-    case 32: return launch_update<T, 32, SGS>(pl, a, s);
-    case 64: return launch_update<T, 64, SGS>(pl, a, s);
-    case 128: return launch_update<T, 128, SGS>(pl, a, s);
-    case 256: return launch_update<T, 256, SGS>(pl, a, s);
-    case 512: return launch_update<T, 512, SGS>(pl, a, s);
-    case 1024: return launch_update<T, 1024, SGS>(pl, a, s);
+#define SNS_UPDATE_CASE(L)                                                                   \
+  case L:                                                                                    \
+    if constexpr (L >= 16) {                                                                 \
+      if (tma) return launch_update_tma<T, L>(pl, a, err, s);                                \
+    }                                                                                        \
+    return launch_update<T, L, SGS>(pl, a, s);
+    SNS_UPDATE_CASE(4)
+    SNS_UPDATE_CASE(8)
+    SNS_UPDATE_CASE(16)
+    SNS_UPDATE_CASE(32)
+    SNS_UPDATE_CASE(64)
+    SNS_UPDATE_CASE(128)
+    SNS_UPDATE_CASE(256)
+    SNS_UPDATE_CASE(512)
+    SNS_UPDATE_CASE(1024)
+#undef SNS_UPDATE_CASE
     default: set_error("fused NS step: nz must be a power of two in [4, 1024]"); return ERR_UNSUPPORTED;
   }
 }
@@ -841,6 +991,22 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
       W *= 2;
     pl.zW = W;
     pl.update_blocks = (nx / W) * ny;
+    // the TMA-staged form on request (SNS_Z_TMA=1), the widest tile up to W
+    // that fits its stage.  Measured on B200 at 256^3 it does not pay: complex64
+    // 0.500 ms (W = 16) and 0.657 (W = 8) against 0.435 direct; complex128
+    // 1.159 (W = 8) against 1.016.  The cross product is only a third of the
+    // pass's reads (V and C0 load in the update), the stage and the rows fill
+    // the SM's shared memory at one CTA, and the persistent tiles add two
+    // barriers each.  The tuner still tries it.
+    const char* ez = getenv("SNS_Z_TMA");
+    pl.z_tma = false;
+    if (ez && ez[0] == '1')
+      for (int w = W; w >= 1 && !pl.z_tma; w /= 2)
+        if (z_tma_ok(pl, w)) {
+          pl.z_tma = true;
+          pl.zW = w;
+          pl.update_blocks = (nx / w) * ny;
+        }
     // closure update: nine fields in the tile
     const int cap = std::min(576, max_threads(prec));
     int Ws = 1;
@@ -1044,7 +1210,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     a.stats = stats;
     a.kc2 = pl.kc2;
     a.kx_half = pl.real;
-    rc = ns_update(pl, a, false, s);
+    rc = ns_update(pl, a, false, s, err_word);
     if (rc) return rc;
     mark();
   }
@@ -1252,13 +1418,22 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
   // K5: adjacent z lines per CTA of the update pass
   if (rc == OK) {
     c.clear();
-    for (int W : {2, 4, 8, 16, 32})
+    for (int W : {2, 4, 8, 16, 32}) {
       if (zw_ok(pl, W, max_blocks)) {
         NSPlan q = pl;
         q.zW = W;
+        q.z_tma = false;
         q.update_blocks = (pl.nx / W) * pl.ny;
         c.push_back(q);
       }
+      if (sync_words && zw_ok(pl, W, max_blocks) && z_tma_ok(pl, W)) {
+        NSPlan q = pl;
+        q.zW = W;
+        q.z_tma = true;
+        q.update_blocks = (pl.nx / W) * pl.ny;
+        c.push_back(q);
+      }
+    }
     if (!c.empty()) rc = pick(c, 0x10u);
   }
   // L2 prefetch distance of all five passes, timed over the whole step
@@ -1277,9 +1452,10 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
   return rc;
 }
 
-int ns_update(const NSPlan& pl, const UpdateArgs& a, bool sgs, cudaStream_t s) {
-  if (pl.prec == PREC_C128) return sgs ? update<double, true>(pl, a, s) : update<double, false>(pl, a, s);
-  return sgs ? update<float, true>(pl, a, s) : update<float, false>(pl, a, s);
+int ns_update(const NSPlan& pl, const UpdateArgs& a, bool sgs, cudaStream_t s, int* err) {
+  if (pl.prec == PREC_C128)
+    return sgs ? update<double, true>(pl, a, err, s) : update<double, false>(pl, a, err, s);
+  return sgs ? update<float, true>(pl, a, err, s) : update<float, false>(pl, a, err, s);
 }
 
 // The normalisation sns_ns_stats applies on the host (mean |div|, 1/2 <|u|^2>,

@@ -11,6 +11,7 @@ struct NSPlan {
   int nx, ny, nz, prec;
   int xG;             // rows per CTA of the x cross pass
   bool x_tma;         // the x cross pass as a persistent pass over TMA-staged rows
+  bool z_tma;         // the update pass as a persistent pass over TMA-staged z lines
   int k1W, k1G;       // K1 tile: adjacent z lines x groups (all six outputs per CTA)
   bool k1_fused;      // K1 loads V once per tile (else one output field per CTA)
   bool k1_reload;     // the fused K1 forms omega from reloads of V (L1), not shared memory
@@ -58,7 +59,10 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
 // The update pass (z-forward + AB2 / projection / CN update) on the fields of
 // `a`; sgs adds the divergence of the Fourier eddy stress a.tau.
 struct UpdateArgs;
-int ns_update(const NSPlan& pl, const UpdateArgs& a, bool sgs, cudaStream_t s);
+// err: the step's error word (the TMA-staged form records its bounded waits
+// there); null keeps the direct-load form.
+int ns_update(const NSPlan& pl, const UpdateArgs& a, bool sgs, cudaStream_t s,
+              int* err = nullptr);
 // Autotuner of the plain complex or real step (the counterpart of the
 // reference's FFTW_MEASURE planning, src/FFT1D.cpp:18-22): times the passes
 // of candidate plans on the stepper's own fields -- which must hold no state

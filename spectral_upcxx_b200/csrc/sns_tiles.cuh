@@ -547,10 +547,15 @@ __device__ __forceinline__ const void* update_field(const UpdateArgs& a, int f) 
 // Tile `blk` holds the W z lines whose xy-plane offsets are blk*W .. blk*W+W-1.
 // With SGS the six stress fields are z-transformed in the same tile (9 fields
 // in shared memory, 9 W TPL threads).
-template <typename T, int L, bool SGS = false>
-__device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
-                                                 const cx_t<T>* __restrict__ tw, int64_t blk,
-                                                 int nthr, cx_t<T>* sm, double (*red)[32]) {
+//
+// The z lines come through load(fld, w, j, v): the E elements j + e*TPL of
+// line w of field fld (zfwd_update_tile reads them from HBM; the TMA-staged
+// pass from its shared-memory stage).
+template <typename T, int L, bool SGS, typename Load>
+__device__ __forceinline__ void zfwd_update_tile_from(const UpdateArgs& a,
+                                                      const cx_t<T>* __restrict__ tw, int64_t blk,
+                                                      int nthr, cx_t<T>* sm, double (*red)[32],
+                                                      Load load) {
   using C = cx_t<T>;
   using P = LinePlan<L>;
   constexpr int E = P::E, TPL = P::TPL;
@@ -560,19 +565,6 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
   const int64_t nxy = (int64_t)a.nx * a.ny;
   const int64_t base = blk * W;
   const int per = W * L;
-  if (!SGS && a.pf > 0 && (blk + a.pf) * W < nxy) {
-    // tile blk + pf's cross product, V and C0 into L2
-    const int64_t bp = (blk + a.pf) * W;
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      prefetch_lines<L>(reinterpret_cast<const char*>(a.U[d]), bp, W, 1, 0, nxy, (int)sizeof(C),
-                        nthr);
-      prefetch_lines<L>(reinterpret_cast<const char*>(a.V[d]), bp, W, 1, 0, nxy, (int)sizeof(C),
-                        nthr);
-      prefetch_lines<L>(reinterpret_cast<const char*>(a.C0[d]), bp, W, 1, 0, nxy, (int)sizeof(C),
-                        nthr);
-    }
-  }
 
   // thread t owns z line (field, base + w) at positions j + e*TPL with
   // w = t mod W, j = (t / W) mod TPL, field = t / (W*TPL): consecutive threads
@@ -581,12 +573,8 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
     const int w = threadIdx.x % W, s = threadIdx.x / W;
     const int j = s % TPL, fld = s / TPL;
     C* row = sm + (fld * W + w) * RS;
-    const C* __restrict__ src = reinterpret_cast<const C*>(
-        SGS ? update_field(a, fld) : (fld == 0 ? a.U[0] : fld == 1 ? a.U[1] : a.U[2]));
-    const int64_t i0 = base + w + nxy * j;
     C v[E];
-#pragma unroll
-    for (int e = 0; e < E; e++) v[e] = src[i0 + nxy * (TPL * e)];
+    load(fld, w, j, v);
     line_fft<L, true>(v, row, j, tw, (T)-1);
 #pragma unroll
     for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
@@ -737,6 +725,39 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
     out[2] = t2;
     out[3] = t3;
   }
+}
+
+// K5 tile with its loads from HBM straight into registers, optionally asking
+// L2 for the inputs of tile blk + pf first.
+template <typename T, int L, bool SGS = false>
+__device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
+                                                 const cx_t<T>* __restrict__ tw, int64_t blk,
+                                                 int nthr, cx_t<T>* sm, double (*red)[32]) {
+  using C = cx_t<T>;
+  constexpr int E = LinePlan<L>::E, TPL = LinePlan<L>::TPL;
+  const int W = a.W;
+  const int64_t nxy = (int64_t)a.nx * a.ny;
+  const int64_t base = blk * W;
+  if (!SGS && a.pf > 0 && (blk + a.pf) * W < nxy) {
+    // tile blk + pf's cross product, V and C0 into L2
+    const int64_t bp = (blk + a.pf) * W;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      prefetch_lines<L>(reinterpret_cast<const char*>(a.U[d]), bp, W, 1, 0, nxy, (int)sizeof(C),
+                        nthr);
+      prefetch_lines<L>(reinterpret_cast<const char*>(a.V[d]), bp, W, 1, 0, nxy, (int)sizeof(C),
+                        nthr);
+      prefetch_lines<L>(reinterpret_cast<const char*>(a.C0[d]), bp, W, 1, 0, nxy, (int)sizeof(C),
+                        nthr);
+    }
+  }
+  zfwd_update_tile_from<T, L, SGS>(a, tw, blk, nthr, sm, red, [&](int fld, int w, int j, C (&v)[E]) {
+    const C* __restrict__ src = reinterpret_cast<const C*>(
+        SGS ? update_field(a, fld) : (fld == 0 ? a.U[0] : fld == 1 ? a.U[1] : a.U[2]));
+    const int64_t i0 = base + w + nxy * j;
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = src[i0 + nxy * (TPL * e)];
+  });
 }
 
 // Entry i of a pointer table in kernel parameters, selected with constant

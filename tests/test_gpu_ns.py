@@ -327,3 +327,30 @@ def test_x_tma_matches_direct_bit_for_bit(sns, cuda, dtype, shape, monkeypatch):
         st.close()
     for a, b in zip(out["1"], out["0"]):
         assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (32, 64, 128), (512, 16, 32)])
+def test_z_tma_update_matches_direct_bit_for_bit(sns, cuda, dtype, shape, monkeypatch):
+    """The update pass over TMA-staged z lines of the cross product
+    (SNS_Z_TMA=1; by default they load straight from HBM) does the same
+    arithmetic on the same values: three steps and their diagnostics are
+    identical bit for bit (nz = 512: two boxes of 256 planes per line)."""
+    N = sns._native
+    V = _random_fourier(shape, dtype, cuda, 11)
+    out, stats = {}, {}
+    monkeypatch.setenv("SNS_GRAPH", "0")
+    for mode in ("0", "1"):
+        monkeypatch.setenv("SNS_Z_TMA", mode)
+        st = sns.NSStepper(shape, 1 / 400, 5e-4, dtype)
+        assert ("(tma) xG" in st.describe()) == (mode == "1"), st.describe()
+        st.bootstrap(V, sns.curl(V))
+        st.step(3)
+        rc = N.lib().sns_ns_check(st.h)
+        assert rc == N.SNS_OK, (mode, rc, N.last_error())
+        out[mode] = [x.clone() for x in st.state()["V1"]] + [x.clone() for x in st.state()["cross0"]]
+        stats[mode] = st.stats()
+        st.close()
+    for a, b in zip(out["1"], out["0"]):
+        assert torch.equal(a, b)
+    assert stats["1"] == stats["0"]

@@ -113,3 +113,31 @@ def test_tma_stage_wait_runs_out_and_recovers(sns, cuda, monkeypatch):
         st.close()
     for a, b in zip(out["SNS_K1_TMA"], out["SNS_K1_RELOAD"]):
         assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("env", ["SNS_X_TMA", "SNS_Z_TMA"])
+def test_tma_x_and_update_waits_run_out_and_recover(sns, cuda, monkeypatch, env):
+    """The same stall test on the TMA-staged x pass and update pass (the z
+    pass on its direct-load form, so the timeout is theirs)."""
+    from spectral_upcxx_b200 import ic
+    N = sns._native
+    n = 64
+    V = [x.to(torch.complex64) for x in ic.solenoidal_spectrum_hat(n, 4, cuda)]
+    monkeypatch.setenv("SNS_GRAPH", "0")
+    monkeypatch.setenv("SNS_K1_TMA", "0")
+    monkeypatch.setenv(env, "1")
+    monkeypatch.setenv("SNS_TMA_STALL_TEST", "20000")
+    st = sns.NSStepper((n, n, n), 1 / 400, 5e-4, torch.complex64)
+    assert "(tma)" in st.describe() and "(tma1)" not in st.describe()
+    st.bootstrap(V, sns.curl(V))
+    st.step(1)
+    assert N.lib().sns_ns_check(st.h) == N.SNS_ERR_TIMEOUT
+    assert "gave up" in N.last_error()
+    assert N.lib().sns_ns_check(st.h) == N.SNS_OK
+    st.close()
+    monkeypatch.delenv("SNS_TMA_STALL_TEST")
+    st = sns.NSStepper((n, n, n), 1 / 400, 5e-4, torch.complex64)
+    st.bootstrap(V, sns.curl(V))
+    st.step(2)
+    assert N.lib().sns_ns_check(st.h) == N.SNS_OK
+    st.close()
