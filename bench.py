@@ -49,10 +49,17 @@ PASSES = {
 
 
 def pass_names(npasses, plan):
-    """Names of the timed passes; the xy phase is named by the plan's mode."""
+    """Names of the timed passes; the xy phase is named by the plan's mode.
+    A plan whose update pass carries the next step's K1 ("(+K1") runs K1 in
+    its first step only: the update pass then also writes the six z-inverted
+    fields (9 + 6 + 6) and K1's steady-state share is empty."""
     names, fields = PASSES[npasses]
     mode = "cluster" if "xy=cluster" in plan else "dataflow" if "xy=dataflow" in plan else "slabs"
-    return [nm % mode if "%s" in nm else nm for nm in names], fields
+    names = [nm % mode if "%s" in nm else nm for nm in names]
+    if "(+K1" in plan:
+        names = names[:-1] + ["K5+K1 z-forward+update+z-inverse+curl"]
+        fields = [0] + list(fields[1:-1]) + [fields[-1] + 6]
+    return names, fields
 STEP_FIELDS = 30  # 9 FFTs x 2 + 12 for the spectral update: 30 N^3 S per step
 
 # DRAM bytes (read + write) per launch of each pass at 256^3 complex64 with the
@@ -533,7 +540,8 @@ def run_b200(args, rank, world, local):
                                "half_spectrum": real},
                       "passes": [{"name": nm, "ms": a, "share": sh,
                                   "gbs": PASS_FIELDS[i] * field_bytes / (a / 1e3) / 1e9}
-                                 for i, (nm, a, sh) in enumerate(zip(PASS_NAMES, avg, share))]},
+                                 for i, (nm, a, sh) in enumerate(zip(PASS_NAMES, avg, share))
+                                 if PASS_FIELDS[i] > 0]},
             gpu_launches=args.steps * st.launches_per_step(),
             diagnostics=stats)
         # ---- e2e through the C-ABI from pinned host buffers

@@ -217,7 +217,9 @@ int sns_ns_stats_async(sns_ns* handle, double* out4);
  * (SNS_ERR_TIMEOUT: the results
  * of those steps are invalid).  sns_ns_stats performs this check too. */
 int sns_ns_check(sns_ns* handle);
-/* Number of kernel launches one sns_ns_step(h, 1) issues. */
+/* Number of kernel launches one sns_ns_step(h, 1) issues in steady state (a
+ * plan whose update pass carries the next step's z-inverse pass launches one
+ * more in the first step after a bootstrap or a new state). */
 int sns_ns_launches_per_step(sns_ns* handle);
 /* Tune the stepper's plan by measurement (no reference counterpart; the
  * reference's planning is FFTW_MEASURE per line plan, src/FFT1D.cpp:18-22):

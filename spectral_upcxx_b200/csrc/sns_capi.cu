@@ -282,6 +282,9 @@ struct sns_ns {
   double* stats_out;
   int* sync_words;  // dataflow xy pass: ticket, per-plane counters, error word
   bool stepped;
+  // U holds K1's output for the current V (left there by a carrying K5); any
+  // call that writes V or U other than a plain step clears it
+  bool carried = false;
   // eddy-viscosity closure (none by default) and its six extra work fields
   Closure cl;
   void* U2[6] = {};
@@ -315,10 +318,11 @@ int step_on(sns_ns* h, cudaStream_t s, cudaEvent_t* ev) {
       U[i] = h->U[i];
       U[6 + i] = h->U2[i];
     }
+    h->carried = false;  // the closure step uses U as work space
     return les_step_once(h->pl, h->V, h->C0, U, h->stats_part, h->nu, h->dt, h->cl, s);
   }
   return ns_step_once(h->pl, h->V, h->C0, h->U, h->stats_part, h->sync_words, h->nu, h->dt, s,
-                      ev, h->W);
+                      ev, h->W, &h->carried);
 }
 
 int capture_step(sns_ns* h) {
@@ -704,6 +708,7 @@ int sns::ns_create(sns_ns** handle, int64_t nx, int64_t ny, int64_t nz, double n
     return rc;
   }
   h->stepped = false;
+  h->carried = false;
   // SNS_GRAPH=0 launches every step's kernels directly
   if (const char* e = getenv("SNS_GRAPH")) h->use_graph = e[0] != '0';
   // SNS_TUNE=1: every new stepper tunes its plan (cached per device and shape)
@@ -732,6 +737,7 @@ int sns_ns_destroy(sns_ns* h) {
   for (int i = 0; i < 6; i++) pool_free(h->U2[i]);
   for (cudaEvent_t e : h->events) cudaEventDestroy(e);
   drop_graph(h);
+  h->carried = false;
   if (h->cap) cudaStreamDestroy(h->cap);
   delete h;
   return OK;
@@ -747,6 +753,7 @@ int sns_ns_set_state(sns_ns* h, const void* const V1[3], const void* const cross
                                h->s);
     if (rc) return rc;
     h->stepped = false;
+    h->carried = false;
     return OK;
   }
   const size_t bytes = esize(h->pl.prec) * (size_t)h->pl.nx * h->pl.ny * h->pl.nz;
@@ -761,6 +768,7 @@ int sns_ns_set_state(sns_ns* h, const void* const V1[3], const void* const cross
       return rc;
   }
   h->stepped = false;
+  h->carried = false;
   return OK;
 }
 
@@ -784,12 +792,14 @@ int sns_ns_bootstrap(sns_ns* h, const void* const V0[3], const void* const omega
     for (void* p : t) pool_free(p);
     if (rc) return rc;
     h->stepped = false;
+    h->carried = false;
     return OK;
   }
   const Dims d{h->pl.nx, h->pl.ny, h->pl.nz};
   rc = ns_bootstrap_fields(d, h->pl.prec, h->nu, h->dt, V0, omega0, h->V, h->C0, h->U, h->s);
   if (rc) return rc;
   h->stepped = false;
+  h->carried = false;
   return OK;
 }
 
@@ -802,6 +812,13 @@ int sns_ns_step(sns_ns* h, int nsteps) {
   if (!h->profiling) {
     for (int t = 0; t < nsteps; t++) {
       int rc = OK;
+      // a captured step of a carrying plan starts from K1's output in U:
+      // make it there first if the state was set since
+      if (h->pl.carry && !h->carried && h->cl.model == CLOSURE_NONE && h->use_graph &&
+          h->eager_done) {
+        if ((rc = ns_k1_once(h->pl, h->V, h->U, h->sync_words, h->s))) return rc;
+        h->carried = true;
+      }
       if (h->use_graph && h->eager_done && !h->exec) rc = capture_step(h);
       if (rc) return rc;
       if (h->exec) {
@@ -832,7 +849,7 @@ int sns_ns_step(sns_ns* h, int nsteps) {
       ev = &h->events[(size_t)h->recorded * (kNSPasses + 1)];
     }
     int rc = ns_step_once(h->pl, h->V, h->C0, h->U, h->stats_part, h->sync_words, h->nu, h->dt,
-                          h->s, ev, h->W);
+                          h->s, ev, h->W, &h->carried);
     if (rc) return rc;
     if (ev) h->recorded++;
     h->stepped = true;
@@ -988,7 +1005,8 @@ int sns_ns_stats_async(sns_ns* h, double* out4) {
 
 int sns_ns_launches_per_step(sns_ns* h) {
   if (!nonnull(h, "sns_ns_launches_per_step")) return ERR_ARG;
-  return h->cl.model != CLOSURE_NONE ? kLESLaunches : h->pl.passes;
+  // a carrying plan skips K1 in every step but the first after a new state
+  return h->cl.model != CLOSURE_NONE ? kLESLaunches : h->pl.passes - (h->pl.carry ? 1 : 0);
 }
 
 namespace {
@@ -1025,6 +1043,7 @@ int sns_ns_tune(sns_ns* h) {
       }
       h->pl = q;
       drop_graph(h);
+      h->carried = false;
       return OK;
     }
   }
@@ -1047,6 +1066,7 @@ int sns_ns_tune(sns_ns* h) {
   }
   h->pl = q;
   drop_graph(h);
+  h->carried = false;
   std::lock_guard<std::mutex> lock(g_tune_mu);
   g_tuned[key] = q;
   return OK;
@@ -1067,7 +1087,7 @@ int sns_ns_describe(sns_ns* h, char* buf, int len) {
                          : p.k1_tma ? (p.k1_stages == 1 ? "(tma1)" : "(tma2)")
                          : p.k1_reload ? "(reload)" : "",
                          p.lineW, p.lineT,
-                         ord[p.lineOrd % 3], p.zW, p.z_tma ? "(tma)" : "", p.xG, p.x_tma ? "(tma)" : "", p.pf_waves, p.real ? " real" : "",
+                         ord[p.lineOrd % 3], p.zW, p.z_tma ? "(tma)" : p.carry ? (p.carry_reload ? "(+K1r)" : "(+K1)") : p.z_pfself ? "(pfs)" : "", p.xG, p.x_tma ? "(tma)" : "", p.pf_waves, p.real ? " real" : "",
                          p.tuned ? " tuned" : "");
   if (buf && len > 0) {
     strncpy(buf, tmp, (size_t)len - 1);
@@ -1116,6 +1136,7 @@ int sns_ns_set_closure(sns_ns* h, int model, double cs_delta2, const void* mlp, 
   h->cl.mlp = mlp;
   h->pl.kc2 = kc > 0 ? kc * kc : 1e300;
   drop_graph(h);
+  h->carried = false;
   h->eager_done = false;
   return OK;
 }
@@ -1129,6 +1150,7 @@ int sns_ns_set_sgs_band(sns_ns* h, double k_lo, double k_hi) {
   h->pl.sgs_klo = k_lo;
   h->pl.sgs_kinv = k_hi > k_lo ? 1.0 / (k_hi - k_lo) : 1e30;
   drop_graph(h);
+  h->carried = false;
   h->eager_done = false;
   return OK;
 }

@@ -17,6 +17,7 @@
 // deep copies per step; here the history copies (ns.cpp:213-217) are
 // in-place updates and every intermediate lives in U.
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 
 #include <algorithm>
@@ -358,6 +359,19 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
   pdl_wait();
   zfwd_update_tile<T, L, SGS>(a, tw, (int64_t)blockIdx.x, (int)blockDim.x,
                               reinterpret_cast<cx_t<T>*>(smem_raw), red);
+}
+
+// K5 with the next step's K1 carried in it (zfwd_update_curl_tile): the
+// update, then the z-inverse of the new V and of i k x V into a.Uo.
+template <typename T, int L, bool RELOAD>
+__global__ void __launch_bounds__(MaxThreads<T>::value)
+    k_zfwd_update_curl(const UpdateArgs a, const cx_t<T>* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[4][32];
+  pdl_trigger();
+  pdl_wait();
+  zfwd_update_curl_tile<T, L, RELOAD>(a, tw, (int64_t)blockIdx.x, (int)blockDim.x,
+                                      reinterpret_cast<cx_t<T>*>(smem_raw), red);
 }
 
 // K5 with TMA-staged tiles (plain step, no closure).  A persistent CTA walks
@@ -776,9 +790,54 @@ int launch_update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
   const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
   UpdateArgs ap = a;
   ap.pf = SGS ? 0 : tiles_in_waves(k_zfwd_update<T, L, SGS>, threads, smem, pl.pf_waves);
+  ap.pf_self = SGS ? 0 : pl.z_pfself;
   cudaError_t e = launch_pdl(k_zfwd_update<T, L, SGS>, dim3(blocks), dim3(threads), smem, s, ap,
                              tw);
   if (e != cudaSuccess) return cuda_status(e, "k_zfwd_update");
+  return OK;
+}
+
+// Shared memory of K5 with K1 carried: 3 W update rows, and 3 W exchange
+// rows unless the new velocity is read back from V (reload).
+inline size_t update_carry_smem(int L, int W, size_t esz, bool reload) {
+  return (size_t)(reload ? 3 : 6) * W * tile_stride(L, W, (int)esz) * esz;
+}
+
+// Whether K5 with K1 carried can run W-line tiles on the box.
+bool carry_ok(const NSPlan& p, int W, bool reload) {
+  if (W > p.nx || p.nx % W) return false;
+  const int TPL = p.nz >= 16 ? p.nz / 16 : 1;
+  const size_t esz = p.prec == PREC_C128 ? 16 : 8;
+  return 3 * W * TPL <= max_threads(p.prec) &&
+         update_carry_smem(p.nz, W, esz, reload) <= 220 * 1024;
+}
+
+template <typename T, int L, bool RELOAD>
+int launch_update_carry(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
+  using C = cx_t<T>;
+  constexpr int TPL = LinePlan<L>::TPL;
+  const int threads = 3 * a.W * TPL;
+  const size_t smem = update_carry_smem(L, a.W, sizeof(C), RELOAD);
+  const int blocks = (int)(((int64_t)pl.nx * pl.ny) / a.W);
+  if (a.W > pl.nx || pl.nx % a.W || threads > MaxThreads<T>::value) {
+    set_error("K5 with K1 carried: the tile width does not fit the box");
+    return ERR_ARG;
+  }
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr[dev & 63]) {
+    cudaError_t e = allow_max_dynamic_smem(k_zfwd_update_curl<T, L, RELOAD>);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_zfwd_update_curl)");
+    attr[dev & 63] = true;
+  }
+  const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
+  UpdateArgs ap = a;
+  ap.pf = tiles_in_waves(k_zfwd_update_curl<T, L, RELOAD>, threads, smem, pl.pf_waves);
+  ap.pf_self = pl.z_pfself;
+  cudaError_t e =
+      launch_pdl(k_zfwd_update_curl<T, L, RELOAD>, dim3(blocks), dim3(threads), smem, s, ap, tw);
+  if (e != cudaSuccess) return cuda_status(e, "k_zfwd_update_curl");
   return OK;
 }
 
@@ -879,6 +938,27 @@ int update(const NSPlan& pl, const UpdateArgs& a, int* err, cudaStream_t s) {
     SNS_UPDATE_CASE(512)
     SNS_UPDATE_CASE(1024)
 #undef SNS_UPDATE_CASE
+    default: set_error("fused NS step: nz must be a power of two in [4, 1024]"); return ERR_UNSUPPORTED;
+  }
+}
+
+template <typename T>
+int update_carry(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
+  const bool r = pl.carry_reload;
+  switch (pl.nz) {
+#define SNS_CARRY_CASE(L)                                                                    \
+  case L:                                                                                    \
+    return r ? launch_update_carry<T, L, true>(pl, a, s) : launch_update_carry<T, L, false>(pl, a, s);
+    SNS_CARRY_CASE(4)
+    SNS_CARRY_CASE(8)
+    SNS_CARRY_CASE(16)
+    SNS_CARRY_CASE(32)
+    SNS_CARRY_CASE(64)
+    SNS_CARRY_CASE(128)
+    SNS_CARRY_CASE(256)
+    SNS_CARRY_CASE(512)
+    SNS_CARRY_CASE(1024)
+#undef SNS_CARRY_CASE
     default: set_error("fused NS step: nz must be a power of two in [4, 1024]"); return ERR_UNSUPPORTED;
   }
 }
@@ -1007,6 +1087,24 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
           pl.zW = w;
           pl.update_blocks = (nx / w) * ny;
         }
+    // K1 carried in the update pass on request (SNS_CARRY=1), at the widest
+    // tile up to W whose update and exchange rows fit two CTAs per SM
+    // (SNS_CARRY=2: the new velocity read back from V, K5's shared memory)
+    const char* ecr = getenv("SNS_CARRY");
+    pl.carry = false;
+    pl.carry_reload = ecr && ecr[0] == '2';
+    if (ecr && (ecr[0] == '1' || ecr[0] == '2'))
+      for (int w = W; w >= 1 && !pl.carry; w /= 2)
+        if (carry_ok(pl, w, pl.carry_reload) &&
+            update_carry_smem(nz, w, esz, pl.carry_reload) <= 110 * 1024) {
+          pl.carry = true;
+          pl.z_tma = false;
+          pl.zW = w;
+          pl.update_blocks = (nx / w) * ny;
+        }
+    // L2 prefetch of each tile's V and C0 before its z-forward (SNS_Z_PFSELF=1)
+    const char* epf = getenv("SNS_Z_PFSELF");
+    pl.z_pfself = epf && epf[0] == '1';
     // closure update: nine fields in the tile
     const int cap = std::min(576, max_threads(prec));
     int Ws = 1;
@@ -1077,9 +1175,36 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
   return OK;
 }
 
+namespace {
+
+// K1 as a z pass of V into U[0..5] (the fused tile or one field per CTA).
+int run_k1(const NSPlan& pl, void* const V[3], void* const U[6], int* err_word, cudaStream_t s) {
+  FieldPtrs f{};
+  f.n = 6;
+  for (int d = 0; d < 3; d++) f.in[d] = V[d];
+  for (int i = 0; i < 6; i++) f.out[i] = U[i];
+  if (pl.k1_fused)
+    return pl.prec == PREC_C128 ? zcurl<double>(pl, f, err_word, s)
+                                : zcurl<float>(pl, f, err_word, s);
+  LineGeo g = axis_geo(2, pl.nx, pl.ny, pl.nz, pl.prec, pl.lineW);
+  g.kx_half = pl.real;
+  return run_line_pass(g, f, +1, 0, 1.0, pl.prec, s, PRO_CURL6);
+}
+
+}  // namespace
+
+int ns_k1_once(const NSPlan& pl, void* const V[3], void* const U[6], int* sync_words,
+               cudaStream_t s) {
+  if (pl.k1_lines) {
+    set_error("ns_k1_once: K1 as a line pass writes the work fields W, not U");
+    return ERR_ARG;
+  }
+  return run_k1(pl, V, U, sync_words ? sync_words + xy_sync_words(pl.nz) - 1 : nullptr, s);
+}
+
 int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* const U[6],
                  double* stats, int* sync_words, double nu, double dt, cudaStream_t s,
-                 cudaEvent_t* ev, void* const* W) {
+                 cudaEvent_t* ev, void* const* W, bool* carried) {
   const int nx = pl.nx, ny = pl.ny, nz = pl.nz, prec = pl.prec;
   // the error word of the step's bounded waits
   int* err_word = sync_words ? sync_words + xy_sync_words(nz) - 1 : nullptr;
@@ -1091,8 +1216,14 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
   };
   mark();
   const bool lines = pl.k1_lines && W && !pl.use_xy && !pl.use_xyc;
+  // K1 carried in the previous step's K5: U already holds its output
+  const bool carry = pl.carry && carried && !lines;
+  const bool have_k1 = carry && *carried;
+  if (carried) *carried = false;
   // K1: z-inverse of (V, i k x V)
-  if (lines) {
+  if (have_k1) {
+    mark();
+  } else if (lines) {
     // V and the z derivatives i kz Vx, i kz Vy (taken on the way in), each
     // field z-inverse-transformed on its own; K2 forms omega from them
     FieldPtrs f{};
@@ -1108,18 +1239,7 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     if (rc) return rc;
     mark();
   } else {
-    FieldPtrs f{};
-    f.n = 6;
-    for (int d = 0; d < 3; d++) f.in[d] = V[d];
-    for (int i = 0; i < 6; i++) f.out[i] = U[i];
-    if (pl.k1_fused) {
-      rc = prec == PREC_C128 ? zcurl<double>(pl, f, err_word, s) : zcurl<float>(pl, f, err_word, s);
-    } else {
-      LineGeo g = axis_geo(2, nx, ny, nz, prec, pl.lineW);
-      g.kx_half = pl.real;
-      rc = run_line_pass(g, f, +1, 0, 1.0, prec, s, PRO_CURL6);
-    }
-    if (rc) return rc;
+    if ((rc = run_k1(pl, V, U, err_word, s))) return rc;
     mark();
   }
   if (pl.use_xy) {
@@ -1210,8 +1330,16 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
     a.stats = stats;
     a.kc2 = pl.kc2;
     a.kx_half = pl.real;
-    rc = ns_update(pl, a, false, s, err_word);
+    if (carry) {
+      // K5 with the next step's K1 carried: U receives the z-inverse of the
+      // new V and of its curl
+      for (int i = 0; i < 6; i++) a.Uo[i] = U[i];
+      rc = prec == PREC_C128 ? update_carry<double>(pl, a, s) : update_carry<float>(pl, a, s);
+    } else {
+      rc = ns_update(pl, a, false, s, err_word);
+    }
     if (rc) return rc;
+    if (carried) *carried = carry;
     mark();
   }
   return OK;
@@ -1291,8 +1419,10 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
   // to set the kernels up, then the least of five timed steps
   auto measure = [&](const NSPlan& c, unsigned passes, float* out) -> int {
     float best = 3.4e38f;
+    bool carried = false;
     for (int r = 0; r < 6; r++) {
-      int e = ns_step_once(c, V, C0, U, stats, sync_words, 0.0, 0.0, s, r ? ev : nullptr, W);
+      int e = ns_step_once(c, V, C0, U, stats, sync_words, 0.0, 0.0, s, r ? ev : nullptr, W,
+                           &carried);
       if (e) return e;
       if (!r) continue;
       if ((e = cuda_status(cudaEventSynchronize(ev[kNSPasses]), "ns_tune_plan"))) return e;
@@ -1308,6 +1438,8 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
     *out = best;
     return OK;
   };
+  // SNS_TUNE_LOG=1 prints every candidate's time to stderr
+  const bool log = getenv("SNS_TUNE_LOG") && getenv("SNS_TUNE_LOG")[0] == '1';
   auto pick = [&](std::vector<NSPlan>& cands, unsigned passes) -> int {
     float best = 3.4e38f;
     int bi = -1;
@@ -1315,6 +1447,15 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
       float t = 0;
       int e = measure(cands[i], passes, &t);
       if (e) return e;
+      if (log)
+        fprintf(stderr,
+                "ns_tune passes=0x%x cand=%zu ms=%.4f k1=%dx%d%s%s xG=%d%s zW=%d%s%s lineW=%d "
+                "lineT=%d ord=%d pf=%d\n",
+                passes, i, t, cands[i].k1W, cands[i].k1G, cands[i].k1_tma ? "(tma)" : "",
+                cands[i].k1_reload ? "(reload)" : "", cands[i].xG, cands[i].x_tma ? "(tma)" : "",
+                cands[i].zW, cands[i].z_tma ? "(tma)" : cands[i].z_pfself ? "(pfs)" : "",
+                cands[i].carry ? (cands[i].carry_reload ? "(+K1r)" : "(+K1)") : "",
+                cands[i].lineW, cands[i].lineT, cands[i].lineOrd, cands[i].pf_waves);
       if (t < best) {
         best = t;
         bi = (int)i;
@@ -1419,13 +1560,15 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
   if (rc == OK) {
     c.clear();
     for (int W : {2, 4, 8, 16, 32}) {
-      if (zw_ok(pl, W, max_blocks)) {
-        NSPlan q = pl;
-        q.zW = W;
-        q.z_tma = false;
-        q.update_blocks = (pl.nx / W) * pl.ny;
-        c.push_back(q);
-      }
+      if (zw_ok(pl, W, max_blocks))
+        for (int pfs = 0; pfs < 2; pfs++) {
+          NSPlan q = pl;
+          q.zW = W;
+          q.z_tma = false;
+          q.z_pfself = pfs == 1;
+          q.update_blocks = (pl.nx / W) * pl.ny;
+          c.push_back(q);
+        }
       if (sync_words && zw_ok(pl, W, max_blocks) && z_tma_ok(pl, W)) {
         NSPlan q = pl;
         q.zW = W;
@@ -1435,6 +1578,24 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
       }
     }
     if (!c.empty()) rc = pick(c, 0x10u);
+  }
+  // K5 with the next step's K1 carried in it (tile widths), against the
+  // plan so far, over the whole step: it trades K1's pass for a heavier K5
+  if (rc == OK && !pl.k1_lines && !getenv("SNS_CARRY")) {
+    c.clear();
+    c.push_back(pl);
+    for (int reload = 0; reload < 2; reload++)
+      for (int Wd : {2, 4, 8, 16, 32})
+        if (zw_ok(pl, Wd, max_blocks) && carry_ok(pl, Wd, reload)) {
+          NSPlan q = pl;
+          q.carry = true;
+          q.carry_reload = reload;
+          q.z_tma = false;
+          q.zW = Wd;
+          q.update_blocks = (pl.nx / Wd) * pl.ny;
+          c.push_back(q);
+        }
+    rc = pick(c, 0x1Fu);
   }
   // L2 prefetch distance of all five passes, timed over the whole step
   // (unless SNS_PF fixes it)

@@ -12,6 +12,12 @@ struct NSPlan {
   int xG;             // rows per CTA of the x cross pass
   bool x_tma;         // the x cross pass as a persistent pass over TMA-staged rows
   bool z_tma;         // the update pass as a persistent pass over TMA-staged z lines
+  bool carry;         // the update pass also does the next step's K1 (z-inverse of
+                      // the new V and its curl into U), so the next step skips K1
+  bool carry_reload;  // ... reading the new V back from V (L1/L2) instead of keeping
+                      // it in a second set of shared-memory rows
+  bool z_pfself;      // the update pass asks L2 for each tile's V and C0 before its
+                      // z-forward
   int k1W, k1G;       // K1 tile: adjacent z lines x groups (all six outputs per CTA)
   bool k1_fused;      // K1 loads V once per tile (else one output field per CTA)
   bool k1_reload;     // the fused K1 forms omega from reloads of V (L1), not shared memory
@@ -51,11 +57,20 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW = 0, int lineW 
 // `ev`, when not null, holds kNSPasses + 1 events recorded around the passes.
 // `sync_words` (xy_sync_words(nz) ints) serves the dataflow xy pass.  W: five
 // more work fields, needed when pl.k1_lines (else may be null).
+// `carried` (may be null: no carrying) tracks, for a plan with pl.carry,
+// whether U already holds K1's output for the current V: when *carried is
+// true the step skips K1 (its pass time is then empty); on return it says
+// whether this step's K5 left the next step's K1 output in U.  Anything else
+// that writes V or U must clear it.
 constexpr int kNSPasses = 5;
 constexpr int kNSLineWork = 5;
 int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* const U[6],
                  double* stats, int* sync_words, double nu, double dt, cudaStream_t s,
-                 cudaEvent_t* ev = nullptr, void* const* W = nullptr);
+                 cudaEvent_t* ev = nullptr, void* const* W = nullptr, bool* carried = nullptr);
+// K1 alone (z-inverse of V and of i k x V into U[0..5]), for a carrying plan
+// whose U does not hold it yet (before a captured steady-state step).
+int ns_k1_once(const NSPlan& pl, void* const V[3], void* const U[6], int* sync_words,
+               cudaStream_t s);
 // The update pass (z-forward + AB2 / projection / CN update) on the fields of
 // `a`; sgs adds the divergence of the Fourier eddy stress a.tau.
 struct UpdateArgs;

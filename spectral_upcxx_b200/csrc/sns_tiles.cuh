@@ -530,6 +530,11 @@ struct UpdateArgs {
   double sgs_klo, sgs_kinv;
   // L2 prefetch distance in tiles (0: none)
   int64_t pf;
+  // the carried z-inverse pass (zfwd_update_curl_tile): out(0..2) = the new
+  // V, out(3..5) = i k x V, both z-inverse-transformed
+  void* Uo[6];
+  // ask L2 for this tile's V and C0 before its z-forward (0: no)
+  int pf_self;
 };
 
 // Field f of the update's z-forward: the cross product (f < 3) or, with the
@@ -551,7 +556,12 @@ __device__ __forceinline__ const void* update_field(const UpdateArgs& a, int f) 
 // The z lines come through load(fld, w, j, v): the E elements j + e*TPL of
 // line w of field fld (zfwd_update_tile reads them from HBM; the TMA-staged
 // pass from its shared-memory stage).
-template <typename T, int L, bool SGS, typename Load>
+//
+// KEEP = true also leaves the new velocity in the tile's first three rows
+// (component d of line w at (d W + w) RS + pad_pos(z), where the z-forward of
+// the cross product was), ordered before the caller's reads by the block
+// barrier of the diagnostics' reduction.
+template <typename T, int L, bool SGS, bool KEEP = false, typename Load>
 __device__ __forceinline__ void zfwd_update_tile_from(const UpdateArgs& a,
                                                       const cx_t<T>* __restrict__ tw, int64_t blk,
                                                       int nthr, cx_t<T>* sm, double (*red)[32],
@@ -662,6 +672,7 @@ __device__ __forceinline__ void zfwd_update_tile_from(const UpdateArgs& a,
       Vn[d] = vv;
       Vp[d][idx] = vv;
       Cp[d][idx] = c1[d];
+      if constexpr (KEEP) sm[(d * W + w) * RS + pad_pos(z)] = vv;
     }
     // diagnostics of the new velocity: per-mode terms in T, sums in FP64
     const C dv = cadd(cadd(ikmul(kx, Vn[0]), ikmul(ky, Vn[1])), ikmul(kz, Vn[2]));
@@ -729,7 +740,7 @@ __device__ __forceinline__ void zfwd_update_tile_from(const UpdateArgs& a,
 
 // K5 tile with its loads from HBM straight into registers, optionally asking
 // L2 for the inputs of tile blk + pf first.
-template <typename T, int L, bool SGS = false>
+template <typename T, int L, bool SGS = false, bool KEEP = false>
 __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
                                                  const cx_t<T>* __restrict__ tw, int64_t blk,
                                                  int nthr, cx_t<T>* sm, double (*red)[32]) {
@@ -738,6 +749,17 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
   const int W = a.W;
   const int64_t nxy = (int64_t)a.nx * a.ny;
   const int64_t base = blk * W;
+  if (!SGS && a.pf_self) {
+    // this tile's V and C0 into L2, so that the update's loads after the
+    // z-forward find them there
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      prefetch_lines<L>(reinterpret_cast<const char*>(a.V[d]), base, W, 1, 0, nxy, (int)sizeof(C),
+                        nthr);
+      prefetch_lines<L>(reinterpret_cast<const char*>(a.C0[d]), base, W, 1, 0, nxy,
+                        (int)sizeof(C), nthr);
+    }
+  }
   if (!SGS && a.pf > 0 && (blk + a.pf) * W < nxy) {
     // tile blk + pf's cross product, V and C0 into L2
     const int64_t bp = (blk + a.pf) * W;
@@ -751,13 +773,95 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
                         nthr);
     }
   }
-  zfwd_update_tile_from<T, L, SGS>(a, tw, blk, nthr, sm, red, [&](int fld, int w, int j, C (&v)[E]) {
+  zfwd_update_tile_from<T, L, SGS, KEEP>(a, tw, blk, nthr, sm, red, [&](int fld, int w, int j, C (&v)[E]) {
     const C* __restrict__ src = reinterpret_cast<const C*>(
         SGS ? update_field(a, fld) : (fld == 0 ? a.U[0] : fld == 1 ? a.U[1] : a.U[2]));
     const int64_t i0 = base + w + nxy * j;
 #pragma unroll
     for (int e = 0; e < E; e++) v[e] = src[i0 + nxy * (TPL * e)];
   });
+}
+
+// K5 with the next step's K1 carried in it: the update of zfwd_update_tile,
+// then the z-inverse of the new velocity and of its curl omega = i k x V from
+// the tile's rows (KEEP), into a.Uo -- what K1 of the next step would compute
+// from V in HBM, with the arithmetic of curl_zpass_tile_staged (same line FFT,
+// same products), so a step that starts from these fields skips K1 and the
+// re-read of V.  The tile's W z lines all lie in one xy-plane run, so their
+// (kx, ky) come from the line's xy offset.  Shared memory: the 3 W rows of the
+// update, then 3 W exchange rows for the line FFTs (the rows of V stay intact
+// while the curl reads them).
+//
+// RELOAD = true keeps K5's shared memory (3 W rows, so as many CTAs per SM
+// as K5): the new velocity is read back from V, which this CTA has just
+// written (L1/L2, not DRAM; the block barrier of the diagnostics makes the
+// stores visible), and each thread's own row serves as its exchange row, as
+// in curl_zpass_tile_reload.
+template <typename T, int L, bool RELOAD = false>
+__device__ __forceinline__ void zfwd_update_curl_tile(const UpdateArgs& a,
+                                                      const cx_t<T>* __restrict__ tw, int64_t blk,
+                                                      int nthr, cx_t<T>* sm, double (*red)[32]) {
+  using C = cx_t<T>;
+  constexpr int E = LinePlan<L>::E, TPL = LinePlan<L>::TPL;
+  zfwd_update_tile<T, L, false, !RELOAD>(a, tw, blk, nthr, sm, red);
+  const int W = a.W;
+  const int RS = tile_stride(L, W, (int)sizeof(C));
+  const int64_t nxy = (int64_t)a.nx * a.ny;
+  const int w = threadIdx.x % W, s = threadIdx.x / W;
+  const int j = s % TPL, d = s / TPL;  // line w of component d, positions j + e TPL
+  const int64_t xy = blk * W + w;
+  const int x = (int)(xy & (a.nx - 1)), y = (int)(xy >> a.lx);
+  const int64_t idx0 = xy + nxy * j, step = nxy * TPL;
+  const C* v0 = reinterpret_cast<const C*>(a.V[0]);
+  const C* v1 = reinterpret_cast<const C*>(a.V[1]);
+  const C* v2 = reinterpret_cast<const C*>(a.V[2]);
+  const C* vr = sm + (d * W + w) * RS;
+  C* xrow = RELOAD ? sm + (d * W + w) * RS : sm + (3 * W + d * W + w) * RS;
+  C v[E];
+  if constexpr (RELOAD) {
+    const C* src = d == 0 ? v0 : d == 1 ? v1 : v2;
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = src[idx0 + e * step];
+  } else {
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = vr[pad_pos(j + TPL * e)];
+  }
+  line_fft<L, true>(v, xrow, j, tw, (T)1);
+  {
+    C* __restrict__ dst = reinterpret_cast<C*>(d == 0 ? a.Uo[0] : d == 1 ? a.Uo[1] : a.Uo[2]);
+#pragma unroll
+    for (int e = 0; e < E; e++) dst[idx0 + e * step] = v[e];
+  }
+  {
+    // (ky Vz - kz Vy, kz Vx - kx Vz, kx Vy - ky Vx) times i, as curl_zpass_tile forms it
+    const C* pa = sm + ((d == 0 ? 2 : d == 1 ? 0 : 1) * W + w) * RS;
+    const C* pb = sm + ((d == 0 ? 1 : d == 1 ? 2 : 0) * W + w) * RS;
+    const C* ga = d == 0 ? v2 : d == 1 ? v0 : v1;
+    const C* gb = d == 0 ? v1 : d == 1 ? v2 : v0;
+    const T kx = a.kx_half ? (T)x : (T)freq_i(x, a.nx);
+    const T ky = (T)freq_i(y, a.ny);
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int p = j + TPL * e;
+      const T kz = (T)freq_i(p, a.nz);
+      const C va = RELOAD ? ga[idx0 + e * step] : pa[pad_pos(p)];
+      const C vb = RELOAD ? gb[idx0 + e * step] : pb[pad_pos(p)];
+      if (d == 0)
+        v[e] = csub(ikmul(ky, va), ikmul(kz, vb));
+      else if (d == 1)
+        v[e] = csub(ikmul(kz, va), ikmul(kx, vb));
+      else
+        v[e] = csub(ikmul(kx, va), ikmul(ky, vb));
+    }
+  }
+  // the last stage of the first transform read its exchange row before a
+  // block barrier, so the second may write it at once
+  line_fft<L, true>(v, xrow, j, tw, (T)1);
+  {
+    C* __restrict__ dst = reinterpret_cast<C*>(d == 0 ? a.Uo[3] : d == 1 ? a.Uo[4] : a.Uo[5]);
+#pragma unroll
+    for (int e = 0; e < E; e++) dst[idx0 + e * step] = v[e];
+  }
 }
 
 // Entry i of a pointer table in kernel parameters, selected with constant

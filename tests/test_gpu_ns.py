@@ -329,6 +329,93 @@ def test_x_tma_matches_direct_bit_for_bit(sns, cuda, dtype, shape, monkeypatch):
         assert torch.equal(a, b)
 
 
+@pytest.mark.parametrize("graph", ["0", "1"])
+@pytest.mark.parametrize("real", [False, True])
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (32, 64, 128), (512, 16, 32), (8, 16, 32)])
+def test_carried_k1_matches_separate_bit_for_bit(sns, cuda, dtype, shape, real, graph,
+                                                 monkeypatch):
+    """The update pass with the next step's K1 carried in it (SNS_CARRY=1:
+    after the update the tile z-inverse-transforms the new V and its curl
+    into the work fields, so the next step skips K1; 2: the new V read back
+    from HBM's caches instead of shared memory) does K1's arithmetic on
+    the same values: five steps, a new state set, three more steps -- the
+    states and diagnostics are identical bit for bit to the plan without
+    carrying (the FP64 diagnostics to 1e-12: their per-tile partials may be
+    summed in another order), with and without the CUDA graph (whose captured
+    step is the one without K1; after the new state K1 runs once before the
+    replay), on complex and half-spectrum (real-field) steppers."""
+    N = sns._native
+    V = _random_fourier(shape, dtype, cuda, 13)
+    V2 = _random_fourier(shape, dtype, cuda, 14)
+    monkeypatch.setenv("SNS_GRAPH", graph)
+    out, stats = {}, {}
+    for mode in ("0", "1", "2"):
+        monkeypatch.setenv("SNS_CARRY", mode)
+        st = sns.NSStepper(shape, 1 / 400, 5e-4, dtype, real=real)
+        assert ("(+K1" in st.describe()) == (mode != "0"), st.describe()
+        assert ("(+K1r)" in st.describe()) == (mode == "2"), st.describe()
+        st.bootstrap(V, sns.curl(V))
+        st.step(5)
+        first = st.stats()
+        mid = [x.clone() for x in st.state()["V1"]]
+        st.set_state(V2, V)
+        st.step(3)
+        rc = N.lib().sns_ns_check(st.h)
+        assert rc == N.SNS_OK, (mode, rc, N.last_error())
+        out[mode] = mid + [x.clone() for x in st.state()["V1"]] + \
+            [x.clone() for x in st.state()["cross0"]]
+        stats[mode] = (first, st.stats())
+        st.close()
+    for mode in ("1", "2"):
+        for a, b in zip(out[mode], out["0"]):
+            assert torch.equal(a, b), mode
+        # the carrying plan may tile the update pass at another width, which
+        # sums the per-tile FP64 diagnostics in another order
+        for s1, s0 in zip(stats[mode], stats["0"]):
+            for k in s0:
+                assert abs(s1[k] - s0[k]) <= 1e-12 * abs(s0[k]), (mode, k, s1[k], s0[k])
+
+
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+def test_update_self_prefetch_bit_for_bit(sns, cuda, dtype, monkeypatch):
+    """Asking L2 for a tile's V and C0 before the update pass's z-forward
+    (SNS_Z_PFSELF=1) is a hint only: three steps are identical bit for bit."""
+    shape = (64, 32, 128)
+    V = _random_fourier(shape, dtype, cuda, 16)
+    out = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("SNS_Z_PFSELF", mode)
+        st = sns.NSStepper(shape, 1 / 400, 5e-4, dtype)
+        assert ("(pfs)" in st.describe()) == (mode == "1"), st.describe()
+        st.bootstrap(V, sns.curl(V))
+        st.step(3)
+        out[mode] = [x.clone() for x in st.state()["V1"]] + [x.clone() for x in st.state()["cross0"]]
+        st.close()
+    for a, b in zip(out["1"], out["0"]):
+        assert torch.equal(a, b)
+
+
+def test_carried_k1_pass_times(sns, cuda, monkeypatch):
+    """Per-pass timing of a carrying plan: K1 runs in the first step only
+    (its later pass times are empty), the update pass carries it."""
+    monkeypatch.setenv("SNS_CARRY", "2")
+    shape = (128, 128, 128)
+    V = _random_fourier(shape, torch.complex64, cuda, 15)
+    st = sns.NSStepper(shape, 1 / 400, 5e-4, torch.complex64)
+    st.bootstrap(V, sns.curl(V))
+    st.profile(True)
+    st.step(1)
+    (k1_first, n1), *_ = st.pass_times()
+    st.profile(True)
+    st.step(4)
+    (k1_later, n4), *_ = st.pass_times()
+    st.close()
+    assert (n1, n4) == (1, 4)
+    assert k1_first > 0
+    assert k1_later / 4 < 0.25 * k1_first, (k1_first, k1_later)
+
+
 @pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
 @pytest.mark.parametrize("shape", [(64, 64, 64), (32, 64, 128), (512, 16, 32)])
 def test_z_tma_update_matches_direct_bit_for_bit(sns, cuda, dtype, shape, monkeypatch):
