@@ -80,11 +80,20 @@ int sns_fft3d_many(void* const* fields, int nfields, int64_t nx, int64_t ny, int
  * nx*ny*nz by measurement (the counterpart of the reference's FFTW_MEASURE
  * planning, src/FFT1D.cpp:18-22): per axis the tile width, thread count and
  * radix order (radix-16 stages with the remainder last or first, or radix-8
- * stages), and for 128 x 128 planes the plane pass against two line passes.
+ * stages), for y and z lines the TMA-staged form of the pass (one or two
+ * shared-memory stages per persistent CTA), and for 128 x 128 planes the
+ * plane pass against two line passes.
  * Runs on scratch fields from the pool; the choice is cached per device and
  * shape and used by every later transform of that shape (results agree with
  * the default plan to rounding).  SNS_TUNE=1 tunes each new shape on first use. */
 int sns_fft3d_tune(int64_t nx, int64_t ny, int64_t nz, int nfields, int prec, void* stream);
+/* Check of the transforms queued so far on this device (no reference
+ * counterpart: the reference's FFTW calls have no asynchronous failure).
+ * The TMA-staged passes of a tuned plan bound every wait; one that runs out,
+ * or a tile box that fails the kernel's own alignment check, is recorded on
+ * the device.  Synchronises `stream`, reads and clears the record:
+ * SNS_ERR_TIMEOUT (results of those transforms invalid) or SNS_OK. */
+int sns_fft3d_check(void* stream);
 /* The line passes of selected axes only (bit 0: x, bit 1: y, bit 2: z), in that
  * order, the last one multiplied by `scale` (1: none).  The local phases of the
  * slab-distributed transform of Scalar::transform (src/Scalar.cpp:419-566: the

@@ -52,6 +52,7 @@ SIGNATURES = {
     "sns_forward": ([_vp, _i64, _i64, _i64, _int, _vp], _int),
     "sns_inverse": ([_vp, _i64, _i64, _i64, _int, _vp], _int),
     "sns_fft3d_tune": ([_i64, _i64, _i64, _int, _int, _vp], _int),
+    "sns_fft3d_check": ([_vp], _int),
     "sns_fft3d_axes": ([_vp, _i64, _i64, _i64, _int, _int, _dbl, _int, _vp], _int),
     "sns_fft1d_many": ([_vp, _i64, _i64, _i64, _i64, _int, _int, _vp], _int),
     "sns_fft1d_many_scaled": ([_vp, _i64, _i64, _i64, _i64, _int, _dbl, _int, _vp], _int),

@@ -527,6 +527,8 @@ int sns_fft3d_tune(int64_t nx, int64_t ny, int64_t nz, int nfields, int prec, vo
   return fft3d_tune((int)nx, (int)ny, (int)nz, nfields, prec, S(stream));
 }
 
+int sns_fft3d_check(void* stream) { return fft_tma_check(S(stream)); }
+
 int sns_fft1d_many(void* data, int64_t n, int64_t stride, int64_t howmany, int64_t dist,
                    int dir, int prec, void* stream) {
   return fft1d_lines(data, n, stride, howmany, dist, dir, 1.0, prec, S(stream));
@@ -1080,14 +1082,15 @@ int sns_ns_describe(sns_ns* h, char* buf, int len) {
   char tmp[256];
   const char* ord[3] = {"16-first", "remainder-first", "radix-8"};
   const int n = snprintf(tmp, sizeof(tmp),
-                         "passes=%d xy=%s k1=%dx%d%s y=W%d/T%d/%s zW=%d%s xG=%d%s pf=%d%s%s",
+                         "passes=%d xy=%s k1=%dx%d%s y=W%d/T%d/%s%s zW=%d%s xG=%d%s pf=%d%s%s",
                          h->cl.model != CLOSURE_NONE ? kLESLaunches : p.passes, xy,
                          p.k1_lines ? p.k1lW : p.k1W, p.k1_lines ? p.k1lT : p.k1G,
                          p.k1_lines ? "(lines)" : !p.k1_fused ? "(split)"
                          : p.k1_tma ? (p.k1_stages == 1 ? "(tma1)" : "(tma2)")
                          : p.k1_reload ? "(reload)" : "",
                          p.lineW, p.lineT,
-                         ord[p.lineOrd % 3], p.zW, p.z_tma ? "(tma)" : p.carry ? (p.carry_reload ? "(+K1r)" : "(+K1)") : p.z_pfself ? "(pfs)" : "", p.xG, p.x_tma ? "(tma)" : "", p.pf_waves, p.real ? " real" : "",
+                         ord[p.lineOrd % 3],
+                         p.y_tma == 1 ? "(tma1)" : p.y_tma == 2 ? "(tma2)" : "", p.zW, p.z_tma ? "(tma)" : p.carry ? (p.carry_reload ? "(+K1r)" : "(+K1)") : p.z_pfself ? "(pfs)" : "", p.xG, p.x_tma ? "(tma)" : "", p.pf_waves, p.real ? " real" : "",
                          p.tuned ? " tuned" : "");
   if (buf && len > 0) {
     strncpy(buf, tmp, (size_t)len - 1);

@@ -8,6 +8,7 @@
 // are disjoint, so passes run in place; the reference's transpose buffer
 // (`tmp`, src/Scalar.cpp:113-122) is not needed.
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -320,6 +321,19 @@ int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int fla
     return tuned ? axis_geo(axis, nx, ny, nz, prec, tc.wmax[axis], tc.tmax[axis], tc.ord[axis])
                  : axis_geo(axis, nx, ny, nz, prec);
   };
+  // a pass of the plan: the TMA-staged form where the tuned plan chose it
+  // (SNS_FFT_TMA = 1 or 2 stages asks for it on the y and z passes of an
+  // untuned plan)
+  int forced = 0;
+  if (const char* e = getenv("SNS_FFT_TMA")) forced = atoi(e);
+  if (forced != 1 && forced != 2) forced = 0;
+  int* err_word = (tuned || forced) && !tw_axes ? fft_tma_err_word() : nullptr;
+  auto pass = [&](int axis, const LineGeo& g, int sg, int fl) {
+    const int S = tuned ? tc.tma[axis] : (axis > 0 ? forced : 0);
+    if (S && err_word && nf <= 6 && line_tma_ok(g, prec, S))
+      return run_line_pass_tma(g, f, sg, fl, 1.0 / N, prec, stream, S, err_word);
+    return run_line_pass(g, f, sg, fl, 1.0 / N, prec, stream);
+  };
   const bool plane = tuned ? tc.plane : true;
   if (!tw_axes && plane && fft_xy_supported(nx, ny, nz, nf, prec)) {
     // two passes: xy planes and z lines (forward xy first, inverse z first),
@@ -328,10 +342,10 @@ int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int fla
     if (sign < 0) {
       int rc = fft_xy_pass(f, nx, nz, sign, z_pass ? 0 : flags, 1.0 / N, prec, stream);
       if (rc || !z_pass) return rc;
-      return run_line_pass(geo(2), f, sign, flags, 1.0 / N, prec, stream);
+      return pass(2, geo(2), sign, flags);
     }
     if (z_pass) {
-      int rc = run_line_pass(geo(2), f, sign, 0, 1.0 / N, prec, stream);
+      int rc = pass(2, geo(2), sign, 0);
       if (rc) return rc;
     }
     return fft_xy_pass(f, nx, nz, sign, flags, 1.0 / N, prec, stream);
@@ -347,7 +361,7 @@ int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int fla
     LineGeo g = geo(axes[i]);
     if (tw_axes) g.tw = tw_axes[axes[i]];
     int fl = (i == na - 1) ? flags : 0;
-    int rc = run_line_pass(g, f, sign, fl, 1.0 / N, prec, stream);
+    int rc = pass(axes[i], g, sign, fl);
     if (rc) return rc;
   }
   if (na == 0 && flags) {
@@ -435,41 +449,55 @@ int fft3d_tune(int nx, int ny, int nz, int nf, int prec, cudaStream_t stream) {
     c.wmax[a] = 0;
     c.tmax[a] = 0;
     c.ord[a] = 0;
+    c.tma[a] = 0;
   }
   c.plane = false;
   const int dims[3] = {nx, ny, nz};
+  // the pass of axis a under a candidate plan (its TMA-staged form if chosen)
+  int* err_word = fft_tma_err_word();
+  auto tma_fits = [&](const FftChoice& q, int a, int S) {
+    return S == 0 || (a > 0 && err_word && nf <= 6 &&
+                      line_tma_ok(axis_geo(a, nx, ny, nz, prec, q.wmax[a], q.tmax[a], q.ord[a]),
+                                  prec, S));
+  };
+  auto one = [&](const FftChoice& q, int a, int sg) {
+    const LineGeo g = axis_geo(a, nx, ny, nz, prec, q.wmax[a], q.tmax[a], q.ord[a]);
+    if (q.tma[a] && tma_fits(q, a, q.tma[a]))
+      return run_line_pass_tma(g, f, sg, 0, 1.0, prec, stream, q.tma[a], err_word);
+    return run_line_pass(g, f, sg, 0, 1.0, prec, stream);
+  };
   for (int a = 0; a < 3 && rc == OK; a++) {
     if (dims[a] < 2) continue;
     // run width (y, z) and thread cap, then radix order, of this axis's pass
     float best = 3.4e38f;
     FftChoice bc = c;
-    for (int W : {4, 8, 16})
-      for (int T : {128, 256, 512}) {
-        if (a == 0 && W != 16) continue;  // x lines are single lines
-        FftChoice q = c;
-        q.wmax[a] = W;
-        q.tmax[a] = T;
-        float t = 0;
-        rc = timed([&](int sg) {
-          return run_line_pass(axis_geo(a, nx, ny, nz, prec, q.wmax[a], q.tmax[a], q.ord[a]), f,
-                               sg, 0, 1.0, prec, stream);
-        }, &t);
-        if (rc) break;
-        if (t < best) {
-          best = t;
-          bc = q;
+    for (int W : {4, 8, 16, 32})
+      for (int T : {128, 256, 512})
+        for (int S = 0; S <= 2 && rc == OK; S++) {
+          if (a == 0 && W != 16) continue;  // x lines are single lines
+          FftChoice q = c;
+          q.wmax[a] = W;
+          q.tmax[a] = T;
+          q.tma[a] = S;
+          if (!tma_fits(q, a, S)) continue;
+          float t = 0;
+          rc = timed([&](int sg) { return one(q, a, sg); }, &t);
+          if (rc) break;
+          if (getenv("SNS_TUNE_LOG") && getenv("SNS_TUNE_LOG")[0] == '1')
+            fprintf(stderr, "fft3d_tune axis=%d W=%d T=%d tma=%d ms=%.4f\n", a, W, T, S, t);
+          if (t < best) {
+            best = t;
+            bc = q;
+          }
         }
-      }
     c = bc;
     if (rc == OK && dims[a] >= 64 && dims[a] <= 1024) {
       for (int o = 1; o < kRadixOrders && rc == OK; o++) {
         FftChoice q = c;
         q.ord[a] = o;
+        if (!tma_fits(q, a, q.tma[a])) continue;
         float t = 0;
-        rc = timed([&](int sg) {
-          return run_line_pass(axis_geo(a, nx, ny, nz, prec, q.wmax[a], q.tmax[a], q.ord[a]), f,
-                               sg, 0, 1.0, prec, stream);
-        }, &t);
+        rc = timed([&](int sg) { return one(q, a, sg); }, &t);
         if (rc == OK && t < best) {
           best = t;
           bc = q;
@@ -482,11 +510,8 @@ int fft3d_tune(int nx, int ny, int nz, int nf, int prec, cudaStream_t stream) {
   if (rc == OK && fft_xy_supported(nx, ny, nz, nf, prec)) {
     float t_lines = 0, t_plane = 0;
     rc = timed([&](int sg) {
-      int e = run_line_pass(axis_geo(0, nx, ny, nz, prec, c.wmax[0], c.tmax[0], c.ord[0]), f, sg,
-                            0, 1.0, prec, stream);
-      if (!e)
-        e = run_line_pass(axis_geo(1, nx, ny, nz, prec, c.wmax[1], c.tmax[1], c.ord[1]), f, sg, 0,
-                          1.0, prec, stream);
+      int e = one(c, 0, sg);
+      if (!e) e = one(c, 1, sg);
       return e;
     }, &t_lines);
     if (rc == OK)
@@ -503,14 +528,16 @@ int fft3d_tune(int nx, int ny, int nz, int nf, int prec, cudaStream_t stream) {
         const int* order = sg < 0 ? axes_fwd : axes_inv;
         const bool plane = ch ? ch->plane : true;
         if (plane && fft_xy_supported(nx, ny, nz, nf, prec)) {
-          LineGeo gz = ch ? axis_geo(2, nx, ny, nz, prec, ch->wmax[2], ch->tmax[2], ch->ord[2])
-                          : axis_geo(2, nx, ny, nz, prec);
+          auto zpass = [&]() {
+            return ch ? one(*ch, 2, sg)
+                      : run_line_pass(axis_geo(2, nx, ny, nz, prec), f, sg, 0, 1.0, prec, stream);
+          };
           int e = 0;
           if (sg < 0) {
             e = fft_xy_pass(f, nx, nz, sg, 0, 1.0, prec, stream);
-            if (!e && nz > 1) e = run_line_pass(gz, f, sg, 0, 1.0, prec, stream);
+            if (!e && nz > 1) e = zpass();
           } else {
-            if (nz > 1) e = run_line_pass(gz, f, sg, 0, 1.0, prec, stream);
+            if (nz > 1) e = zpass();
             if (!e) e = fft_xy_pass(f, nx, nz, sg, 0, 1.0, prec, stream);
           }
           return e;
@@ -518,9 +545,8 @@ int fft3d_tune(int nx, int ny, int nz, int nf, int prec, cudaStream_t stream) {
         for (int i = 0; i < 3; i++) {
           const int a = order[i];
           if (dims[a] < 2) continue;
-          LineGeo g = ch ? axis_geo(a, nx, ny, nz, prec, ch->wmax[a], ch->tmax[a], ch->ord[a])
-                         : axis_geo(a, nx, ny, nz, prec);
-          int e = run_line_pass(g, f, sg, 0, 1.0, prec, stream);
+          int e = ch ? one(*ch, a, sg)
+                     : run_line_pass(axis_geo(a, nx, ny, nz, prec), f, sg, 0, 1.0, prec, stream);
           if (e) return e;
         }
         return OK;
@@ -534,10 +560,13 @@ int fft3d_tune(int nx, int ny, int nz, int nf, int prec, cudaStream_t stream) {
         c.wmax[a] = 0;
         c.tmax[a] = 0;
         c.ord[a] = 0;
+        c.tma[a] = 0;
       }
       c.plane = true;
     }
   }
+  // a TMA-staged candidate that recorded a failure must not be kept
+  if (rc == OK) rc = fft_tma_check(stream);
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
   for (int i = 0; i < nf; i++) pool_free(fld[i]);

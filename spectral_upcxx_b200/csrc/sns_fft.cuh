@@ -116,6 +116,15 @@ bool line_supported(int64_t L);
 int run_line_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags, double scale,
                   int prec, cudaStream_t stream, int prologue = PRO_LOAD);
 
+// The same pass (plain loads only, y or z lines, 1..6 fields, L = 32..512)
+// as a persistent pass over TMA-staged tiles with `stages` (1 or 2) shared
+// memory stages (sns_line_tma.cu); its bounded waits record into *err
+// (1: a wait ran out, 2: a box failed the kernel's own check).  Same results
+// bit for bit as run_line_pass.
+bool line_tma_ok(const LineGeo& geo, int prec, int stages);
+int run_line_pass_tma(const LineGeo& geo, const FieldPtrs& f, int sign, int flags, double scale,
+                      int prec, cudaStream_t stream, int stages, int* err);
+
 // Geometry of the lines along `axis` (0 = x, 1 = y, 2 = z) of nx*ny*nz fields.
 // wmax > 0 caps the adjacent lines per tile at that width (a tuned value).
 // Geometry of the lines along `axis`; wmax caps the adjacent lines of a tile,
@@ -142,8 +151,14 @@ int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int fla
 // and whether the xy plane pass is used where it is available.
 struct FftChoice {
   int wmax[3], tmax[3], ord[3];
+  int tma[3];  // stages of the TMA-staged form of the y and z passes (0: direct loads)
   bool plane;
 };
+// Error word of the transform's TMA-staged passes on the current device
+// (null if it cannot be set up), and its check: reads and clears it,
+// SNS_ERR_TIMEOUT with the error text when a pass recorded a failure.
+int* fft_tma_err_word();
+int fft_tma_check(cudaStream_t s);
 // Measure candidate plans for nf fields of nx*ny*nz on pool scratch fields and
 // cache the fastest for this device (the counterpart of FFTW_MEASURE,
 // src/FFT1D.cpp:18-22); fft3d then uses it for that shape.

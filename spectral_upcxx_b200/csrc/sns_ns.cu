@@ -1133,6 +1133,14 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
   pl.lineW = lineW > 0 ? lineW : 0;
   pl.lineT = 0;
   pl.lineOrd = 0;
+  {
+    // the y passes over TMA-staged tiles on request (SNS_Y_TMA = 1 or 2 stages)
+    const char* e = getenv("SNS_Y_TMA");
+    const int v = e ? atoi(e) : 0;
+    pl.y_tma = 0;
+    if ((v == 1 || v == 2) && line_tma_ok(axis_geo(1, nx, ny, nz, prec), prec, v))
+      pl.y_tma = v;
+  }
   pl.tuned = false;
   pl.k1_lines = false;  // enabled by a caller that provides the work fields W
   {
@@ -1276,7 +1284,9 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
       for (int i = 0; i < 6; i++) f.in[i] = f.out[i] = Uc[i];
       LineGeo g = axis_geo(1, nx, ny, pz, prec, pl.lineW, pl.lineT, pl.lineOrd);
       g.pfw = pl.pf_waves;
-      int r = run_line_pass(g, f, +1, 0, 1.0, prec, s);
+      int r = pl.y_tma && err_word && line_tma_ok(g, prec, pl.y_tma)
+                  ? run_line_pass_tma(g, f, +1, 0, 1.0, prec, s, pl.y_tma, err_word)
+                  : run_line_pass(g, f, +1, 0, 1.0, prec, s);
       if (r) return r;
       if (marks) mark();
     }
@@ -1296,7 +1306,9 @@ int ns_step_once(const NSPlan& pl, void* const V[3], void* const C0[3], void* co
       for (int i = 0; i < 3; i++) f.in[i] = f.out[i] = Uc[i];
       LineGeo g = axis_geo(1, nx, ny, pz, prec, pl.lineW, pl.lineT, pl.lineOrd);
       g.pfw = pl.pf_waves;
-      int r = run_line_pass(g, f, -1, 0, 1.0, prec, s);
+      int r = pl.y_tma && err_word && line_tma_ok(g, prec, pl.y_tma)
+                  ? run_line_pass_tma(g, f, -1, 0, 1.0, prec, s, pl.y_tma, err_word)
+                  : run_line_pass(g, f, -1, 0, 1.0, prec, s);
       if (r) return r;
     }
     return OK;
@@ -1450,12 +1462,13 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
       if (log)
         fprintf(stderr,
                 "ns_tune passes=0x%x cand=%zu ms=%.4f k1=%dx%d%s%s xG=%d%s zW=%d%s%s lineW=%d "
-                "lineT=%d ord=%d pf=%d\n",
+                "lineT=%d ord=%d ytma=%d pf=%d\n",
                 passes, i, t, cands[i].k1W, cands[i].k1G, cands[i].k1_tma ? "(tma)" : "",
                 cands[i].k1_reload ? "(reload)" : "", cands[i].xG, cands[i].x_tma ? "(tma)" : "",
                 cands[i].zW, cands[i].z_tma ? "(tma)" : cands[i].z_pfself ? "(pfs)" : "",
                 cands[i].carry ? (cands[i].carry_reload ? "(+K1r)" : "(+K1)") : "",
-                cands[i].lineW, cands[i].lineT, cands[i].lineOrd, cands[i].pf_waves);
+                cands[i].lineW, cands[i].lineT, cands[i].lineOrd, cands[i].y_tma,
+                cands[i].pf_waves);
       if (t < best) {
         best = t;
         bi = (int)i;
@@ -1519,13 +1532,18 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
   // K2 + K4: run width and thread cap, then radix order, of the y line passes
   if (rc == OK) {
     c.clear();
-    for (int W : {4, 8, 16})
-      for (int T : {128, 256, 512}) {
-        NSPlan q = pl;
-        q.lineW = W;
-        q.lineT = T;
-        c.push_back(q);
-      }
+    for (int W : {4, 8, 16, 32})
+      for (int T : {128, 256, 512})
+        for (int S = 0; S <= (sync_words ? 2 : 0); S++) {
+          NSPlan q = pl;
+          q.lineW = W;
+          q.lineT = T;
+          q.y_tma = S;
+          if (S && !line_tma_ok(axis_geo(1, pl.nx, pl.ny, pl.nz, pl.prec, W, T, pl.lineOrd),
+                                pl.prec, S))
+            continue;
+          c.push_back(q);
+        }
     rc = pick(c, 0xAu);
   }
   if (rc == OK && pl.ny >= 64 && pl.ny <= 1024) {
@@ -1533,6 +1551,9 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
     for (int o = 0; o < kRadixOrders; o++) {
       NSPlan q = pl;
       q.lineOrd = o;
+      if (q.y_tma && !line_tma_ok(axis_geo(1, pl.nx, pl.ny, pl.nz, pl.prec, pl.lineW, pl.lineT, o),
+                                  pl.prec, q.y_tma))
+        continue;
       c.push_back(q);
     }
     rc = pick(c, 0xAu);

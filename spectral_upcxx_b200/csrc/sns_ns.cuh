@@ -37,6 +37,8 @@ struct NSPlan {
   int lineW;          // adjacent lines per tile of the y/z line passes (0 = default)
   int lineT;          // threads per CTA up to which line groups are added (0 = default)
   int lineOrd;        // radix order of the y line passes (RadixOrder)
+  int y_tma;          // the y line passes over TMA-staged tiles: 0 (direct loads), or
+                      // the number of shared-memory stages (1, 2)
   bool tuned;         // the knobs above were chosen by measurement (ns_tune_plan)
   int pf_waves;       // L2 prefetch of each pass's tile this many waves ahead (0: none)
   int passes;         // timed phases per step: z-inverse, xy, z-forward+update

@@ -200,6 +200,60 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
   }
 }
 
+// One tile of a plain-load line pass (PRO_LOAD) whose input is already in
+// shared memory (`stage`, put there by the TMA as one box of field `blk mod
+// nf`): position p of line (w, g) at (g L + p) W + w for y lines (the box's
+// [z][y][x] order, groups along z) and at (p G + g) W + w for z lines (groups
+// along y).  The arithmetic and the epilogue are line_pass_tile's on the same
+// values, so both give the same bits.  after_reads() is called by every
+// thread once the tile's reads of the stage are issued (the CTA may then
+// refill it).
+template <typename T, int L, typename Fields, int ORD, typename AfterReads>
+__device__ __forceinline__ void line_pass_tile_staged(const LineGeo& geo, const Fields& f, int nf,
+                                                      const cx_t<T>* __restrict__ tw, T sg,
+                                                      T scale, int flags, int wshift, int64_t blk,
+                                                      const cx_t<T>* stage, cx_t<T>* sm,
+                                                      AfterReads after_reads) {
+  using C = cx_t<T>;
+  using P = LinePlan<L>;
+  constexpr int E = P::E, TPL = P::TPL;
+  const int field = (int)(blk % nf);
+  const int64_t t = blk / nf;
+  const int64_t base = (t % geo.TA) * geo.sa + (t / geo.TA) * geo.sb;
+  const int W = geo.W, G = geo.G;
+  const int w = threadIdx.x & (W - 1);
+  const int s = threadIdx.x >> wshift;
+  const int j = s & (TPL - 1);
+  const int g = s / TPL;
+  const int RS = tile_stride(L, W, (int)sizeof(C));
+  C* row = sm + (w + W * g) * RS;
+  const LineCoord lc = line_coord(geo, base, w, g, j, TPL);
+  const bool ylines = geo.axis == 1;
+  const int q0 = ylines ? (g * L + j) * W + w : (j * G + g) * W + w;
+  const int qs = ylines ? TPL * W : TPL * G * W;
+  C v[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) v[e] = stage[q0 + e * qs];
+  after_reads();
+  line_fft<L, true, ORD>(v, row, j, tw, sg);
+
+  C* __restrict__ dst = reinterpret_cast<C*>(f.out(field));
+  const bool do_scale = flags & PASS_SCALE;
+  const bool do_zero = flags & PASS_ZERO_NYQUIST;
+  const bool line_on_plane = (geo.axis != 0 && !geo.kx_half && lc.x == (geo.nx >> 1)) ||
+                             (geo.axis != 1 && lc.y == (geo.ny >> 1)) ||
+                             (geo.axis != 2 && lc.z == (geo.nz >> 1));
+  const int half_axis = geo.axis == 0 ? (geo.nx >> 1) : geo.axis == 1 ? (geo.ny >> 1)
+                                                                      : (geo.nz >> 1);
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    C val = v[e];
+    if (do_scale) val = cscale(scale, val);
+    if (do_zero && (line_on_plane || j + TPL * e == half_axis)) val = mk((T)0, (T)0);
+    dst[lc.idx0 + e * lc.step] = val;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // K1 of the NS step with one tile for all six outputs: z lines of a W x G tile
 // of the three components of V are loaded once (thread layout of

@@ -396,6 +396,34 @@ def test_update_self_prefetch_bit_for_bit(sns, cuda, dtype, monkeypatch):
         assert torch.equal(a, b)
 
 
+@pytest.mark.parametrize("real", [False, True])
+@pytest.mark.parametrize("stages", ["1", "2"])
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (32, 128, 64), (16, 512, 32), (8, 32, 64)])
+def test_y_tma_matches_direct_bit_for_bit(sns, cuda, dtype, shape, stages, real, monkeypatch):
+    """The y line passes (K2, K4) over TMA-staged tiles (SNS_Y_TMA = 1 or 2
+    stages; by default each CTA loads its tile straight from HBM) do the same
+    arithmetic on the same values: three steps are identical bit for bit, for
+    line lengths 32 to 512 (ny = 512: boxes of 256 positions), on complex and
+    half-spectrum (real-field) steppers."""
+    N = sns._native
+    V = _random_fourier(shape, dtype, cuda, 17)
+    out = {}
+    monkeypatch.setenv("SNS_GRAPH", "0")
+    for mode in ("0", stages):
+        monkeypatch.setenv("SNS_Y_TMA", mode)
+        st = sns.NSStepper(shape, 1 / 400, 5e-4, dtype, real=real)
+        assert ("(tma%s) zW" % stages in st.describe()) == (mode != "0"), st.describe()
+        st.bootstrap(V, sns.curl(V))
+        st.step(3)
+        rc = N.lib().sns_ns_check(st.h)
+        assert rc == N.SNS_OK, (mode, rc, N.last_error())
+        out[mode] = [x.clone() for x in st.state()["V1"]] + [x.clone() for x in st.state()["cross0"]]
+        st.close()
+    for a, b in zip(out[stages], out["0"]):
+        assert torch.equal(a, b)
+
+
 def test_carried_k1_pass_times(sns, cuda, monkeypatch):
     """Per-pass timing of a carrying plan: K1 runs in the first step only
     (its later pass times are empty), the update pass carries it."""

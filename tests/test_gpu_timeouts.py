@@ -115,10 +115,10 @@ def test_tma_stage_wait_runs_out_and_recovers(sns, cuda, monkeypatch):
         assert torch.equal(a, b)
 
 
-@pytest.mark.parametrize("env", ["SNS_X_TMA", "SNS_Z_TMA"])
+@pytest.mark.parametrize("env", ["SNS_X_TMA", "SNS_Z_TMA", "SNS_Y_TMA"])
 def test_tma_x_and_update_waits_run_out_and_recover(sns, cuda, monkeypatch, env):
-    """The same stall test on the TMA-staged x pass and update pass (the z
-    pass on its direct-load form, so the timeout is theirs)."""
+    """The same stall test on the TMA-staged x pass, update pass and y passes
+    (the z pass on its direct-load form, so the timeout is theirs)."""
     from spectral_upcxx_b200 import ic
     N = sns._native
     n = 64
@@ -128,7 +128,10 @@ def test_tma_x_and_update_waits_run_out_and_recover(sns, cuda, monkeypatch, env)
     monkeypatch.setenv(env, "1")
     monkeypatch.setenv("SNS_TMA_STALL_TEST", "20000")
     st = sns.NSStepper((n, n, n), 1 / 400, 5e-4, torch.complex64)
-    assert "(tma)" in st.describe() and "(tma1)" not in st.describe()
+    if env == "SNS_Y_TMA":
+        assert "(tma1) zW" in st.describe() and "k1=" in st.describe(), st.describe()
+    else:
+        assert "(tma)" in st.describe() and "(tma1)" not in st.describe()
     st.bootstrap(V, sns.curl(V))
     st.step(1)
     assert N.lib().sns_ns_check(st.h) == N.SNS_ERR_TIMEOUT
@@ -141,3 +144,29 @@ def test_tma_x_and_update_waits_run_out_and_recover(sns, cuda, monkeypatch, env)
     st.step(2)
     assert N.lib().sns_ns_check(st.h) == N.SNS_OK
     st.close()
+
+
+def test_fft_tma_wait_runs_out_and_recovers(sns, cuda, monkeypatch):
+    """The 3D transform's TMA-staged passes (SNS_FFT_TMA=1) with the stall
+    test: the first tile's wait runs out, the CTA records it and ends;
+    sns_fft3d_check reports SNS_ERR_TIMEOUT and clears the record, and a
+    transform afterwards without the stall is correct and checks clean."""
+    from spectral_upcxx_b200 import ic
+    N = sns._native
+    shape = (64, 64, 64)
+    f = ic.uniform_complex(shape, 41)
+    monkeypatch.setenv("SNS_FFT_TMA", "1")
+    monkeypatch.setenv("SNS_TMA_STALL_TEST", "20000")
+    t = torch.from_numpy(f).to(cuda, torch.complex64)
+    sns.forward(t)
+    assert N.lib().sns_fft3d_check(None) == N.SNS_ERR_TIMEOUT
+    assert "gave up" in N.last_error()
+    assert N.lib().sns_fft3d_check(None) == N.SNS_OK  # the record was cleared
+    monkeypatch.delenv("SNS_TMA_STALL_TEST")
+    t = torch.from_numpy(f).to(cuda, torch.complex64)
+    sns.forward(t)
+    assert N.lib().sns_fft3d_check(None) == N.SNS_OK
+    monkeypatch.setenv("SNS_FFT_TMA", "0")
+    r = torch.from_numpy(f).to(cuda, torch.complex64)
+    sns.forward(r)
+    assert torch.equal(t, r)
