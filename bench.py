@@ -64,10 +64,10 @@ STEP_FIELDS = 30  # 9 FFTs x 2 + 12 for the spectral update: 30 N^3 S per step
 
 # DRAM bytes (read + write) per launch of each pass at 256^3 complex64 with the
 # tuned plan, from the one-kernel ncu captures summarised in
-# profiles/ns_step_256_c64_launches.md.
+# profiles/ns_step_256_c64_launches.md (K1 and K2: their TMA-staged forms).
 NCU_TRAFFIC = {
-    ("ns256_fp32", "K1 z-inverse+curl"): (403 + 761) * 1e6,
-    ("ns256_fp32", "K2 y-inverse x6"): (806 + 746) * 1e6,
+    ("ns256_fp32", "K1 z-inverse+curl"): (404 + 773) * 1e6,
+    ("ns256_fp32", "K2 y-inverse x6"): (810 + 749) * 1e6,
     ("ns256_fp32", "K3 x-inv+cross+x-fwd"): (805 + 359) * 1e6,
     ("ns256_fp32", "K4 y-forward x3"): (403 + 341) * 1e6,
     ("ns256_fp32", "K5 z-forward+update"): (1208 + 752) * 1e6,
@@ -715,6 +715,9 @@ def fft_bench(S, torch, dev, stream, n, dtype, esz, args, world, hbm, peak_src, 
         s1.record(stream)
     stream.synchronize()
     e2e_ms = max_over_ranks(s0.elapsed_time(s1))
+    # the tuned plan's TMA-staged passes record any bounded wait that ran out
+    from spectral_upcxx_b200 import _native as NN
+    NN.call("sns_fft3d_check", C.c_void_p(stream.cuda_stream))
     return {"metric": "3D FFT forward+inverse GB/s", "value": gbs, "unit": "GB/s",
             "ms_per_step": ms / args.steps, "dtype": "fp32" if esz == 8 else "fp64",
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -1048,6 +1051,7 @@ def secondary(S, torch, dev, stream, n, hbm):
             e1.record(stream)
         stream.synchronize()
         ms = e0.elapsed_time(e1) / 10
+        S._native.call("sns_fft3d_check", C.c_void_p(stream.cuda_stream))
         out[f"fft{n}_{prec}_fwd_inv_gbs"] = 4 * n ** 3 * esz / (ms / 1e3) / 1e9
         # comparison row only: the same transform pair through cuFFT (torch.fft)
         with torch.cuda.stream(stream):
