@@ -776,7 +776,13 @@ int launch_update(const NSPlan& pl, const UpdateArgs& a, cudaStream_t s) {
   using C = cx_t<T>;
   constexpr int TPL = LinePlan<L>::TPL;
   constexpr int NF = SGS ? 9 : 3;
-  const int threads = NF * a.W * TPL;
+  // a tile wider than the thread limit is z-transformed in two halves
+  int threads = NF * a.W * TPL;
+  if (threads > MaxThreads<T>::value && a.W % 2 == 0) threads /= 2;
+  if (threads > MaxThreads<T>::value) {
+    set_error("update pass: the tile width does not fit the thread limit");
+    return ERR_ARG;
+  }
   const size_t smem = (size_t)NF * a.W * tile_stride(L, a.W, (int)sizeof(C)) * sizeof(C);
   const int blocks = (int)(((int64_t)pl.nx * pl.ny) / a.W);
   static bool attr[64] = {false};
@@ -1061,13 +1067,18 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
     int W = 1;
     int Wmax = prec == PREC_C128 ? 8 : 16;
     if (zW > 0) Wmax = zW;  // a tuned width
-    // tile width override for tuning sweeps (SNS_Z_W, a power of two)
+    // tile width override for tuning sweeps (SNS_Z_W, a power of two; a
+    // width beyond the thread limit is transformed in two halves, with one
+    // CTA per SM)
+    bool wide = false;
     if (const char* e = zW > 0 ? nullptr : getenv("SNS_Z_W")) {
       const int v = atoi(e);
       if (v >= 1 && (v & (v - 1)) == 0) Wmax = v;
+      wide = true;
     }
-    while (W * 2 <= Wmax && nx % (W * 2) == 0 && 3 * (W * 2) * TPL <= max_threads(prec) &&
-           (size_t)3 * W * 2 * tile_stride(nz, W * 2, (int)esz) * esz <= 110 * 1024)
+    while (W * 2 <= Wmax && nx % (W * 2) == 0 &&
+           3 * (W * 2) * TPL <= (wide ? 2 : 1) * max_threads(prec) &&
+           (size_t)3 * W * 2 * tile_stride(nz, W * 2, (int)esz) * esz <= (wide ? 220 : 110) * 1024)
       W *= 2;
     pl.zW = W;
     pl.update_blocks = (nx / W) * ny;
@@ -1401,10 +1412,12 @@ bool xg_ok(const NSPlan& p, int G) {
   return ((int64_t)p.ny * p.nz) % G == 0 && 6 * G * TPL <= cap &&
          (size_t)6 * G * xrow_stride(p.nx, (int)esz) * esz <= kTuneSmemCap;
 }
-bool zw_ok(const NSPlan& p, int W, int max_blocks) {
+bool zw_ok(const NSPlan& p, int W, int max_blocks, bool halves = false) {
   const int TPL = p.nz / elems(p.nz);
   const size_t esz = p.prec == PREC_C128 ? 16 : 8;
-  return p.nx % W == 0 && 3 * W * TPL <= max_threads(p.prec) &&
+  // halves: the plain update pass may transform a tile in two halves of W/2
+  const int thr = 3 * W * TPL / (halves && 3 * W * TPL > max_threads(p.prec) ? 2 : 1);
+  return p.nx % W == 0 && thr <= max_threads(p.prec) &&
          (size_t)3 * W * tile_stride(p.nz, W, (int)esz) * esz <= kTuneSmemCap &&
          ((int64_t)p.nx * p.ny) / W <= max_blocks;
 }
@@ -1580,8 +1593,8 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
   // K5: adjacent z lines per CTA of the update pass
   if (rc == OK) {
     c.clear();
-    for (int W : {2, 4, 8, 16, 32}) {
-      if (zw_ok(pl, W, max_blocks))
+    for (int W : {2, 4, 8, 16, 32, 64}) {
+      if (zw_ok(pl, W, max_blocks, true))
         for (int pfs = 0; pfs < 2; pfs++) {
           NSPlan q = pl;
           q.zW = W;

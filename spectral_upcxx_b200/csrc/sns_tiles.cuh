@@ -632,16 +632,24 @@ __device__ __forceinline__ void zfwd_update_tile_from(const UpdateArgs& a,
 
   // thread t owns z line (field, base + w) at positions j + e*TPL with
   // w = t mod W, j = (t / W) mod TPL, field = t / (W*TPL): consecutive threads
-  // load adjacent x, so the direct loads are coalesced
+  // load adjacent x, so the direct loads are coalesced.  A CTA of half the
+  // threads (nthr = NF W TPL / 2, W even) transforms the tile in two halves of
+  // W/2 adjacent lines, one after the other: a wide tile (W = 32) keeps the
+  // update's rows of 32 adjacent x within the thread limit.
   {
-    const int w = threadIdx.x % W, s = threadIdx.x / W;
-    const int j = s % TPL, fld = s / TPL;
-    C* row = sm + (fld * W + w) * RS;
-    C v[E];
-    load(fld, w, j, v);
-    line_fft<L, true>(v, row, j, tw, (T)-1);
+    constexpr int NF = SGS ? 9 : 3;
+    const int WH = NF * W * TPL > nthr ? W / 2 : W;  // lines along x per half
+#pragma unroll 1
+    for (int w0 = 0; w0 < W; w0 += WH) {
+      const int w = w0 + threadIdx.x % WH, s = threadIdx.x / WH;
+      const int j = s % TPL, fld = s / TPL;
+      C* row = sm + (fld * W + w) * RS;
+      C v[E];
+      load(fld, w, j, v);
+      line_fft<L, true>(v, row, j, tw, (T)-1);
 #pragma unroll
-    for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
+      for (int e = 0; e < E; e++) row[pad_pos(j + TPL * e)] = v[e];
+    }
   }
   __syncthreads();
 

@@ -424,6 +424,37 @@ def test_y_tma_matches_direct_bit_for_bit(sns, cuda, dtype, shape, stages, real,
         assert torch.equal(a, b)
 
 
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+@pytest.mark.parametrize("shape", [(256, 16, 64), (64, 64, 64), (32, 16, 128)])
+def test_update_wide_tile_halves_bit_for_bit(sns, cuda, dtype, shape, monkeypatch):
+    """An update-pass tile wider than the thread limit (SNS_Z_W=32 at nz = 256
+    in complex64, 16 in complex128) is z-transformed in two halves of
+    adjacent lines by half the threads: the same values as narrower tiles,
+    three steps identical bit for bit (diagnostics to 1e-12: the per-tile
+    partials are summed in another order)."""
+    N = sns._native
+    V = _random_fourier(shape, dtype, cuda, 18)
+    out, stats = {}, {}
+    monkeypatch.setenv("SNS_GRAPH", "0")
+    wide = "32" if dtype == torch.complex64 else "16"
+    for mode in ("4", wide):
+        monkeypatch.setenv("SNS_Z_W", mode)
+        st = sns.NSStepper(shape, 1 / 400, 5e-4, dtype)
+        st.bootstrap(V, sns.curl(V))
+        st.step(3)
+        rc = N.lib().sns_ns_check(st.h)
+        assert rc == N.SNS_OK, (mode, rc, N.last_error())
+        out[mode] = [x.clone() for x in st.state()["V1"]] + [x.clone() for x in st.state()["cross0"]]
+        stats[mode] = st.stats()
+        desc = st.describe()
+        st.close()
+    assert "zW=%s" % min(int(wide), shape[2]) in desc, desc
+    for a, b in zip(out[wide], out["4"]):
+        assert torch.equal(a, b)
+    for k in stats["4"]:
+        assert abs(stats[wide][k] - stats["4"][k]) <= 1e-12 * abs(stats["4"][k])
+
+
 def test_carried_k1_pass_times(sns, cuda, monkeypatch):
     """Per-pass timing of a carrying plan: K1 runs in the first step only
     (its later pass times are empty), the update pass carries it."""
