@@ -1113,7 +1113,9 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
           pl.zW = w;
           pl.update_blocks = (nx / w) * ny;
         }
-    // L2 prefetch of each tile's V and C0 before its z-forward (SNS_Z_PFSELF=1)
+    // L2 prefetch of each tile's V and C0 once its cross product's loads are
+    // in flight (SNS_Z_PFSELF=1; asked before those loads it delayed them and
+    // measured slower)
     const char* epf = getenv("SNS_Z_PFSELF");
     pl.z_pfself = epf && epf[0] == '1';
     // closure update: nine fields in the tile

@@ -16,8 +16,8 @@ struct NSPlan {
                       // the new V and its curl into U), so the next step skips K1
   bool carry_reload;  // ... reading the new V back from V (L1/L2) instead of keeping
                       // it in a second set of shared-memory rows
-  bool z_pfself;      // the update pass asks L2 for each tile's V and C0 before its
-                      // z-forward
+  bool z_pfself;      // the update pass asks L2 for each tile's V and C0 once the
+                      // cross product's loads are in flight
   int k1W, k1G;       // K1 tile: adjacent z lines x groups (all six outputs per CTA)
   bool k1_fused;      // K1 loads V once per tile (else one output field per CTA)
   bool k1_reload;     // the fused K1 forms omega from reloads of V (L1), not shared memory

@@ -811,17 +811,6 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
   const int W = a.W;
   const int64_t nxy = (int64_t)a.nx * a.ny;
   const int64_t base = blk * W;
-  if (!SGS && a.pf_self) {
-    // this tile's V and C0 into L2, so that the update's loads after the
-    // z-forward find them there
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      prefetch_lines<L>(reinterpret_cast<const char*>(a.V[d]), base, W, 1, 0, nxy, (int)sizeof(C),
-                        nthr);
-      prefetch_lines<L>(reinterpret_cast<const char*>(a.C0[d]), base, W, 1, 0, nxy,
-                        (int)sizeof(C), nthr);
-    }
-  }
   if (!SGS && a.pf > 0 && (blk + a.pf) * W < nxy) {
     // tile blk + pf's cross product, V and C0 into L2
     const int64_t bp = (blk + a.pf) * W;
@@ -841,6 +830,17 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
     const int64_t i0 = base + w + nxy * j;
 #pragma unroll
     for (int e = 0; e < E; e++) v[e] = src[i0 + nxy * (TPL * e)];
+    if (!SGS && a.pf_self) {
+      // with the cross product's loads in flight, ask L2 for this tile's V
+      // and C0, so that the update's loads after the z-forward find them there
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        prefetch_lines<L>(reinterpret_cast<const char*>(a.V[d]), base, W, 1, 0, nxy,
+                          (int)sizeof(C), nthr);
+        prefetch_lines<L>(reinterpret_cast<const char*>(a.C0[d]), base, W, 1, 0, nxy,
+                          (int)sizeof(C), nthr);
+      }
+    }
   });
 }
 

@@ -379,8 +379,9 @@ def test_carried_k1_matches_separate_bit_for_bit(sns, cuda, dtype, shape, real, 
 
 @pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
 def test_update_self_prefetch_bit_for_bit(sns, cuda, dtype, monkeypatch):
-    """Asking L2 for a tile's V and C0 before the update pass's z-forward
-    (SNS_Z_PFSELF=1) is a hint only: three steps are identical bit for bit."""
+    """Asking L2 for a tile's V and C0 while the update pass's cross-product
+    loads are in flight (SNS_Z_PFSELF=1) is a hint only: three steps are
+    identical bit for bit."""
     shape = (64, 32, 128)
     V = _random_fourier(shape, dtype, cuda, 16)
     out = {}
