@@ -119,6 +119,8 @@ __device__ __forceinline__ void ens_item(const EnsClass* __restrict__ k,
       a.kc2 = 1e300;
       a.kx_half = 0;
       a.pf = 0;
+      a.pf_self = 0;
+      for (int i = 0; i < 6; i++) a.Uo[i] = nullptr;
     }
     __syncthreads();
     zfwd_update_tile<T, L>(a, tw, blk, (int)blockDim.x, sm, red);

@@ -127,15 +127,6 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
   const int64_t t = blk / nf;
   const int64_t base = (t % geo.TA) * geo.sa + (t / geo.TA) * geo.sb;
   const int W = geo.W;
-  if constexpr (PRO == PRO_LOAD || PRO == PRO_IKAXIS) {
-    const int64_t bp = blk + geo.pf;
-    if (geo.pf > 0 && bp < geo.TA * geo.TB * nf) {
-      const int64_t tp = bp / nf;
-      prefetch_lines<L>(reinterpret_cast<const char*>(f.in((int)(bp % nf))),
-                        (tp % geo.TA) * geo.sa + (tp / geo.TA) * geo.sb, W, geo.G, geo.gs,
-                        geo.ps, (int)sizeof(C), (int)blockDim.x);
-    }
-  }
   const int w = threadIdx.x & (W - 1);
   const int s = threadIdx.x >> wshift;
   const int j = s & (TPL - 1);
@@ -179,6 +170,16 @@ __device__ __forceinline__ void line_pass_tile(const LineGeo& geo, const Fields&
                                 geo.axis == 0 ? kp : kx0, geo.axis == 1 ? kp : ky0,
                                 geo.axis == 2 ? kp : kz0);
       }
+    }
+  }
+  if constexpr (PRO == PRO_LOAD || PRO == PRO_IKAXIS) {
+    // with this tile's loads in flight, the tile pf launches ahead into L2
+    const int64_t bp = blk + geo.pf;
+    if (geo.pf > 0 && bp < geo.TA * geo.TB * nf) {
+      const int64_t tp = bp / nf;
+      prefetch_lines<L>(reinterpret_cast<const char*>(f.in((int)(bp % nf))),
+                        (tp % geo.TA) * geo.sa + (tp / geo.TA) * geo.sb, W, geo.G, geo.gs,
+                        geo.ps, (int)sizeof(C), (int)blockDim.x);
     }
   }
   line_fft<L, true, ORD>(v, row, j, tw, sg);
@@ -545,18 +546,19 @@ __device__ __forceinline__ void xcross_tile(const Fields& f, const cx_t<T>* __re
                                             int64_t pf = 0, int64_t nblk = 0) {
   using C = cx_t<T>;
   constexpr int E = LinePlan<L>::E, TPL = LinePlan<L>::TPL;
-  if (pf > 0 && blk + pf < nblk) {
-    // the six input rows of tile blk + pf into L2
-#pragma unroll
-    for (int fl = 0; fl < 6; fl++)
-      prefetch_lines<L>(reinterpret_cast<const char*>(f.in(fl)), (blk + pf) * G * L, 1, G, L, 1,
-                        (int)sizeof(C), nthr);
-  }
   xcross_tile_from<T, L>(f, tw, G, scale2, blk, nthr, sm, [&](int fld, int gl, int j, C (&v)[E]) {
     const C* __restrict__ src = reinterpret_cast<const C*>(f.in(fld));
     const int64_t i0 = (blk * G + gl) * L + j;
 #pragma unroll
     for (int e = 0; e < E; e++) v[e] = src[i0 + TPL * e];
+    if (pf > 0 && blk + pf < nblk) {
+      // with this tile's loads in flight, the six input rows of tile blk + pf
+      // into L2
+#pragma unroll
+      for (int fl = 0; fl < 6; fl++)
+        prefetch_lines<L>(reinterpret_cast<const char*>(f.in(fl)), (blk + pf) * G * L, 1, G, L, 1,
+                          (int)sizeof(C), nthr);
+    }
   });
 }
 
@@ -811,19 +813,6 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
   const int W = a.W;
   const int64_t nxy = (int64_t)a.nx * a.ny;
   const int64_t base = blk * W;
-  if (!SGS && a.pf > 0 && (blk + a.pf) * W < nxy) {
-    // tile blk + pf's cross product, V and C0 into L2
-    const int64_t bp = (blk + a.pf) * W;
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      prefetch_lines<L>(reinterpret_cast<const char*>(a.U[d]), bp, W, 1, 0, nxy, (int)sizeof(C),
-                        nthr);
-      prefetch_lines<L>(reinterpret_cast<const char*>(a.V[d]), bp, W, 1, 0, nxy, (int)sizeof(C),
-                        nthr);
-      prefetch_lines<L>(reinterpret_cast<const char*>(a.C0[d]), bp, W, 1, 0, nxy, (int)sizeof(C),
-                        nthr);
-    }
-  }
   zfwd_update_tile_from<T, L, SGS, KEEP>(a, tw, blk, nthr, sm, red, [&](int fld, int w, int j, C (&v)[E]) {
     const C* __restrict__ src = reinterpret_cast<const C*>(
         SGS ? update_field(a, fld) : (fld == 0 ? a.U[0] : fld == 1 ? a.U[1] : a.U[2]));
@@ -838,6 +827,19 @@ __device__ __forceinline__ void zfwd_update_tile(const UpdateArgs& a,
         prefetch_lines<L>(reinterpret_cast<const char*>(a.V[d]), base, W, 1, 0, nxy,
                           (int)sizeof(C), nthr);
         prefetch_lines<L>(reinterpret_cast<const char*>(a.C0[d]), base, W, 1, 0, nxy,
+                          (int)sizeof(C), nthr);
+      }
+    }
+    if (!SGS && a.pf > 0 && (blk + a.pf) * W < nxy) {
+      // and tile blk + pf's cross product, V and C0
+      const int64_t bp = (blk + a.pf) * W;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        prefetch_lines<L>(reinterpret_cast<const char*>(a.U[d]), bp, W, 1, 0, nxy,
+                          (int)sizeof(C), nthr);
+        prefetch_lines<L>(reinterpret_cast<const char*>(a.V[d]), bp, W, 1, 0, nxy,
+                          (int)sizeof(C), nthr);
+        prefetch_lines<L>(reinterpret_cast<const char*>(a.C0[d]), bp, W, 1, 0, nxy,
                           (int)sizeof(C), nthr);
       }
     }

@@ -456,6 +456,30 @@ def test_update_wide_tile_halves_bit_for_bit(sns, cuda, dtype, shape, monkeypatc
         assert abs(stats[wide][k] - stats["4"][k]) <= 1e-12 * abs(stats["4"][k])
 
 
+@pytest.mark.parametrize("waves", ["1", "2"])
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+def test_next_wave_prefetch_bit_for_bit(sns, cuda, dtype, waves, monkeypatch):
+    """Asking L2 for the tiles one or two waves of resident CTAs ahead
+    (SNS_PF, issued once each tile's own loads are in flight; the direct-load
+    K1, y passes, x pass and update pass) is a hint only: three steps are
+    identical bit for bit to the run without it."""
+    shape = (64, 64, 128)
+    V = _random_fourier(shape, dtype, cuda, 19)
+    out = {}
+    monkeypatch.setenv("SNS_K1_TMA", "0")
+    monkeypatch.setenv("SNS_K1_RELOAD", "1")
+    for mode in ("0", waves):
+        monkeypatch.setenv("SNS_PF", mode)
+        st = sns.NSStepper(shape, 1 / 400, 5e-4, dtype)
+        assert ("pf=%s" % mode) in st.describe(), st.describe()
+        st.bootstrap(V, sns.curl(V))
+        st.step(3)
+        out[mode] = [x.clone() for x in st.state()["V1"]] + [x.clone() for x in st.state()["cross0"]]
+        st.close()
+    for a, b in zip(out[waves], out["0"]):
+        assert torch.equal(a, b)
+
+
 def test_carried_k1_pass_times(sns, cuda, monkeypatch):
     """Per-pass timing of a carrying plan: K1 runs in the first step only
     (its later pass times are empty), the update pass carries it."""
