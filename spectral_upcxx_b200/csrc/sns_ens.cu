@@ -56,6 +56,8 @@ struct EnsClass {
   int nf;         // fields of a line stage
   double scale2;  // 1/N^2 of the cross product
   const void* tw;
+  int pf_self;    // update stage: ask L2 for a tile's V and C0 once its cross
+                  // product's loads are in flight
 };
 
 // Kernel parameter of one stage launch.
@@ -119,7 +121,7 @@ __device__ __forceinline__ void ens_item(const EnsClass* __restrict__ k,
       a.kc2 = 1e300;
       a.kx_half = 0;
       a.pf = 0;
-      a.pf_self = 0;
+      a.pf_self = k->pf_self;
       for (int i = 0; i < 6; i++) a.Uo[i] = nullptr;
     }
     __syncthreads();
@@ -351,6 +353,11 @@ bool make_class(const sns_ens* e, int s, int c, const StageCfg& cfg, EnsClass& k
     k.L = nz;
     k.W = W;
     k.tiles = cols / W;
+    // the update stage's L2 prefetch of V and C0 (SNS_ENS_PFSELF=0: off).
+    // Measured on B200 for 32 x 32^3 + 24 x 64^3 + 8 x 128^3 boxes: update
+    // stage 0.646 against 0.675 ms
+    const char* pe = getenv("SNS_ENS_PFSELF");
+    k.pf_self = pe ? (pe[0] == '1') : 1;
     smem = (size_t)3 * W * tile_stride(nz, W, (int)esz) * esz;
   }
   k.tw = twiddles(k.L, e->prec);
