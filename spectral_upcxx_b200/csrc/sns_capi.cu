@@ -1090,7 +1090,7 @@ int sns_ns_describe(sns_ns* h, char* buf, int len) {
                          : p.k1_reload ? "(reload)" : "",
                          p.lineW, p.lineT,
                          ord[p.lineOrd % 3],
-                         p.y_tma == 1 ? "(tma1)" : p.y_tma == 2 ? "(tma2)" : "", p.zW, p.z_tma ? "(tma)" : p.carry ? (p.carry_reload ? "(+K1r)" : "(+K1)") : p.z_pfself ? "(pfs)" : "", p.xG, p.x_tma ? "(tma)" : "", p.pf_waves, p.real ? " real" : "",
+                         p.y_tma == 1 ? "(tma1)" : p.y_tma == 2 ? "(tma2)" : "", p.zW, p.z_tma ? "(tma)" : p.carry ? (p.carry_reload ? "(+K1r)" : "(+K1)") : p.z_pfself ? "(pfs)" : "", p.xG, p.x_tma ? "(tma)" : p.x_occ ? "(occ)" : "", p.pf_waves, p.real ? " real" : "",
                          p.tuned ? " tuned" : "");
   if (buf && len > 0) {
     strncpy(buf, tmp, (size_t)len - 1);

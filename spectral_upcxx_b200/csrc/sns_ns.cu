@@ -44,6 +44,19 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
                     reinterpret_cast<cx_t<T>*>(smem_raw), pf, (int64_t)gridDim.x);
 }
 
+// K3 for CTAs of at most 192 threads, compiled for five resident CTAs per SM
+// (64 registers per thread instead of 80): more warps to hide the row loads'
+// latency, at the price of a few spilled registers.
+template <typename T, int L>
+__global__ void __launch_bounds__(192, 5)
+    k_xcross_occ(FieldPtrs f, const cx_t<T>* __restrict__ tw, int G, T scale2, int64_t pf) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_trigger();
+  pdl_wait();
+  xcross_tile<T, L>(ParamFields{f}, tw, G, scale2, (int64_t)blockIdx.x, (int)blockDim.x,
+                    reinterpret_cast<cx_t<T>*>(smem_raw), pf, (int64_t)gridDim.x);
+}
+
 // K3 with TMA-staged tiles: a persistent CTA walks the tiles blockIdx.x,
 // + gridDim.x, ...; the G rows of each of the six fields of its next tile (G L
 // contiguous elements per field) come into a shared-memory stage as six bulk
@@ -499,6 +512,23 @@ int launch_xcross(const NSPlan& pl, const FieldPtrs& f, int64_t rows, cudaStream
   const int G = pl.xG;
   const int threads = 6 * G * TPL;
   const size_t smem = (size_t)6 * G * xrow_stride(L, (int)sizeof(C)) * sizeof(C);
+  if (pl.x_occ && threads <= 192) {
+    static bool attr_o[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!attr_o[dev & 63]) {
+      cudaError_t e = allow_max_dynamic_smem(k_xcross_occ<T, L>);
+      if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_xcross_occ)");
+      attr_o[dev & 63] = true;
+    }
+    const C* tw = reinterpret_cast<const C*>(twiddles(L, sizeof(T) == 8 ? PREC_C128 : PREC_C64));
+    const double N = (double)pl.nx * pl.ny * pl.nz;
+    const int64_t pf = tiles_in_waves(k_xcross_occ<T, L>, threads, smem, pl.pf_waves);
+    cudaError_t e = launch_pdl(k_xcross_occ<T, L>, dim3((unsigned)(rows / G)), dim3(threads), smem,
+                               s, f, tw, G, (T)(1.0 / (N * N)), pf);
+    if (e != cudaSuccess) return cuda_status(e, "k_xcross_occ");
+    return OK;
+  }
   static bool attr[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -1022,6 +1052,9 @@ int ns_plan(NSPlan& pl, int nx, int ny, int nz, int prec, int zW, int lineW, boo
     // complex128 0.700 against 0.756 (G = 4) and 0.599 (G = 1, direct): the
     // rows are contiguous, so direct loads already stream, and the stage
     // halves the CTAs an SM holds.  The tuner still tries it.
+    // the five-CTA form of the direct-load pass on request (SNS_X_OCC=1)
+    const char* eo = getenv("SNS_X_OCC");
+    pl.x_occ = eo && eo[0] == '1';
     const char* e = getenv("SNS_X_TMA");
     pl.x_tma = false;
     if (e && e[0] == '1')
@@ -1479,7 +1512,8 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
                 "ns_tune passes=0x%x cand=%zu ms=%.4f k1=%dx%d%s%s xG=%d%s zW=%d%s%s lineW=%d "
                 "lineT=%d ord=%d ytma=%d pf=%d\n",
                 passes, i, t, cands[i].k1W, cands[i].k1G, cands[i].k1_tma ? "(tma)" : "",
-                cands[i].k1_reload ? "(reload)" : "", cands[i].xG, cands[i].x_tma ? "(tma)" : "",
+                cands[i].k1_reload ? "(reload)" : "", cands[i].xG,
+                cands[i].x_tma ? "(tma)" : cands[i].x_occ ? "(occ)" : "",
                 cands[i].zW, cands[i].z_tma ? "(tma)" : cands[i].z_pfself ? "(pfs)" : "",
                 cands[i].carry ? (cands[i].carry_reload ? "(+K1r)" : "(+K1)") : "",
                 cands[i].lineW, cands[i].lineT, cands[i].lineOrd, cands[i].y_tma,
@@ -1581,11 +1615,18 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
         NSPlan q = pl;
         q.xG = G;
         q.x_tma = false;
+        q.x_occ = false;
         c.push_back(q);
+        // the five-CTA form, for CTAs of at most 192 threads (complex64)
+        if (!pl.real && pl.prec == PREC_C64 && 6 * G * (pl.nx / elems(pl.nx)) <= 192) {
+          q.x_occ = true;
+          c.push_back(q);
+        }
       }
       if (sync_words && x_tma_ok(pl, G)) {
         NSPlan q = pl;
         q.xG = G;
+        q.x_occ = false;
         q.x_tma = true;
         c.push_back(q);
       }

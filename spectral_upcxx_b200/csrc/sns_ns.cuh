@@ -11,6 +11,7 @@ struct NSPlan {
   int nx, ny, nz, prec;
   int xG;             // rows per CTA of the x cross pass
   bool x_tma;         // the x cross pass as a persistent pass over TMA-staged rows
+  bool x_occ;         // its direct-load form compiled for five CTAs of <= 192 threads per SM
   bool z_tma;         // the update pass as a persistent pass over TMA-staged z lines
   bool carry;         // the update pass also does the next step's K1 (z-inverse of
                       // the new V and its curl into U), so the next step skips K1

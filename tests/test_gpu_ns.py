@@ -480,6 +480,27 @@ def test_next_wave_prefetch_bit_for_bit(sns, cuda, dtype, waves, monkeypatch):
         assert torch.equal(a, b)
 
 
+@pytest.mark.parametrize("dtype", [torch.complex128, torch.complex64])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (16, 32, 256), (32, 16, 128)])
+def test_x_occ_matches_direct_bit_for_bit(sns, cuda, dtype, shape, monkeypatch):
+    """The x cross pass compiled for five CTAs of at most 192 threads per SM
+    (SNS_X_OCC=1; used where its tile has at most 192 threads) does the same
+    arithmetic: three steps are identical bit for bit."""
+    V = _random_fourier(shape, dtype, cuda, 20)
+    out = {}
+    monkeypatch.setenv("SNS_GRAPH", "0")
+    for mode in ("0", "1"):
+        monkeypatch.setenv("SNS_X_OCC", mode)
+        st = sns.NSStepper(shape, 1 / 400, 5e-4, dtype)
+        assert ("(occ)" in st.describe()) == (mode == "1"), st.describe()
+        st.bootstrap(V, sns.curl(V))
+        st.step(3)
+        out[mode] = [x.clone() for x in st.state()["V1"]] + [x.clone() for x in st.state()["cross0"]]
+        st.close()
+    for a, b in zip(out["1"], out["0"]):
+        assert torch.equal(a, b)
+
+
 def test_carried_k1_pass_times(sns, cuda, monkeypatch):
     """Per-pass timing of a carrying plan: K1 runs in the first step only
     (its later pass times are empty), the update pass carries it."""
