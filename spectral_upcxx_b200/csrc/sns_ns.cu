@@ -1500,8 +1500,11 @@ int ns_tune_plan(NSPlan& pl, void* const V[3], void* const C0[3], void* const U[
   };
   // SNS_TUNE_LOG=1 prints every candidate's time to stderr
   const bool log = getenv("SNS_TUNE_LOG") && getenv("SNS_TUNE_LOG")[0] == '1';
-  auto pick = [&](std::vector<NSPlan>& cands, unsigned passes) -> int {
-    float best = 3.4e38f;
+  // margin > 0: cands[0] is the incumbent plan, and another candidate
+  // replaces it only when faster by that fraction (whole-step timings of a few
+  // steps vary by 1-2 % between runs)
+  auto pick = [&](std::vector<NSPlan>& cands, unsigned passes, float margin = 0.f) -> int {
+    float best = 3.4e38f, t0 = 3.4e38f;
     int bi = -1;
     for (size_t i = 0; i < cands.size(); i++) {
       float t = 0;
