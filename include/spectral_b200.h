@@ -80,7 +80,7 @@ int sns_fft3d_many(void* const* fields, int nfields, int64_t nx, int64_t ny, int
  * nx*ny*nz by measurement (the counterpart of the reference's FFTW_MEASURE
  * planning, src/FFT1D.cpp:18-22): per axis the tile width, thread count and
  * radix order (radix-16 stages with the remainder last or first, or radix-8
- * stages), for y and z lines the TMA-staged form of the pass (one or two
+ * stages), for each axis the TMA-staged form of the pass (one or two
  * shared-memory stages per persistent CTA), and for 128 x 128 planes the
  * plane pass against two line passes.
  * Runs on scratch fields from the pool; the choice is cached per device and

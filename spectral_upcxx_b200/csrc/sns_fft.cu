@@ -322,14 +322,14 @@ int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int fla
                  : axis_geo(axis, nx, ny, nz, prec);
   };
   // a pass of the plan: the TMA-staged form where the tuned plan chose it
-  // (SNS_FFT_TMA = 1 or 2 stages asks for it on the y and z passes of an
-  // untuned plan)
+  // (SNS_FFT_TMA = 1 or 2 stages asks for it on the passes of an untuned
+  // plan)
   int forced = 0;
   if (const char* e = getenv("SNS_FFT_TMA")) forced = atoi(e);
   if (forced != 1 && forced != 2) forced = 0;
   int* err_word = (tuned || forced) && !tw_axes ? fft_tma_err_word() : nullptr;
   auto pass = [&](int axis, const LineGeo& g, int sg, int fl) {
-    const int S = tuned ? tc.tma[axis] : (axis > 0 ? forced : 0);
+    const int S = tuned ? tc.tma[axis] : forced;
     if (S && err_word && nf <= 6 && line_tma_ok(g, prec, S))
       return run_line_pass_tma(g, f, sg, fl, 1.0 / N, prec, stream, S, err_word);
     return run_line_pass(g, f, sg, fl, 1.0 / N, prec, stream);
@@ -456,7 +456,7 @@ int fft3d_tune(int nx, int ny, int nz, int nf, int prec, cudaStream_t stream) {
   // the pass of axis a under a candidate plan (its TMA-staged form if chosen)
   int* err_word = fft_tma_err_word();
   auto tma_fits = [&](const FftChoice& q, int a, int S) {
-    return S == 0 || (a > 0 && err_word && nf <= 6 &&
+    return S == 0 || (err_word && nf <= 6 &&
                       line_tma_ok(axis_geo(a, nx, ny, nz, prec, q.wmax[a], q.tmax[a], q.ord[a]),
                                   prec, S));
   };

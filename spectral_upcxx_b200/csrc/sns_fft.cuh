@@ -116,7 +116,8 @@ bool line_supported(int64_t L);
 int run_line_pass(const LineGeo& geo, const FieldPtrs& f, int sign, int flags, double scale,
                   int prec, cudaStream_t stream, int prologue = PRO_LOAD);
 
-// The same pass (plain loads only, y or z lines, 1..6 fields, L = 32..512)
+// The same pass (plain loads only, x, y or z lines, 1..6 fields, L = 32..512;
+// x lines of at most 256 8-byte units)
 // as a persistent pass over TMA-staged tiles with `stages` (1 or 2) shared
 // memory stages (sns_line_tma.cu); its bounded waits record into *err
 // (1: a wait ran out, 2: a box failed the kernel's own check).  Same results
@@ -151,7 +152,7 @@ int fft3d(void* const* fields, int nf, int nx, int ny, int nz, int sign, int fla
 // and whether the xy plane pass is used where it is available.
 struct FftChoice {
   int wmax[3], tmax[3], ord[3];
-  int tma[3];  // stages of the TMA-staged form of the y and z passes (0: direct loads)
+  int tma[3];  // stages of the TMA-staged form of each axis's pass (0: direct loads)
   bool plane;
 };
 // Error word of the transform's TMA-staged passes on the current device

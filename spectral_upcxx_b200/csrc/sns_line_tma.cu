@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int W = geo.W, G = geo.G, lines = W * G;
   const int per = lines * L;
-  const bool ylines = geo.axis == 1;
+  const bool ylines = geo.axis == 1, xlines = geo.axis == 0;
   const uint32_t raw = tc::smem_u32(smem_raw);
   C* stage0 = reinterpret_cast<C*>(smem_raw + (((raw + 127u) & ~127u) - raw));
   C* rows = stage0 + S * per;
@@ -78,9 +78,22 @@ __global__ void __launch_bounds__(MaxThreads<T>::value)
     const int64_t t = blk / nf;
     const CUtensorMap* m = pick_map(fld, m0, m1, m2, m3, m4, m5);
     const int u = (int)(sizeof(C) / 8);
+    C* st = stage0 + k * per;
+    if (xlines) {
+      // G whole rows of one xy plane: one (nx, G, 1) box at row r0 = t G
+      const int64_t r0 = t * G;
+      const int y0 = (int)(r0 % geo.ny), z0 = (int)(r0 / geo.ny);
+      if (y0 + G > geo.ny || z0 >= geo.nz || (tc::smem_u32(st) & 127u)) {
+        atomicExch(err, 2);
+        tma::arrive(&full[k]);
+        return;
+      }
+      tma::expect_tx(&full[k], (uint32_t)(per * sizeof(C)));
+      tma::load_3d(st, m, 0, y0, z0, &full[k]);
+      return;
+    }
     const int x0 = (int)((t % geo.TA) * W) * u;
     const int g0 = (int)((t / geo.TA) * G);
-    C* st = stage0 + k * per;
     // self-check of the box (16-byte aligned x, inside the field, 128-byte
     // aligned destination): a bad one is recorded and not loaded, and the
     // stage's barrier is released without it
@@ -166,10 +179,13 @@ int launch_line_tma(const LineGeo& geo, const FieldPtrs& f, int sign, int flags,
   const size_t smem = line_tma_smem(L, geo.W, geo.G, S, sizeof(C));
   CUtensorMap m[kMaxTmaFields];
   for (int i = 0; i < f.n; i++) {
-    const int rc = ylines ? field_tensor_map(&m[i], f.in[i], geo.nx, geo.ny, geo.nz, esz, geo.W,
-                                             LB, geo.G)
-                          : field_tensor_map(&m[i], f.in[i], geo.nx, geo.ny, geo.nz, esz, geo.W,
-                                             geo.G, LB);
+    const int rc = geo.axis == 0
+                       ? field_tensor_map(&m[i], f.in[i], geo.nx, geo.ny, geo.nz, esz, geo.nx,
+                                          geo.G, 1)
+                   : ylines ? field_tensor_map(&m[i], f.in[i], geo.nx, geo.ny, geo.nz, esz,
+                                               geo.W, LB, geo.G)
+                            : field_tensor_map(&m[i], f.in[i], geo.nx, geo.ny, geo.nz, esz,
+                                               geo.W, geo.G, LB);
     if (rc) return rc;
   }
   for (int i = f.n; i < kMaxTmaFields; i++) m[i] = m[0];
@@ -221,7 +237,7 @@ int dispatch_line_tma(const LineGeo& geo, const FieldPtrs& f, int sign, int flag
 
 bool line_tma_ok(const LineGeo& geo, int prec, int stages) {
   const int L = geo.L;
-  if (geo.axis != 1 && geo.axis != 2) return false;
+  if (geo.axis != 0 && geo.axis != 1 && geo.axis != 2) return false;
   if (L != 32 && L != 64 && L != 128 && L != 256 && L != 512) return false;
   if (geo.ord != RADIX16_FIRST && geo.ord != RADIX_REM_FIRST) return false;
   if (stages != 1 && stages != 2) return false;
@@ -234,6 +250,10 @@ bool line_tma_ok(const LineGeo& geo, int prec, int stages) {
   const int TPL = L / 16;
   if (geo.W * geo.G * TPL > max_threads(prec)) return false;
   if (line_tma_smem(L, geo.W, geo.G, stages, esz) > 220 * 1024) return false;
+  // x lines: G whole rows of one plane per box, at most 256 units (8 bytes) long
+  if (geo.axis == 0)
+    return geo.W == 1 && geo.ny % geo.G == 0 && field_box_ok(geo.nx, geo.ny, geo.nz, esz, geo.nx,
+                                                              geo.G, 1);
   return ylines ? field_box_ok(geo.nx, geo.ny, geo.nz, esz, geo.W, LB, geo.G)
                 : field_box_ok(geo.nx, geo.ny, geo.nz, esz, geo.W, geo.G, LB);
 }

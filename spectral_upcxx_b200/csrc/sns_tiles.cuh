@@ -229,7 +229,8 @@ __device__ __forceinline__ void line_pass_tile_staged(const LineGeo& geo, const 
   const int RS = tile_stride(L, W, (int)sizeof(C));
   C* row = sm + (w + W * g) * RS;
   const LineCoord lc = line_coord(geo, base, w, g, j, TPL);
-  const bool ylines = geo.axis == 1;
+  // x and y lines: [g][p][w] (x lines have W = 1); z lines: [p][g][w]
+  const bool ylines = geo.axis != 2;
   const int q0 = ylines ? (g * L + j) * W + w : (j * G + g) * W + w;
   const int qs = ylines ? TPL * W : TPL * G * W;
   C v[E];

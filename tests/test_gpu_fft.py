@@ -182,9 +182,9 @@ def test_xy_plane_pass_batched_fields(sns, oracle, cuda, dtype):
 @pytest.mark.parametrize("shape", [(64, 128, 64), (512, 16, 32), (32, 256, 16), (8, 64, 128)])
 def test_tma_staged_passes_match_direct_bit_for_bit(sns, oracle, cuda, monkeypatch, dtype, shape,
                                                     stages):
-    """The y and z passes of the 3D transform over TMA-staged tiles
-    (SNS_FFT_TMA = 1 or 2 stages; a tuned plan may choose them) give the
-    direct-load passes' results bit for bit, forward (with Nyquist zeroing)
+    """The passes of the 3D transform over TMA-staged tiles (SNS_FFT_TMA = 1
+    or 2 stages; a tuned plan may choose them; x lines where a row fits one
+    box) give the direct-load passes' results bit for bit, forward (with Nyquist zeroing)
     and inverse (with 1/N), 1 and 3 fields; the record of the bounded waits
     stays clear (sns_fft3d_check)."""
     from spectral_upcxx_b200 import ic
